@@ -1,0 +1,316 @@
+// Test-infrastructure harness around the UNMODIFIED reference (JLiu-1/Falcons) headers.
+//
+// oracle/Makefile compiles this file against the reference's own include tree and its
+// vendored FSE sources, producing oracle/_ref/libfalcons_ref.so.  Only the tests, the
+// fixture generator under tests/golden/ and bench.py's reference arm load it, and only
+// as a checker or a timed CPU baseline.  Nothing in the product links it.
+//
+// Entry points (all extern "C", plain pointers):
+//   ref_compress_<t>            include/Falcons/api/falcons.hpp:54       (Falcons_compress into a buffer)
+//   ref_decompress_<t>          include/Falcons/api/falcons.hpp:184      (capacity-checked Falcons_decompress)
+//   ref_size_bound_<t>          include/Falcons/api/impl/FalconsImpl.hpp:44
+//   ref_interp_compress_<t>     decomposition/InterpolationDecomposition.hpp:131 (codes + unpred, in stream order)
+//   ref_interp_decompress_<t>   decomposition/InterpolationDecomposition.hpp:48
+//   ref_rlefse_encode/decode    encoder/RleFseEncoder.hpp:850-1079
+//   ref_zstd_compress/decompress lossless/Lossless_zstd.hpp:29-78
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "Falcons/api/falcons.hpp"
+
+using namespace Falcons;
+
+extern "C" {
+struct ref_conf {
+    int32_t cmprAlgo;
+    int32_t errorBoundMode;
+    double absErrorBound;
+    double relErrorBound;
+    double psnrErrorBound;
+    double l2normErrorBound;
+    int32_t interpAlgo;
+    int32_t interpDirection;
+    int32_t interpAnchorStride;
+    int32_t openmp;
+    double interpAlpha;
+    double interpBeta;
+    int32_t quantbinCnt;
+    int32_t lorenzo;
+    int32_t lorenzo2;
+    int32_t regression;
+    int32_t regression2;
+    int32_t blockSize;
+};
+}
+
+static thread_local std::string g_err;
+
+static Config make_conf(const size_t *dims, int N, const ref_conf *c) {
+    Config conf;
+    conf.setDims(dims, dims + N);
+    conf.cmprAlgo = static_cast<uint8_t>(c->cmprAlgo);
+    conf.errorBoundMode = static_cast<uint8_t>(c->errorBoundMode);
+    conf.absErrorBound = c->absErrorBound;
+    conf.relErrorBound = c->relErrorBound;
+    conf.psnrErrorBound = c->psnrErrorBound;
+    conf.l2normErrorBound = c->l2normErrorBound;
+    conf.interpAlgo = static_cast<uint8_t>(c->interpAlgo);
+    conf.interpDirection = static_cast<uint8_t>(c->interpDirection);
+    conf.interpAnchorStride = c->interpAnchorStride;
+    conf.openmp = c->openmp != 0;
+    conf.interpAlpha = c->interpAlpha;
+    conf.interpBeta = c->interpBeta;
+    if (c->quantbinCnt > 0) conf.quantbinCnt = c->quantbinCnt;
+    conf.lorenzo = c->lorenzo != 0;
+    conf.lorenzo2 = c->lorenzo2 != 0;
+    conf.regression = c->regression != 0;
+    conf.regression2 = c->regression2 != 0;
+    if (c->blockSize > 0) conf.blockSize = c->blockSize;
+    return conf;
+}
+
+template <class T>
+static long long do_compress(const size_t *dims, int N, const ref_conf *c, T *data, char *out, size_t cap) {
+    try {
+        Config conf = make_conf(dims, N, c);
+        return static_cast<long long>(Falcons_compress<T>(conf, data, out, cap));
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+template <class T>
+static long long do_size_bound(const size_t *dims, int N, const ref_conf *c) {
+    Config conf = make_conf(dims, N, c);
+    return static_cast<long long>(Falcons_compress_size_bound<T>(conf));
+}
+
+template <class T>
+static int do_decompress(const char *cmp, size_t size, T *out, size_t cap, size_t *dims_out, int *N_out) {
+    try {
+        Config conf;
+        T *dst = out;
+        Falcons_decompress<T>(conf, cmp, size, dst, cap);
+        *N_out = conf.N;
+        for (int i = 0; i < conf.N; i++) dims_out[i] = conf.dims[i];
+        return 0;
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+template <class T, uint N>
+static int interp_compress_n(const size_t *dims, const ref_conf *c, int tuning, T *data, int16_t *codes,
+                             size_t *ncodes, T *unpred, size_t *nunpred) {
+    Config conf = make_conf(dims, N, c);
+    conf.cmprAlgo = ALGO_INTERP;
+    if (conf.interpAnchorStride < 0) {
+        std::array<size_t, 4> anchor_strides = {4096, 128, 32, 16};
+        conf.interpAnchorStride = anchor_strides[N - 1];
+    }
+    int16_t *q = nullptr;
+    uint64_t nq = 0;
+    std::vector<T> up;
+    if (tuning) {
+        auto dec = make_decomposition_interpolation<TUNING::ENABLED, T, N>(
+            conf, LinearQuantizer<T>(conf.absErrorBound, conf.quantbinCnt / 2));
+        std::tie(q, nq) = dec.compress(conf, data);
+        up = dec.test_unpred();
+    } else {
+        auto dec = make_decomposition_interpolation<TUNING::DISABLED, T, N>(
+            conf, LinearQuantizer<T>(conf.absErrorBound, conf.quantbinCnt / 2));
+        std::tie(q, nq) = dec.compress(conf, data);
+        up = dec.test_unpred();
+    }
+    if (nq > *ncodes || up.size() > *nunpred) {
+        delete[] q;
+        g_err = "output arrays too small";
+        return -1;
+    }
+    memcpy(codes, q, nq * sizeof(int16_t));
+    memcpy(unpred, up.data(), up.size() * sizeof(T));
+    *ncodes = nq;
+    *nunpred = up.size();
+    delete[] q;
+    return 0;
+}
+
+template <class T, uint N>
+static int interp_decompress_n(const size_t *dims, const ref_conf *c, const int16_t *codes, size_t ncodes,
+                               const T *unpred, size_t nunpred, T *out) {
+    Config conf = make_conf(dims, N, c);
+    conf.cmprAlgo = ALGO_INTERP;
+    if (conf.interpAnchorStride < 0) {
+        std::array<size_t, 4> anchor_strides = {4096, 128, 32, 16};
+        conf.interpAnchorStride = anchor_strides[N - 1];
+    }
+    // Serialise the decomposition header exactly as InterpolationDecomposition::save does
+    // (InterpolationDecomposition.hpp:241-251 + LinearQuantizer.hpp:142-152), then load it.
+    std::vector<uchar> buf(256 + nunpred * sizeof(T));
+    uchar *p = buf.data();
+    size_t max_dim = 1;
+    for (uint i = 0; i < N; i++) max_dim = std::max(max_dim, dims[i]);
+    for (uint i = 0; i < N; i++) write(static_cast<size_t>(dims[i]), p);
+    write(static_cast<uint>(max_dim), p);
+    write(static_cast<int>(conf.interpAlgo), p);
+    write(static_cast<int>(conf.interpDirection), p);
+    write(static_cast<size_t>(conf.interpAnchorStride), p);
+    write(conf.interpAlpha, p);
+    write(conf.interpBeta, p);
+    write(static_cast<uchar>(0b10), p);
+    write(conf.absErrorBound, p);
+    write(static_cast<int>(conf.quantbinCnt / 2), p);
+    write(static_cast<int>(nunpred), p);
+    write(unpred, nunpred, p);
+    const uchar *rp = buf.data();
+    size_t remaining = p - buf.data();
+    auto dec = make_decomposition_interpolation<TUNING::DISABLED, T, N>(
+        conf, LinearQuantizer<T>(conf.absErrorBound, conf.quantbinCnt / 2));
+    dec.load(rp, remaining);
+    std::vector<int16_t> q(codes, codes + ncodes);
+    q.resize(ncodes + 64);
+    dec.decompress(conf, q.data(), out);
+    return 0;
+}
+
+template <class T>
+static int do_interp_compress(const size_t *dims, int N, const ref_conf *c, int tuning, T *data, int16_t *codes,
+                              size_t *ncodes, T *unpred, size_t *nunpred) {
+    try {
+        switch (N) {
+            case 1: return interp_compress_n<T, 1>(dims, c, tuning, data, codes, ncodes, unpred, nunpred);
+            case 2: return interp_compress_n<T, 2>(dims, c, tuning, data, codes, ncodes, unpred, nunpred);
+            case 3: return interp_compress_n<T, 3>(dims, c, tuning, data, codes, ncodes, unpred, nunpred);
+            case 4: return interp_compress_n<T, 4>(dims, c, tuning, data, codes, ncodes, unpred, nunpred);
+        }
+    } catch (std::exception &e) {
+        g_err = e.what();
+    }
+    return -1;
+}
+
+template <class T>
+static int do_interp_decompress(const size_t *dims, int N, const ref_conf *c, const int16_t *codes, size_t ncodes,
+                                const T *unpred, size_t nunpred, T *out) {
+    try {
+        switch (N) {
+            case 1: return interp_decompress_n<T, 1>(dims, c, codes, ncodes, unpred, nunpred, out);
+            case 2: return interp_decompress_n<T, 2>(dims, c, codes, ncodes, unpred, nunpred, out);
+            case 3: return interp_decompress_n<T, 3>(dims, c, codes, ncodes, unpred, nunpred, out);
+            case 4: return interp_decompress_n<T, 4>(dims, c, codes, ncodes, unpred, nunpred, out);
+        }
+    } catch (std::exception &e) {
+        g_err = e.what();
+    }
+    return -1;
+}
+
+extern "C" {
+const char *ref_last_error() { return g_err.c_str(); }
+
+long long ref_compress_f32(const size_t *d, int N, const ref_conf *c, float *x, char *o, size_t cap) {
+    return do_compress<float>(d, N, c, x, o, cap);
+}
+long long ref_compress_f64(const size_t *d, int N, const ref_conf *c, double *x, char *o, size_t cap) {
+    return do_compress<double>(d, N, c, x, o, cap);
+}
+long long ref_size_bound_f32(const size_t *d, int N, const ref_conf *c) { return do_size_bound<float>(d, N, c); }
+long long ref_size_bound_f64(const size_t *d, int N, const ref_conf *c) { return do_size_bound<double>(d, N, c); }
+int ref_decompress_f32(const char *s, size_t n, float *o, size_t cap, size_t *dims, int *N) {
+    return do_decompress<float>(s, n, o, cap, dims, N);
+}
+int ref_decompress_f64(const char *s, size_t n, double *o, size_t cap, size_t *dims, int *N) {
+    return do_decompress<double>(s, n, o, cap, dims, N);
+}
+int ref_interp_compress_f32(const size_t *d, int N, const ref_conf *c, int tuning, float *x, int16_t *q, size_t *nq,
+                            float *u, size_t *nu) {
+    return do_interp_compress<float>(d, N, c, tuning, x, q, nq, u, nu);
+}
+int ref_interp_compress_f64(const size_t *d, int N, const ref_conf *c, int tuning, double *x, int16_t *q, size_t *nq,
+                            double *u, size_t *nu) {
+    return do_interp_compress<double>(d, N, c, tuning, x, q, nq, u, nu);
+}
+int ref_interp_decompress_f32(const size_t *d, int N, const ref_conf *c, const int16_t *q, size_t nq, const float *u,
+                              size_t nu, float *o) {
+    return do_interp_decompress<float>(d, N, c, q, nq, u, nu, o);
+}
+int ref_interp_decompress_f64(const size_t *d, int N, const ref_conf *c, const int16_t *q, size_t nq, const double *u,
+                              size_t nu, double *o) {
+    return do_interp_decompress<double>(d, N, c, q, nq, u, nu, o);
+}
+
+// RleFseEncoder<int16_t>: [u8 method|delta<<7][u16 lo][u16 mode] + payload, as FalconsGenericCompressor writes it.
+long long ref_rlefse_encode(const int16_t *codes, size_t n, uint8_t *out, size_t cap) {
+    try {
+        std::vector<int16_t> tmp(codes, codes + n);
+        tmp.resize(n + 16);
+        RleFseEncoder<int16_t> enc;
+        enc.preprocess_encode(tmp.data(), n, 65536);
+        std::vector<uchar> buf(std::max<size_t>(cap, 8 * n + 65536));
+        uchar *p = buf.data();
+        enc.save(p);
+        enc.encode(tmp.data(), n, p);
+        size_t len = p - buf.data();
+        if (len > cap) {
+            g_err = "capacity";
+            return -1;
+        }
+        memcpy(out, buf.data(), len);
+        return static_cast<long long>(len);
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+long long ref_rlefse_decode(const uint8_t *in, size_t n_in, size_t n_codes, int16_t *out) {
+    try {
+        RleFseEncoder<int16_t> enc;
+        const uchar *p = in;
+        size_t rem = n_in;
+        enc.load(p, rem);
+        int16_t *q = enc.decode(p, n_codes);
+        memcpy(out, q, n_codes * sizeof(int16_t));
+        delete[] q;
+        return static_cast<long long>(p - in);
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+long long ref_zstd_compress(const uint8_t *src, size_t n, uint8_t *dst, size_t cap) {
+    try {
+        Lossless_zstd z;
+        return static_cast<long long>(z.compress(src, n, dst, cap));
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+long long ref_zstd_decompress(const uint8_t *src, size_t n, uint8_t *dst, size_t cap) {
+    try {
+        Lossless_zstd z;
+        uchar *d = nullptr;
+        size_t dl = 0;
+        z.decompress(src, n, d, dl);
+        if (dl > cap) {
+            free(d);
+            g_err = "capacity";
+            return -1;
+        }
+        memcpy(dst, d, dl);
+        free(d);
+        return static_cast<long long>(dl);
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+}
