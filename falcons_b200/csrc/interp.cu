@@ -1,0 +1,708 @@
+// Interpolation decomposition kernels (prediction + linear quantization) for sm_100a.
+//
+// Plan construction mirrors the reference's level loop and pass order:
+//   levels / anchors / per-level eb   InterpolationDecomposition.hpp:131-239, 286-359
+//   non-tuning pass order             InterpolationDecomposition.hpp:2294-2527
+//   tuning / 4-D generic sweeps       InterpolationDecomposition.hpp:436-528 (fastest_dim_first)
+//   legacy 1-D line (tuning N<=2)     InterpolationDecomposition.hpp:371-419
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+#include "interp.cuh"
+
+namespace fb2 {
+
+static long long count_of(long long dim, long long st) { return (dim - 1) / st + 1; }
+
+// ------------------------------------------------------------------------------------------ plan
+namespace {
+
+struct Builder {
+    InterpPlan &P;
+    const InterpParams &prm;
+    long long pos = 0;  // next code position
+
+    Builder(InterpPlan &p, const InterpParams &q) : P(p), prm(q) {}
+
+    static PassLaunch blank() {
+        PassLaunch L{};
+        for (int i = 0; i < 4; i++) { L.cnt[i] = 1; L.est[i] = 0; }
+        return L;
+    }
+
+    // Row-buffer pass along dim pd; `outer` (may be -1) and `inner` are the other dims.
+    void rows(int level, long long s, int pd, int outer, long long so, int inner, long long sk, bool skip) {
+        const long long n = (P.dims[pd] - 1) / s + 1;
+        if (n <= 1) return;
+        const long long co = outer >= 0 ? count_of(P.dims[outer], so) : 1;
+        const long long C = count_of(P.dims[inner], sk);
+        const long long m = n / 2;
+        const bool cubic = prm.cubic != 0;
+        const bool late = cubic && (n % 2 == 0) && n > 2 && P.N == 3;
+        const bool lin_tail = !cubic && (n % 2 == 0) && n >= 3 && !skip;
+        const long long mr = late ? m - 1 : m;
+        PassLaunch L = blank();
+        L.kind = KIND_ROW;
+        L.cubic = cubic;
+        L.skip = skip;
+        L.n = (int)n;
+        L.step = s * P.off[pd];
+        L.A = co;
+        L.C = C;
+        L.sa = outer >= 0 ? so * P.off[outer] : 0;
+        L.sc = sk * P.off[inner];
+        L.t0 = 1;
+        L.rows_in_group = mr;
+        L.b_off = 0;
+        L.p_base = pos;
+        L.level = level;
+        L.B = lin_tail ? mr - 1 : mr;
+        if (L.B > 0) P.passes.push_back(L);
+        if (lin_tail) {
+            PassLaunch T = L;
+            T.B = 1;
+            T.t0 = (int)(n - 1);
+            T.b_off = mr - 1;
+            P.passes.push_back(T);
+        }
+        if (late) {
+            PassLaunch E = L;
+            E.B = 1;
+            E.t0 = (int)(n - 1);
+            E.rows_in_group = 1;
+            E.b_off = 0;
+            E.p_base = pos + co * mr * C;
+            P.passes.push_back(E);
+        }
+        pos += co * m * C;
+    }
+
+    // 1-D line pass along the last dim; lines enumerated by (a over dim0, b over dim1) as given.
+    void lines(int level, long long s, int pd, long long A, long long sa, long long B, long long sb, bool skip) {
+        const long long n = (P.dims[pd] - 1) / s + 1;
+        if (n <= 1) return;
+        PassLaunch L = blank();
+        L.kind = KIND_LINE;
+        L.cubic = prm.cubic != 0;
+        L.skip = skip;
+        L.n = (int)n;
+        L.step = s * P.off[pd];
+        L.A = A;
+        L.B = B;
+        L.C = n / 2;
+        L.sa = sa;
+        L.sb = sb;
+        L.p_base = pos;
+        L.level = level;
+        P.passes.push_back(L);
+        pos += A * B * (n / 2);
+    }
+
+    void disabled_level(int level, long long s, bool last) {
+        const long long s2 = 2 * s;
+        const int N = P.N;
+        if (N == 1) {
+            lines(level, s, 0, 1, 0, 1, 0, last);
+        } else if (N == 2) {
+            if (prm.direction == 0) {
+                rows(level, s, 0, -1, 0, 1, s2, false);
+                lines(level, s, 1, 1, 0, count_of(P.dims[0], s), s * P.off[0], last);
+            } else {
+                lines(level, s, 1, 1, 0, count_of(P.dims[0], s2), s2 * P.off[0], false);
+                rows(level, s, 0, -1, 0, 1, s, last);
+            }
+        } else {
+            if (prm.direction == 0) {
+                rows(level, s, 0, 1, s2, 2, s2, false);
+                rows(level, s, 1, 0, s, 2, s2, false);
+                lines(level, s, 2, count_of(P.dims[0], s), s * P.off[0], count_of(P.dims[1], s), s * P.off[1], last);
+            } else {
+                lines(level, s, 2, count_of(P.dims[0], s2), s2 * P.off[0], count_of(P.dims[1], s2), s2 * P.off[1],
+                      false);
+                rows(level, s, 1, 0, s2, 2, s, false);
+                rows(level, s, 0, 1, s, 2, s, last);
+            }
+        }
+    }
+
+    // One foreach sweep of interpolation_1d_fastest_dim_first with the pass dim restricted to
+    // t in [t0, t1) step 2.
+    void generic_sweep(int level, long long s, int pd, const long long *st, long long t0, long long t1, int mode) {
+        const long long n = (P.dims[pd] - 1) / s + 1;
+        PassLaunch L = blank();
+        L.kind = KIND_GENERIC;
+        L.cubic = prm.cubic != 0;
+        L.n = (int)n;
+        L.step = s * P.off[pd];
+        L.N = P.N;
+        L.pd = pd;
+        L.g_t0 = (int)t0;
+        L.g_mode = mode;
+        long long total = 1;
+        for (int d = 0; d < P.N; d++) {
+            if (d == pd) {
+                L.cnt[d] = t1 > t0 ? (t1 - t0 + 1) / 2 : 0;
+                L.est[d] = 2 * L.step;
+            } else {
+                L.cnt[d] = count_of(P.dims[d], st[d]);
+                L.est[d] = st[d] * P.off[d];
+            }
+            total *= L.cnt[d];
+        }
+        L.A = 1;
+        L.B = 1;
+        L.C = total;
+        L.p_base = pos;
+        L.level = level;
+        if (total > 0) P.passes.push_back(L);
+        pos += total;
+    }
+
+    void generic_pass(int level, long long s, int pd, const long long *st) {
+        const long long n = (P.dims[pd] - 1) / s + 1;
+        if (n <= 1) return;
+        if (!prm.cubic) {
+            generic_sweep(level, s, pd, st, 1, n - 1, 0);
+            if (n % 2 == 0) generic_sweep(level, s, pd, st, n - 1, n, 2);
+        } else {
+            generic_sweep(level, s, pd, st, 3, n >= 3 ? n - 3 : 0, 0);
+            long long b[4];
+            int nb = 0;
+            b[nb++] = 1;
+            if (n % 2 == 1 && n > 3) b[nb++] = n - 2;
+            if (n % 2 == 0 && n > 4) b[nb++] = n - 3;
+            if (n % 2 == 0 && n > 2) b[nb++] = n - 1;
+            for (int i = 0; i < nb; i++) generic_sweep(level, s, pd, st, b[i], b[i] + 1, 1);
+        }
+    }
+
+    void tuning_level(int level, long long s) {
+        int seq[4];
+        {
+            int a[4] = {0, 1, 2, 3};
+            for (int it = 0; it < prm.direction; it++) {
+                int i = P.N - 2;
+                while (i >= 0 && a[i] >= a[i + 1]) i--;
+                if (i < 0) break;
+                int j = P.N - 1;
+                while (a[j] <= a[i]) j--;
+                std::swap(a[i], a[j]);
+                std::reverse(a + i + 1, a + P.N);
+            }
+            for (int i = 0; i < 4; i++) seq[i] = a[i];
+        }
+        const long long s2 = 2 * s;
+        if (P.N >= 3) {
+            long long st[4] = {s2, s2, s2, s2};
+            generic_pass(level, s, seq[0], st);
+            for (int i = 1; i < P.N; i++) {
+                st[seq[i - 1]] = s;
+                generic_pass(level, s, seq[i], st);
+            }
+        } else {
+            throw std::invalid_argument("tuning path for N<=2 is handled by the legacy line launcher");
+        }
+    }
+};
+
+}  // namespace
+
+InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
+    if (N < 1 || N > 4) throw std::invalid_argument("Data dimension higher than 4 is not supported.");
+    if (!(p.eb > 0) || !std::isfinite(p.eb)) throw std::invalid_argument("error bound must be positive and finite");
+    if (p.radius < 1 || p.radius > 32768) throw std::invalid_argument("quantization radius must be in [1, 32768]");
+    if (p.anchor < 0 || (p.anchor & (p.anchor - 1)) != 0)
+        throw std::invalid_argument("Anchor stride should be 0 or 2's exponentials");
+    if (p.cubic != 0 && p.cubic != 1) throw std::invalid_argument("interpAlgo must be linear (0) or cubic (1)");
+    int fact = 1;
+    for (int i = 2; i <= N; i++) fact *= i;
+    if (p.direction < 0 || p.direction >= fact) throw std::invalid_argument("interpDirection out of range");
+    if (!p.tuning && N >= 2 && N <= 3 && p.direction != 0 && p.direction != fact - 1)
+        throw std::invalid_argument("interpDirection must be 0 or N!-1 for 2-D and 3-D fields");
+    if (p.tuning && N <= 2) throw std::invalid_argument("device tuning sweeps support N >= 3 only");
+
+    InterpPlan P;
+    P.N = N;
+    P.num = 1;
+    for (int d = 0; d < N; d++) {
+        if (dims[d] < 1) throw std::invalid_argument("zero-sized dimension");
+        P.dims[d] = dims[d];
+        P.num *= dims[d];
+    }
+    for (int d = N; d < 4; d++) { P.dims[d] = 1; }
+    P.off[N - 1] = 1;
+    for (int d = N - 2; d >= 0; d--) P.off[d] = P.off[d + 1] * P.dims[d + 1];
+    for (int d = N; d < 4; d++) P.off[d] = 0;
+    if (P.num > (1LL << 40)) throw std::invalid_argument("field too large");
+
+    int level_count = -1;
+    bool use_anchor = false;
+    for (int d = 0; d < N; d++) {
+        int lv = (int)std::ceil(std::log2((double)P.dims[d]));
+        if (level_count < lv) level_count = lv;
+        if (P.dims[d] > p.anchor) use_anchor = true;
+    }
+    P.anchor = use_anchor ? p.anchor : 0;
+    if (P.anchor > 0) {
+        int maxl = (int)std::log2((double)P.anchor) + 1;
+        if (maxl <= level_count) level_count = maxl;
+    }
+    // index 0: the constructor's reciprocal 0.5/eb (used only by the anchor-free first point)
+    P.levels.push_back(QParams{p.eb, 2 * p.eb, 0.5 / p.eb, p.radius});
+    Builder b(P, p);
+    P.first_point = 0;
+    P.n_anchor = 0;
+    if (P.anchor == 0) {
+        P.first_point = 1;
+        b.pos = 1;
+    } else {
+        P.n_anchor = 1;
+        for (int d = 0; d < N; d++) P.n_anchor *= count_of(P.dims[d], P.anchor);
+        level_count--;
+    }
+    for (int level = level_count; level > 0; level--) {
+        double cur = p.eb;
+        if (p.alpha < 0) {
+            cur = level >= 3 ? p.eb * 0.5 : p.eb;
+        } else if (p.alpha >= 1) {
+            double ratio = std::pow(p.alpha, level - 1);
+            if (ratio > p.beta) ratio = p.beta;
+            cur = p.eb / ratio;
+        }
+        const int li = (int)P.levels.size();
+        P.levels.push_back(QParams{cur, 2 * cur, 1.0 / (2 * cur), p.radius});
+        const long long s = 1LL << (level - 1);
+        if (p.tuning || N == 4) b.tuning_level(li, s);
+        else b.disabled_level(li, s, level == 1);
+    }
+    P.n_codes = b.pos;
+    if (P.n_codes + P.n_anchor != P.num) throw std::logic_error("interpolation plan does not cover the field");
+    return P;
+}
+
+// ------------------------------------------------------------------------------------------ kernels
+namespace {
+
+constexpr int kTile = 4096;         // codes per escape-scan tile
+constexpr int kTileThreads = 256;   // 16 codes per thread
+constexpr int kPassThreads = 256;
+
+template <class T, int KIND, bool DECOMP>
+__global__ void __launch_bounds__(kPassThreads) k_pass(const PassLaunch L, T *__restrict__ x,
+                                                      int16_t *__restrict__ codes, T *__restrict__ esc,
+                                                      const QParams qp) {
+    const long long cstride = (long long)gridDim.x * blockDim.x;
+    for (long long a = blockIdx.z; a < L.A; a += gridDim.z) {
+        for (long long b = blockIdx.y; b < L.B; b += gridDim.y) {
+            for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.C; c += cstride) {
+                long long line, p;
+                int t;
+                Rule r;
+                if (KIND == KIND_ROW) {
+                    t = L.t0 + 2 * (int)b;
+                    line = a * L.sa + c * L.sc;
+                    p = L.p_base + (a * L.rows_in_group + b + L.b_off) * L.C + c;
+                    r = row_rule(L.cubic, t, L.n, L.skip);
+                } else if (KIND == KIND_LINE) {
+                    t = 1 + 2 * (int)c;
+                    line = a * L.sa + b * L.sb;
+                    p = L.p_base + (a * L.B + b) * L.C + c;
+                    r = line_rule(L.cubic, t, L.n);
+                } else if (KIND == KIND_GENERIC) {
+                    long long rem = c, off = 0;
+                    int tg = 0;
+#pragma unroll
+                    for (int d = 3; d >= 0; d--) {
+                        if (d >= L.N) continue;
+                        const long long i = rem % L.cnt[d];
+                        rem /= L.cnt[d];
+                        if (d == L.pd) tg = L.g_t0 + 2 * (int)i;
+                        else off += i * L.est[d];
+                    }
+                    t = tg;
+                    line = off;
+                    p = L.p_base + c;
+                    if (L.g_mode == 2) {
+                        r = L.n < 3 ? mk_rule(F_EQUAL, L.n - 2) : mk_rule(F_LINEAR1, L.n - 3, L.n - 2);
+                    } else if (L.g_mode == 1) {
+                        const int bb = t, n = L.n;
+                        if (bb >= 3) {
+                            if (bb + 3 < n) r = mk_rule(F_CUBIC, bb - 3, bb - 1, bb + 1, bb + 3);
+                            else if (bb + 1 < n) r = mk_rule(F_QUAD2, bb - 3, bb - 1, bb + 1);
+                            else r = mk_rule(F_LINEAR1, bb - 3, bb - 1);
+                        } else {
+                            if (bb + 3 < n) r = mk_rule(F_QUAD1, bb - 1, bb + 1, bb + 3);
+                            else if (bb + 1 < n) r = mk_rule(F_LINEAR, bb - 1, bb + 1);
+                            else r = mk_rule(F_EQUAL, bb - 1);
+                        }
+                    } else if (L.cubic) {
+                        r = mk_rule(F_CUBIC, t - 3, t - 1, t + 1, t + 3);
+                    } else {
+                        r = mk_rule(F_LINEAR, t - 1, t + 1);
+                    }
+                } else {  // KIND_LEGACY: one fixed target t per line
+                    t = L.g_t0;
+                    line = a * L.sa;
+                    p = L.p_base + a;
+                    r = mk_rule(L.g_rule[0], L.g_rule[1], L.g_rule[2], L.g_rule[3], L.g_rule[4]);
+                }
+                const long long st = L.step;
+                // Operands are never written by this launch: read them through the read-only path.
+                const T o0 = __ldg(x + line + (long long)r.o0 * st);
+                const T o1 = r.f != F_EQUAL ? __ldg(x + line + (long long)r.o1 * st) : o0;
+                const T o2 = r.f >= F_QUAD1 ? __ldg(x + line + (long long)r.o2 * st) : o0;
+                const T o3 = r.f == F_CUBIC ? __ldg(x + line + (long long)r.o3 * st) : o0;
+                const T pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+                T *xp = x + line + (long long)t * st;
+                if (!DECOMP) {
+                    const T v = *xp;
+                    T recon;
+                    const int q = quantize<T>(v, pred, qp, recon);
+                    codes[p] = (int16_t)q;
+                    if (q == -qp.radius) esc[p] = v;
+                    else if (!L.skip) *xp = recon;
+                } else {
+                    const int q = codes[p];
+                    *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
+                }
+            }
+        }
+    }
+}
+
+template <class T, bool DECOMP>
+__global__ void k_first_point(T *x, int16_t *codes, T *esc, const QParams qp) {
+    if (!DECOMP) {
+        T recon;
+        const T v = x[0];
+        const int q = quantize<T>(v, T(0), qp, recon);
+        codes[0] = (int16_t)q;
+        if (q == -qp.radius) esc[0] = v;
+        else x[0] = recon;
+    } else {
+        const int q = codes[0];
+        x[0] = q != -qp.radius ? dequantize<T>(q, T(0), qp) : esc[0];
+    }
+}
+
+struct AnchorGrid {
+    int N;
+    long long cnt[4], est[4];
+    long long total;
+};
+
+template <class T, bool DECOMP>
+__global__ void k_anchors(const AnchorGrid G, T *x, T *unpred) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < G.total;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long rem = i, off = 0;
+        for (int d = G.N - 1; d >= 0; d--) {
+            off += (rem % G.cnt[d]) * G.est[d];
+            rem /= G.cnt[d];
+        }
+        if (!DECOMP) unpred[i] = x[off];
+        else x[off] = unpred[i];
+    }
+}
+
+// Escape counting per tile of kTile codes.
+__global__ void __launch_bounds__(kTileThreads) k_esc_count(const int16_t *__restrict__ codes, long long n, int esc,
+                                                            unsigned *__restrict__ tile_count) {
+    const long long base = (long long)blockIdx.x * kTile + threadIdx.x * 16;
+    int cnt = 0;
+    if (base + 16 <= n) {
+        const int4 *v = reinterpret_cast<const int4 *>(codes + base);
+        int4 w[2] = {__ldg(v), __ldg(v + 1)};
+        const int16_t *h = reinterpret_cast<const int16_t *>(w);
+#pragma unroll
+        for (int j = 0; j < 16; j++) cnt += (h[j] == esc);
+    } else {
+        for (long long j = base; j < n && j < base + 16; j++) cnt += (codes[j] == esc);
+    }
+    // block reduction
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    __shared__ int ws[kTileThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int v2 = threadIdx.x < kTileThreads / 32 ? ws[threadIdx.x] : 0;
+        v2 = __reduce_add_sync(0xffffffffu, v2);
+        if (threadIdx.x == 0) tile_count[blockIdx.x] = v2;
+    }
+}
+
+// Exclusive scan of tile counts (single block, chunked); writes offsets[0..ntiles] and the total.
+__global__ void __launch_bounds__(1024) k_scan_u32(const unsigned *__restrict__ in, unsigned long long *__restrict__ out,
+                                                   long long n, unsigned long long *total) {
+    __shared__ unsigned long long warp_sums[32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < n; base += 1024) {
+        const long long i = base + threadIdx.x;
+        unsigned long long v = i < n ? in[i] : 0;
+        // inclusive warp scan
+        unsigned long long s = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) >= o) s += y;
+        }
+        if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = s;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            unsigned long long w = warp_sums[threadIdx.x];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (threadIdx.x >= o) w += y;
+            }
+            warp_sums[threadIdx.x] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const unsigned long long wprev = (threadIdx.x >> 5) ? warp_sums[(threadIdx.x >> 5) - 1] : 0;
+        if (i < n) out[i] = carry + wprev + s - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += wprev + s;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[n] = carry;
+        if (total) *total = carry;
+    }
+}
+
+// Per tile: rank the escapes in stream order and move their values between the scattered
+// per-position array `esc` and the compact unpredictable list (after the anchors).
+template <class T, bool DECOMP>
+__global__ void __launch_bounds__(kTileThreads) k_esc_scatter(const int16_t *__restrict__ codes, long long n, int esc_code,
+                                                              const unsigned long long *__restrict__ tile_off,
+                                                              T *__restrict__ esc, T *__restrict__ unpred,
+                                                              long long n_anchor) {
+    const unsigned long long t0 = tile_off[blockIdx.x], t1 = tile_off[blockIdx.x + 1];
+    if (t0 == t1) return;
+    const long long base = (long long)blockIdx.x * kTile + threadIdx.x * 16;
+    unsigned mask = 0;
+    for (int j = 0; j < 16; j++) {
+        const long long i = base + j;
+        if (i < n && codes[i] == esc_code) mask |= 1u << j;
+    }
+    const int cnt = __popc(mask);
+    // block exclusive scan of cnt
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int s = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+    }
+    __shared__ int wsum[kTileThreads / 32];
+    if (lane == 31) wsum[wid] = s;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < wid; w++) before += wsum[w];
+    unsigned long long r = t0 + before + s - cnt;
+    while (mask) {
+        const int j = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const long long i = base + j;
+        if (!DECOMP) unpred[n_anchor + r] = esc[i];
+        else esc[i] = unpred[n_anchor + r];
+        r++;
+    }
+}
+
+template <class T, bool DECOMP>
+void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
+    dim3 block(kPassThreads);
+    const long long gx = std::min<long long>((L.C + kPassThreads - 1) / kPassThreads, 1 << 20);
+    dim3 grid((unsigned)std::max<long long>(gx, 1), (unsigned)std::min<long long>(L.B, 65535),
+              (unsigned)std::min<long long>(L.A, 65535));
+    switch (L.kind) {
+        case KIND_ROW: k_pass<T, KIND_ROW, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
+        case KIND_LINE: k_pass<T, KIND_LINE, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
+        case KIND_GENERIC: k_pass<T, KIND_GENERIC, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
+        default: k_pass<T, KIND_LEGACY, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
+    }
+    FB2_CHECK_LAUNCH();
+}
+
+struct WsLayout {
+    size_t esc_off, tiles_off, scan_off, total_off, bytes;
+    long long ntiles;
+};
+
+WsLayout ws_layout(const InterpPlan &plan, int elem) {
+    WsLayout w;
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    w.ntiles = (plan.n_codes + kTile - 1) / kTile;
+    w.esc_off = 0;
+    w.tiles_off = al(w.esc_off + (size_t)std::max<long long>(plan.n_codes, 1) * elem);
+    w.scan_off = al(w.tiles_off + (size_t)(w.ntiles + 1) * 4);
+    w.total_off = al(w.scan_off + (size_t)(w.ntiles + 1) * 8);
+    w.bytes = al(w.total_off + 8);
+    return w;
+}
+
+AnchorGrid anchor_grid(const InterpPlan &plan) {
+    AnchorGrid G;
+    G.N = plan.N;
+    G.total = plan.n_anchor;
+    for (int d = 0; d < 4; d++) {
+        G.cnt[d] = d < plan.N ? count_of(plan.dims[d], plan.anchor) : 1;
+        G.est[d] = d < plan.N ? plan.anchor * plan.off[d] : 0;
+    }
+    return G;
+}
+
+}  // namespace
+
+size_t interp_workspace_bytes(const InterpPlan &plan, int elem_size) { return ws_layout(plan, elem_size).bytes; }
+
+template <class T>
+void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
+                     unsigned long long *d_n_esc, cudaStream_t st) {
+    const WsLayout w = ws_layout(plan, sizeof(T));
+    char *ws = static_cast<char *>(d_ws);
+    T *esc = reinterpret_cast<T *>(ws + w.esc_off);
+    unsigned *tiles = reinterpret_cast<unsigned *>(ws + w.tiles_off);
+    unsigned long long *scan = reinterpret_cast<unsigned long long *>(ws + w.scan_off);
+    if (plan.n_anchor > 0) {
+        const AnchorGrid G = anchor_grid(plan);
+        const int blocks = (int)std::min<long long>((G.total + 255) / 256, 4096);
+        k_anchors<T, false><<<blocks, 256, 0, st>>>(G, d_x, d_unpred);
+        FB2_CHECK_LAUNCH();
+    }
+    if (plan.first_point) {
+        k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0]);
+        FB2_CHECK_LAUNCH();
+    }
+    for (const PassLaunch &L : plan.passes) launch_pass<T, false>(L, d_x, d_codes, esc, plan.levels[L.level], st);
+    const int escc = -plan.levels[0].radius;
+    if (w.ntiles > 0) {
+        k_esc_count<<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, tiles);
+        FB2_CHECK_LAUNCH();
+        k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, d_n_esc);
+        FB2_CHECK_LAUNCH();
+        k_esc_scatter<T, false><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, scan, esc,
+                                                                           d_unpred, plan.n_anchor);
+        FB2_CHECK_LAUNCH();
+    } else if (d_n_esc) {
+        FB2_CUDA(cudaMemsetAsync(d_n_esc, 0, 8, st));
+    }
+}
+
+template <class T>
+void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, T *d_x, void *d_ws,
+                       cudaStream_t st) {
+    const WsLayout w = ws_layout(plan, sizeof(T));
+    char *ws = static_cast<char *>(d_ws);
+    T *esc = reinterpret_cast<T *>(ws + w.esc_off);
+    unsigned *tiles = reinterpret_cast<unsigned *>(ws + w.tiles_off);
+    unsigned long long *scan = reinterpret_cast<unsigned long long *>(ws + w.scan_off);
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(ws + w.total_off);
+    int16_t *codes = const_cast<int16_t *>(d_codes);
+    T *unpred = const_cast<T *>(d_unpred);
+    if (plan.n_anchor > 0) {
+        const AnchorGrid G = anchor_grid(plan);
+        const int blocks = (int)std::min<long long>((G.total + 255) / 256, 4096);
+        k_anchors<T, true><<<blocks, 256, 0, st>>>(G, d_x, unpred);
+        FB2_CHECK_LAUNCH();
+    }
+    const int escc = -plan.levels[0].radius;
+    if (w.ntiles > 0) {
+        k_esc_count<<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(codes, plan.n_codes, escc, tiles);
+        FB2_CHECK_LAUNCH();
+        k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, total);
+        FB2_CHECK_LAUNCH();
+        k_esc_scatter<T, true><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(codes, plan.n_codes, escc, scan, esc,
+                                                                          unpred, plan.n_anchor);
+        FB2_CHECK_LAUNCH();
+    }
+    if (plan.first_point) {
+        k_first_point<T, true><<<1, 1, 0, st>>>(d_x, codes, esc, plan.levels[0]);
+        FB2_CHECK_LAUNCH();
+    }
+    for (const PassLaunch &L : plan.passes) launch_pass<T, true>(L, d_x, codes, esc, plan.levels[L.level], st);
+}
+
+// ------------------------------------------------------------------------------------------ range
+namespace {
+constexpr int kRangeBlocks = 1184;  // 8 x 148 SMs
+
+template <class T>
+__global__ void __launch_bounds__(256) k_minmax(const T *__restrict__ x, long long n, T *__restrict__ part) {
+    T lo = x[0], hi = x[0];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const T v = __ldg(x + i);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+    }
+    __shared__ T slo[256], shi[256];
+    slo[threadIdx.x] = lo;
+    shi[threadIdx.x] = hi;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            slo[threadIdx.x] = slo[threadIdx.x + s] < slo[threadIdx.x] ? slo[threadIdx.x + s] : slo[threadIdx.x];
+            shi[threadIdx.x] = shi[threadIdx.x + s] > shi[threadIdx.x] ? shi[threadIdx.x + s] : shi[threadIdx.x];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = slo[0];
+        part[2 * blockIdx.x + 1] = shi[0];
+    }
+}
+
+template <class T>
+__global__ void k_minmax_final(const T *__restrict__ part, int nb, T *out) {
+    __shared__ T slo[256], shi[256];
+    T lo = part[0], hi = part[1];
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+        lo = part[2 * i] < lo ? part[2 * i] : lo;
+        hi = part[2 * i + 1] > hi ? part[2 * i + 1] : hi;
+    }
+    slo[threadIdx.x] = lo;
+    shi[threadIdx.x] = hi;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            slo[threadIdx.x] = slo[threadIdx.x + s] < slo[threadIdx.x] ? slo[threadIdx.x + s] : slo[threadIdx.x];
+            shi[threadIdx.x] = shi[threadIdx.x + s] > shi[threadIdx.x] ? shi[threadIdx.x + s] : shi[threadIdx.x];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = Arith<T>::sub(shi[0], slo[0]);
+        out[1] = slo[0];
+        out[2] = shi[0];
+    }
+}
+}  // namespace
+
+size_t range_workspace_bytes() { return (size_t)kRangeBlocks * 2 * sizeof(double); }
+
+template <class T>
+void device_range(const T *d_x, long long n, T *d_out, void *d_ws, cudaStream_t st) {
+    T *part = static_cast<T *>(d_ws);
+    const int nb = (int)std::max<long long>(1, std::min<long long>(kRangeBlocks, (n + 255) / 256));
+    k_minmax<T><<<nb, 256, 0, st>>>(d_x, n, part);
+    FB2_CHECK_LAUNCH();
+    k_minmax_final<T><<<1, 256, 0, st>>>(part, nb, d_out);
+    FB2_CHECK_LAUNCH();
+}
+
+template void interp_compress<float>(const InterpPlan &, float *, int16_t *, float *, void *, unsigned long long *,
+                                     cudaStream_t);
+template void interp_compress<double>(const InterpPlan &, double *, int16_t *, double *, void *,
+                                      unsigned long long *, cudaStream_t);
+template void interp_decompress<float>(const InterpPlan &, const int16_t *, const float *, float *, void *,
+                                       cudaStream_t);
+template void interp_decompress<double>(const InterpPlan &, const int16_t *, const double *, double *, void *,
+                                        cudaStream_t);
+template void device_range<float>(const float *, long long, float *, void *, cudaStream_t);
+template void device_range<double>(const double *, long long, double *, void *, cudaStream_t);
+
+}  // namespace fb2

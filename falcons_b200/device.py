@@ -1,0 +1,105 @@
+"""Stage-level entry points on device-resident torch tensors (CUDA), through the C ABI.
+
+These expose the individual stages of the path — value range, interpolation decomposition,
+entropy coding — for tests, benchmarks and callers that keep fields in HBM.  PyTorch is used
+only to own device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+
+_DT = {torch.float32: _lib.F32, torch.float64: _lib.F64}
+
+
+def _dtype_code(t: torch.Tensor) -> int:
+    if t.dtype not in _DT:
+        raise TypeError("unsupported on GPU build: only float32 and float64 fields are supported")
+    return _DT[t.dtype]
+
+
+def _stream_ptr(stream) -> ctypes.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def interp_params(eb, interp_algo=1, direction=0, anchor_stride=None, ndim=3, alpha=1.25, beta=2.0,
+                  radius=32768, tuning=False) -> _lib.InterpParams:
+    if anchor_stride is None or anchor_stride < 0:
+        anchor_stride = {1: 4096, 2: 128, 3: 32, 4: 16}[ndim]
+    return _lib.InterpParams(float(eb), int(interp_algo), int(direction), int(anchor_stride), float(alpha),
+                             float(beta), int(radius), int(tuning))
+
+
+def value_range(x: torch.Tensor, ctx=None, stream=None) -> float:
+    ctx = ctx or _lib.default_context(x.device.index or 0)
+    out = ctypes.c_double(0)
+    _lib.check(_lib.lib().falcons_device_range(ctx.ptr, _dtype_code(x), ctypes.c_void_p(x.data_ptr()),
+                                                ctypes.c_size_t(x.numel()), ctypes.byref(out),
+                                                _stream_ptr(stream)), "device_range")
+    return out.value
+
+
+def interp_compress(x: torch.Tensor, params: _lib.InterpParams, ctx=None, stream=None):
+    """Predict + quantize `x` in place (it ends as the reference's partial reconstruction).
+
+    Returns (codes int16 [n_codes], unpred [anchors + escapes]) in stream order, on the device.
+    """
+    assert x.is_cuda and x.is_contiguous()
+    ctx = ctx or _lib.default_context(x.device.index or 0)
+    dims = (ctypes.c_size_t * x.dim())(*x.shape)
+    codes = torch.empty(x.numel() + 16, dtype=torch.int16, device=x.device)
+    unpred = torch.empty(x.numel() + 16, dtype=x.dtype, device=x.device)
+    nq, nu = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    _lib.check(_lib.lib().falcons_interp_compress(ctx.ptr, _dtype_code(x), dims, x.dim(), ctypes.byref(params),
+                                                  ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(codes.data_ptr()),
+                                                  ctypes.c_void_p(unpred.data_ptr()), ctypes.byref(nq),
+                                                  ctypes.byref(nu), _stream_ptr(stream)), "interp_compress")
+    return codes[:nq.value], unpred[:nu.value]
+
+
+def interp_decompress(shape, dtype, codes: torch.Tensor, unpred: torch.Tensor, params: _lib.InterpParams,
+                      out: torch.Tensor | None = None, ctx=None, stream=None) -> torch.Tensor:
+    dev = codes.device
+    ctx = ctx or _lib.default_context(dev.index or 0)
+    if out is None:
+        out = torch.empty(tuple(shape), dtype=dtype, device=dev)
+    dims = (ctypes.c_size_t * len(shape))(*shape)
+    codes = codes.contiguous()
+    unpred = unpred.contiguous()
+    _lib.check(_lib.lib().falcons_interp_decompress(ctx.ptr, _dtype_code(out), dims, len(shape),
+                                                    ctypes.byref(params), ctypes.c_void_p(codes.data_ptr()),
+                                                    ctypes.c_size_t(codes.numel()),
+                                                    ctypes.c_void_p(unpred.data_ptr()),
+                                                    ctypes.c_size_t(unpred.numel()), ctypes.c_void_p(out.data_ptr()),
+                                                    _stream_ptr(stream)), "interp_decompress")
+    return out
+
+
+def encode_codes(codes: torch.Tensor, ctx=None, stream=None) -> torch.Tensor:
+    """RleFseEncoder-format entropy coding of int16 codes on the device; returns a uint8 tensor."""
+    assert codes.dtype == torch.int16 and codes.is_cuda
+    ctx = ctx or _lib.default_context(codes.device.index or 0)
+    codes = codes.contiguous()
+    cap = 4 * codes.numel() + (1 << 20)
+    out = torch.empty(cap, dtype=torch.uint8, device=codes.device)
+    n = ctypes.c_size_t(0)
+    _lib.check(_lib.lib().falcons_encode_codes(ctx.ptr, ctypes.c_void_p(codes.data_ptr()),
+                                               ctypes.c_size_t(codes.numel()), ctypes.c_void_p(out.data_ptr()),
+                                               ctypes.c_size_t(cap), ctypes.byref(n), _stream_ptr(stream)),
+               "encode_codes")
+    return out[:n.value]
+
+
+def decode_codes(payload: torch.Tensor, n: int, ctx=None, stream=None) -> torch.Tensor:
+    assert payload.dtype == torch.uint8 and payload.is_cuda
+    ctx = ctx or _lib.default_context(payload.device.index or 0)
+    payload = payload.contiguous()
+    out = torch.empty(max(n, 1), dtype=torch.int16, device=payload.device)
+    _lib.check(_lib.lib().falcons_decode_codes(ctx.ptr, ctypes.c_void_p(payload.data_ptr()),
+                                               ctypes.c_size_t(payload.numel()), ctypes.c_size_t(n),
+                                               ctypes.c_void_p(out.data_ptr()), _stream_ptr(stream)), "decode_codes")
+    return out[:n]

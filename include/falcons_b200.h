@@ -1,0 +1,123 @@
+/*
+ * falcons_b200.h — C ABI of the B200-native Falcons compression path (libfalcons_b200.so).
+ *
+ * Plain pointers and sizes only.  Host pointers are ordinary (pageable or pinned) memory;
+ * device pointers are CUDA global memory on the context's device.  `stream` is a cudaStream_t
+ * passed as void* (NULL = the context's private stream).  Every function returns a status
+ * (FALCONS_OK = 0) and leaves a message for falcons_last_error() on failure.  Status codes map
+ * onto the reference's exception types in include/Falcons/api/falcons.hpp:
+ *   FALCONS_EINVAL  -> std::invalid_argument
+ *   FALCONS_ELENGTH -> std::length_error
+ *   FALCONS_ERUNTIME, FALCONS_ECUDA, FALCONS_ENOMEM -> std::runtime_error
+ *
+ * Reference interfaces each entry point replaces (JLiu-1/Falcons, include/Falcons/...):
+ *   falcons_compress             api/falcons.hpp:54      Falcons_compress<T>(conf, data, cmpData, cmpCap)
+ *   falcons_compress_size_bound  api/impl/FalconsImpl.hpp:44  Falcons_compress_size_bound<T>(conf)
+ *   falcons_read_config          api/falcons.hpp:122     Falcons_read_config(conf, cmpData, cmpSize)
+ *   falcons_decompress           api/falcons.hpp:158,184 Falcons_decompress<T>(conf, cmpData, cmpSize, decData[, cap])
+ *   falcons_compress_device      api/falcons.hpp:54      same, with the field already in device memory
+ *   falcons_decompress_device    api/falcons.hpp:158     same, reconstructing into device memory
+ *   falcons_interp_compress      decomposition/InterpolationDecomposition.hpp:131  compress() -> codes, unpred
+ *   falcons_interp_decompress    decomposition/InterpolationDecomposition.hpp:48   decompress()
+ *   falcons_device_range         utils/Statistic.hpp:160  data_range()
+ *   falcons_encode_codes         encoder/RleFseEncoder.hpp:850-982,1072  preprocess_encode + save + encode
+ *   falcons_decode_codes         encoder/RleFseEncoder.hpp:984-1079      load + decode
+ */
+#ifndef FALCONS_B200_H
+#define FALCONS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    FALCONS_OK = 0,
+    FALCONS_EINVAL = 1,
+    FALCONS_ELENGTH = 2,
+    FALCONS_ERUNTIME = 3,
+    FALCONS_ECUDA = 4,
+    FALCONS_ENOMEM = 5
+};
+
+enum { FALCONS_DTYPE_F32 = 0, FALCONS_DTYPE_F64 = 1 };
+
+typedef struct falcons_ctx falcons_ctx;
+
+/* Parameters of the interpolation decomposition (InterpolationDecomposition.hpp:131-146). */
+typedef struct {
+    double eb;               /* absolute error bound, already resolved */
+    int32_t interp_algo;     /* 0 linear, 1 cubic (Config::interpAlgo) */
+    int32_t direction;       /* Config::interpDirection: 0 or N!-1 */
+    int64_t anchor_stride;   /* Config::interpAnchorStride, resolved (>= 0, power of two) */
+    double alpha;            /* Config::interpAlpha */
+    double beta;             /* Config::interpBeta */
+    int32_t radius;          /* Config::quantbinCnt / 2 */
+    int32_t tuning;          /* 1: the auto-tuner's trial sweeps (TUNING::ENABLED), N >= 3 */
+} falcons_interp_params;
+
+/* The fields of Falcons::Config (utils/Config.hpp:482-511) that the path reads or writes. */
+typedef struct {
+    int32_t N;
+    uint64_t dims[4];        /* slowest first, C order */
+    uint64_t num;
+    int32_t cmprAlgo;        /* ALGO_LORENZO_REG=0, ALGO_INTERP_LORENZO=1, ALGO_INTERP=2, ALGO_NOPRED=3, ALGO_LOSSLESS=4 */
+    int32_t errorBoundMode;  /* EB_ABS=0, EB_REL, EB_PSNR, EB_L2NORM, EB_ABS_AND_REL, EB_ABS_OR_REL */
+    double absErrorBound;
+    double relErrorBound;
+    double psnrErrorBound;
+    double l2normErrorBound;
+    int32_t lorenzo, lorenzo2, regression, regression2, openmp;
+    int32_t quantbinCnt;
+    int32_t blockSize;
+    int32_t predDim;
+    int32_t dataType;
+    int32_t interpAlgo;
+    int32_t interpDirection;
+    int32_t interpAnchorStride;  /* -1: default {4096, 128, 32, 16}[N-1] */
+    double interpAlpha;
+    double interpBeta;
+} falcons_config;
+
+/* falcons_compress flags */
+#define FALCONS_FLAG_WRITEBACK 1u  /* copy the partially reconstructed field back into the caller's
+                                      buffer, as the reference's in-place compressor leaves it */
+
+/* ---- context ---- */
+int falcons_ctx_create(falcons_ctx **out, int device);
+int falcons_ctx_destroy(falcons_ctx *ctx);
+const char *falcons_last_error(void);
+const char *falcons_version(void);
+
+/* ---- drop-in API (host buffers) ---- */
+size_t falcons_compress_size_bound(int dtype, const falcons_config *conf);
+int falcons_compress(falcons_ctx *ctx, int dtype, const falcons_config *conf, void *data, uint32_t flags,
+                     void *out, size_t cap, size_t *out_len, falcons_config *conf_out);
+int falcons_read_config(const void *stream_bytes, size_t len, falcons_config *conf_out);
+int falcons_decompress(falcons_ctx *ctx, int dtype, const void *stream_bytes, size_t len, void *out,
+                       size_t cap_elems, falcons_config *conf_out);
+
+/* ---- device-resident variants (field in HBM; compressed stream in host or device memory) ---- */
+int falcons_compress_device(falcons_ctx *ctx, int dtype, const falcons_config *conf, void *d_data,
+                            void *d_out, size_t cap, size_t *out_len, falcons_config *conf_out, void *stream);
+int falcons_decompress_device(falcons_ctx *ctx, int dtype, const void *d_stream, size_t len, void *d_out,
+                              size_t cap_elems, falcons_config *conf_out, void *stream);
+
+/* ---- stage-level entry points (device pointers) ---- */
+int falcons_interp_compress(falcons_ctx *ctx, int dtype, const size_t *dims, int N, const falcons_interp_params *p,
+                            void *d_data, int16_t *d_codes, void *d_unpred, size_t *n_codes, size_t *n_unpred,
+                            void *stream);
+int falcons_interp_decompress(falcons_ctx *ctx, int dtype, const size_t *dims, int N,
+                              const falcons_interp_params *p, const int16_t *d_codes, size_t n_codes,
+                              const void *d_unpred, size_t n_unpred, void *d_out, void *stream);
+int falcons_device_range(falcons_ctx *ctx, int dtype, const void *d_data, size_t n, double *range_out, void *stream);
+int falcons_encode_codes(falcons_ctx *ctx, const int16_t *d_codes, size_t n, void *d_out, size_t cap,
+                         size_t *out_len, void *stream);
+int falcons_decode_codes(falcons_ctx *ctx, const void *d_in, size_t len, size_t n, int16_t *d_codes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FALCONS_B200_H */
