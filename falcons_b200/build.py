@@ -20,14 +20,14 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-fmad=false",
 
 
 def sources():
-    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def _needs(obj, src):
     if not os.path.exists(obj):
         return True
     t = os.path.getmtime(obj)
-    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
+    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h", ".hpp"))]
     deps.append(os.path.join(HERE, "..", "include", "falcons_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -38,7 +38,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     todo = []
     for s in sources():
         src = os.path.join(CSRC, s)
-        obj = os.path.join(OBJ, s.replace(".cu", ".o"))
+        obj = os.path.join(OBJ, os.path.splitext(s)[0] + ".o")
         objs.append(obj)
         if _needs(obj, src):
             todo.append((src, obj))
@@ -57,7 +57,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         list(ex.map(compile_one, todo))
     if todo or not os.path.exists(LIB):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -1,0 +1,181 @@
+#include "assemble.cuh"
+
+namespace fb2 {
+
+Pool::Pool(cudaStream_t s) : st(s) {
+    static bool configured = false;
+    if (!configured) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaMemPool_t mp;
+        if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+            uint64_t thr = ~0ULL;  // keep freed blocks for reuse by the next call
+            cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        configured = true;
+    }
+}
+
+Pool::~Pool() {
+    for (void *p : ptrs) cudaFreeAsync(p, st);
+}
+
+namespace {
+__global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__restrict__ out) {
+    for (int p = blockIdx.x; p < np; p += gridDim.x) {
+        const Piece pc = pieces[p];
+        const uint8_t *s = pc.src;
+        uint8_t *d = out + pc.dst;
+        if ((((uintptr_t)s ^ (uintptr_t)d) & 15) == 0) {
+            unsigned long long head = (16 - ((uintptr_t)s & 15)) & 15;
+            if (head > pc.len) head = pc.len;
+            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
+            const unsigned long long nv = (pc.len - head) / 16;
+            const int4 *sv = reinterpret_cast<const int4 *>(s + head);
+            int4 *dv = reinterpret_cast<int4 *>(d + head);
+            for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
+            for (unsigned long long i = head + nv * 16 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
+        } else if ((((uintptr_t)s ^ (uintptr_t)d) & 3) == 0) {
+            unsigned long long head = (4 - ((uintptr_t)s & 3)) & 3;
+            if (head > pc.len) head = pc.len;
+            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
+            const unsigned long long nv = (pc.len - head) / 4;
+            const uint32_t *sv = reinterpret_cast<const uint32_t *>(s + head);
+            uint32_t *dv = reinterpret_cast<uint32_t *>(d + head);
+            for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
+            for (unsigned long long i = head + nv * 4 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
+        } else {
+            // misaligned: aligned 4-byte destination words assembled from a funnel of source words
+            unsigned long long head = (4 - ((uintptr_t)d & 3)) & 3;
+            if (head > pc.len) head = pc.len;
+            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
+            const uint8_t *s2 = s + head;
+            uint32_t *dw = reinterpret_cast<uint32_t *>(d + head);
+            const unsigned long long nw = (pc.len - head) / 4;
+            const int sh = (int)((uintptr_t)s2 & 3);
+            const uint32_t *sw = reinterpret_cast<const uint32_t *>(s2 - sh);
+            for (unsigned long long i = threadIdx.x; i < nw; i += blockDim.x) {
+                const uint32_t lo = sw[i], hi = sw[i + 1];
+                dw[i] = __funnelshift_r(lo, hi, 8 * sh);
+            }
+            for (unsigned long long i = head + nw * 4 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
+        }
+    }
+}
+}  // namespace
+
+void launch_gather(Pool &pool, const std::vector<Piece> &pieces, uint8_t *d_out, cudaStream_t st) {
+    if (pieces.empty()) return;
+    Piece *dp = h2d(pool, pieces, st);
+    k_gather<<<(unsigned)std::min<size_t>(pieces.size(), 65535), 256, 0, st>>>(dp, (int)pieces.size(), d_out);
+    FB2_CHECK_LAUNCH();
+}
+
+size_t zstd_raw_frame_header(uint8_t *out, size_t content) {
+    // Frame_Header_Descriptor: Single_Segment_flag (bit 5) with the smallest Frame_Content_Size field.
+    int fcs_flag, fcs_bytes;
+    if (content < 256) { fcs_flag = 0; fcs_bytes = 1; }
+    else if (content < 65536 + 256) { fcs_flag = 1; fcs_bytes = 2; }
+    else if (content <= 0xFFFFFFFFull) { fcs_flag = 2; fcs_bytes = 4; }
+    else { fcs_flag = 3; fcs_bytes = 8; }
+    size_t p = 0;
+    const uint32_t magic = kZstdMagic;
+    memcpy(out + p, &magic, 4);
+    p += 4;
+    out[p++] = (uint8_t)((fcs_flag << 6) | (1 << 5));
+    uint64_t v = (fcs_flag == 1) ? (uint64_t)content - 256 : (uint64_t)content;
+    for (int i = 0; i < fcs_bytes; i++) out[p++] = (uint8_t)(v >> (8 * i));
+    return p;
+}
+
+size_t zstd_raw_frame_size(size_t content) {
+    uint8_t tmp[16];
+    const size_t hdr = zstd_raw_frame_header(tmp, content);
+    const size_t blocks = content == 0 ? 1 : (content + kZstdBlock - 1) / kZstdBlock;
+    return hdr + blocks * 3 + content;
+}
+
+void Assembler::run(Pool &pool, uint8_t *d_out, cudaStream_t st) {
+    if (pieces.empty()) return;
+    uint8_t *dh = h2d(pool, host, st);
+    std::vector<Piece> p = pieces;
+    for (auto &r : host_refs) p[r.first].src = dh + r.second;
+    launch_gather(pool, p, d_out, st);
+    FB2_CUDA(cudaStreamSynchronize(st));  // the host vectors must outlive the async copies
+}
+
+size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
+    const size_t L = pos;
+    std::vector<uint8_t> hb = host;  // extra host bytes: length word, frame header, block headers
+    std::vector<Piece> out;
+    auto add_host = [&](const uint8_t *b, size_t n, unsigned long long dst) {
+        const size_t off = hb.size();
+        hb.insert(hb.end(), b, b + n);
+        out.push_back(Piece{reinterpret_cast<const uint8_t *>(off), dst, n});  // patched below
+    };
+    std::vector<size_t> host_pieces;  // indices into `out` whose src is a host offset
+    uint8_t tmp[16];
+    const uint64_t L64 = L;
+    host_pieces.push_back(out.size());
+    add_host(reinterpret_cast<const uint8_t *>(&L64), 8, 0);
+    const size_t fh = zstd_raw_frame_header(tmp, L);
+    host_pieces.push_back(out.size());
+    add_host(tmp, fh, 8);
+    const size_t base = 8 + fh;
+    const size_t nblocks = L == 0 ? 1 : (L + kZstdBlock - 1) / kZstdBlock;
+    for (size_t b = 0; b < nblocks; b++) {
+        const size_t bs = std::min(kZstdBlock, L - b * kZstdBlock);
+        const uint32_t h = (uint32_t)((b + 1 == nblocks) ? 1 : 0) | (0u << 1) | ((uint32_t)bs << 3);
+        uint8_t hh[3] = {(uint8_t)h, (uint8_t)(h >> 8), (uint8_t)(h >> 16)};
+        host_pieces.push_back(out.size());
+        add_host(hh, 3, base + b * (kZstdBlock + 3));
+    }
+    // logical pieces split at block boundaries
+    std::vector<bool> is_host(pieces.size(), false);
+    std::vector<size_t> host_off(pieces.size(), 0);
+    for (auto &r : host_refs) {
+        is_host[r.first] = true;
+        host_off[r.first] = r.second;
+    }
+    for (size_t i = 0; i < pieces.size(); i++) {
+        const Piece &pc = pieces[i];
+        unsigned long long x = pc.dst, rem = pc.len, so = 0;
+        while (rem) {
+            const unsigned long long in_blk = kZstdBlock - x % kZstdBlock;
+            const unsigned long long c = std::min(rem, in_blk);
+            const unsigned long long phys = base + (x / kZstdBlock) * (kZstdBlock + 3) + 3 + (x % kZstdBlock);
+            if (is_host[i]) {
+                host_pieces.push_back(out.size());
+                out.push_back(Piece{reinterpret_cast<const uint8_t *>(host_off[i] + so), phys, c});
+            } else {
+                out.push_back(Piece{pc.src + so, phys, c});
+            }
+            x += c;
+            so += c;
+            rem -= c;
+        }
+    }
+    uint8_t *dh = h2d(pool, hb, st);
+    for (size_t i : host_pieces) out[i].src = dh + reinterpret_cast<uintptr_t>(out[i].src);
+    launch_gather(pool, out, d_out, st);
+    FB2_CUDA(cudaStreamSynchronize(st));
+    return 8 + zstd_raw_frame_size(L);
+}
+
+void logical_pieces(const uint8_t *d_base, bool framed, size_t off, size_t n, unsigned long long dst,
+                    std::vector<Piece> &out) {
+    if (!framed) {
+        if (n) out.push_back(Piece{d_base + off, dst, n});
+        return;
+    }
+    while (n) {
+        const size_t c = std::min(n, kZstdBlock - off % kZstdBlock);
+        const size_t phys = (off / kZstdBlock) * (kZstdBlock + 3) + 3 + (off % kZstdBlock);
+        out.push_back(Piece{d_base + phys, dst, c});
+        off += c;
+        dst += c;
+        n -= c;
+    }
+}
+
+}  // namespace fb2

@@ -1,0 +1,152 @@
+// Stream assembly helpers shared by the entropy stage and the pipeline:
+//   Pool       stream-ordered device scratch (cudaMallocAsync on the default pool, retained)
+//   Assembler  a list of byte pieces (device or host-built) laid out back to back and copied into
+//              place by one gather kernel; optionally framed as a Zstandard frame of raw blocks
+//              (RFC 8878 section 3.1: magic, frame header with content size, 3-byte block headers)
+//   ByteView   logical read access to a byte range that may sit inside such a raw-block frame
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "common.cuh"
+
+namespace fb2 {
+
+constexpr size_t kZstdBlock = 128 * 1024;   // Block_Maximum_Size
+constexpr uint32_t kZstdMagic = 0xFD2FB528u;
+
+struct Pool {
+    cudaStream_t st;
+    std::vector<void *> ptrs;
+    explicit Pool(cudaStream_t s);
+    template <class T>
+    T *get(size_t count) {
+        void *p = nullptr;
+        FB2_CUDA(cudaMallocAsync(&p, std::max<size_t>(count * sizeof(T), 16) + 64, st));
+        ptrs.push_back(p);
+        return static_cast<T *>(p);
+    }
+    ~Pool();
+};
+
+template <class T>
+std::vector<T> d2h(const T *d, size_t n, cudaStream_t st) {
+    std::vector<T> h(n);
+    if (n) {
+        FB2_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+    }
+    return h;
+}
+
+template <class T>
+T *h2d(Pool &pool, const std::vector<T> &h, cudaStream_t st) {
+    T *d = pool.get<T>(h.size());
+    if (!h.empty()) FB2_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return d;
+}
+
+inline unsigned grid_for(long long n, int threads, long long cap = 1 << 20) {
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, cap));
+}
+
+struct Piece {
+    const uint8_t *src;
+    unsigned long long dst;
+    unsigned long long len;
+};
+
+// Copies every piece to out + dst (one CTA per piece, 16-byte vectors when src and dst line up).
+void launch_gather(Pool &pool, const std::vector<Piece> &pieces, uint8_t *d_out, cudaStream_t st);
+
+// Size of a raw-block zstd frame holding `content` bytes.
+size_t zstd_raw_frame_size(size_t content);
+// Frame header bytes (magic + descriptor + content size); returns its length.
+size_t zstd_raw_frame_header(uint8_t *out, size_t content);
+
+struct Assembler {
+    std::vector<Piece> pieces;                         // logical layout
+    std::vector<uint8_t> host;                         // host-built bytes
+    std::vector<std::pair<size_t, size_t>> host_refs;  // (piece index, host offset)
+    unsigned long long pos = 0;
+    void dev(const void *src, size_t len) {
+        if (!len) return;
+        pieces.push_back(Piece{static_cast<const uint8_t *>(src), pos, len});
+        pos += len;
+    }
+    void bytes(const void *p, size_t len) {
+        if (!len) return;
+        const size_t off = host.size();
+        host.insert(host.end(), static_cast<const uint8_t *>(p), static_cast<const uint8_t *>(p) + len);
+        host_refs.push_back({pieces.size(), off});
+        pieces.push_back(Piece{nullptr, pos, len});
+        pos += len;
+    }
+    template <class T>
+    void val(T v) {
+        bytes(&v, sizeof(T));
+    }
+    // Copies the logical layout to d_out[0, pos).  Synchronizes the stream.
+    void run(Pool &pool, uint8_t *d_out, cudaStream_t st);
+    // Writes [u64 pos][zstd raw-block frame of the layout] to d_out; returns the bytes written.
+    size_t run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st);
+    size_t framed_size() const { return 8 + zstd_raw_frame_size(pos); }
+};
+
+// Logical bytes [0, len) stored either flat or as the content of a raw-block zstd frame.
+struct ByteView {
+    const uint8_t *base = nullptr;   // host pointer (flat bytes or the frame's first block header)
+    size_t len = 0;                  // logical length (from origin)
+    bool framed = false;
+    size_t origin = 0;               // logical offset of index 0
+    size_t phys(size_t i) const {
+        i += origin;
+        return framed ? (i / kZstdBlock) * (kZstdBlock + 3) + 3 + (i % kZstdBlock) : i;
+    }
+    ByteView sub(size_t off) const {
+        if (off > len) throw std::invalid_argument("Invalid or truncated Falcons payload");
+        ByteView v = *this;
+        v.origin += off;
+        v.len -= off;
+        return v;
+    }
+    uint8_t at(size_t i) const {
+        if (i >= len) throw std::invalid_argument("Invalid or truncated Falcons payload");
+        return base[phys(i)];
+    }
+    void read(void *dst, size_t off, size_t n) const {
+        if (off + n > len || off + n < off) throw std::invalid_argument("Invalid or truncated Falcons payload");
+        uint8_t *d = static_cast<uint8_t *>(dst);
+        if (!framed) {
+            memcpy(d, base + origin + off, n);
+            return;
+        }
+        while (n) {
+            const size_t in_blk = kZstdBlock - (origin + off) % kZstdBlock;
+            const size_t c = std::min(n, in_blk);
+            memcpy(d, base + phys(off), c);
+            d += c;
+            off += c;
+            n -= c;
+        }
+    }
+    template <class T>
+    T rd(size_t &off) const {
+        T v;
+        read(&v, off, sizeof(T));
+        off += sizeof(T);
+        return v;
+    }
+};
+
+// Device counterpart: pieces that move logical [off, off+n) of a (possibly framed) device buffer
+// to dst (flat).  Returns the pieces (the caller launches the gather).
+void logical_pieces(const uint8_t *d_base, bool framed, size_t off, size_t n, unsigned long long dst,
+                    std::vector<Piece> &out);
+
+}  // namespace fb2

@@ -14,6 +14,7 @@
 #include <stdexcept>
 #include <vector>
 
+#include "assemble.cuh"
 #include "entropy.cuh"
 #include "fse.cuh"
 #include "scan.cuh"
@@ -48,119 +49,6 @@ __host__ __device__ __forceinline__ int o1_sym(int code) {
 __host__ __device__ __forceinline__ int unzz(uint32_t z) { return (int)((z >> 1) ^ (~(z & 1) + 1)); }
 
 __host__ __device__ __forceinline__ uint32_t zigzag(int v) { return ((uint32_t)v << 1) ^ (uint32_t)(v >> 31); }
-
-// ------------------------------------------------------------------ scratch (stream-ordered pool)
-struct Pool {
-    cudaStream_t st;
-    std::vector<void *> ptrs;
-    explicit Pool(cudaStream_t s) : st(s) {
-        static bool configured = false;
-        if (!configured) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaMemPool_t mp;
-            if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
-                uint64_t thr = ~0ULL;
-                cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
-            }
-            configured = true;
-        }
-    }
-    template <class T>
-    T *get(size_t count) {
-        void *p = nullptr;
-        FB2_CUDA(cudaMallocAsync(&p, std::max<size_t>(count * sizeof(T), 16) + 64, st));
-        ptrs.push_back(p);
-        return static_cast<T *>(p);
-    }
-    ~Pool() {
-        for (void *p : ptrs) cudaFreeAsync(p, st);
-    }
-};
-
-template <class T>
-std::vector<T> d2h(const T *d, size_t n, cudaStream_t st) {
-    std::vector<T> h(n);
-    if (n) {
-        FB2_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaStreamSynchronize(st));
-    }
-    return h;
-}
-
-template <class T>
-T *h2d(Pool &pool, const std::vector<T> &h, cudaStream_t st) {
-    T *d = pool.get<T>(h.size());
-    if (!h.empty()) FB2_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-    return d;
-}
-
-inline unsigned grid_for(long long n, int threads, long long cap = 1 << 20) {
-    return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, cap));
-}
-
-// ------------------------------------------------------------------ gather (stream assembly)
-struct Piece {
-    const uint8_t *src;
-    unsigned long long dst;
-    unsigned long long len;
-};
-
-__global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__restrict__ out) {
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
-        const Piece pc = pieces[p];
-        const uint8_t *s = pc.src;
-        uint8_t *d = out + pc.dst;
-        // 16-byte vector copy when both ends line up
-        if ((((uintptr_t)s ^ (uintptr_t)d) & 15) == 0) {
-            unsigned long long head = (16 - ((uintptr_t)s & 15)) & 15;
-            if (head > pc.len) head = pc.len;
-            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
-            const unsigned long long nv = (pc.len - head) / 16;
-            const int4 *sv = reinterpret_cast<const int4 *>(s + head);
-            int4 *dv = reinterpret_cast<int4 *>(d + head);
-            for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
-            for (unsigned long long i = head + nv * 16 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
-        } else {
-            for (unsigned long long i = threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
-        }
-    }
-}
-
-struct Assembler {
-    std::vector<Piece> pieces;
-    std::vector<uint8_t> host;               // host-built bytes (headers)
-    std::vector<std::pair<size_t, size_t>> host_refs;  // (piece index, host offset)
-    unsigned long long pos = 0;
-    void dev(const void *src, size_t len) {
-        if (!len) return;
-        pieces.push_back(Piece{static_cast<const uint8_t *>(src), pos, len});
-        pos += len;
-    }
-    void bytes(const void *p, size_t len) {
-        if (!len) return;
-        const size_t off = host.size();
-        host.insert(host.end(), static_cast<const uint8_t *>(p), static_cast<const uint8_t *>(p) + len);
-        host_refs.push_back({pieces.size(), off});
-        pieces.push_back(Piece{nullptr, pos, len});
-        pos += len;
-    }
-    template <class T>
-    void val(T v) {
-        bytes(&v, sizeof(T));
-    }
-    // Launches the copies into d_out (capacity checked by the caller).
-    void run(Pool &pool, uint8_t *d_out, cudaStream_t st) {
-        if (pieces.empty()) return;
-        uint8_t *dh = h2d(pool, host, st);
-        for (auto &r : host_refs) pieces[r.first].src = dh + r.second;
-        Piece *dp = h2d(pool, pieces, st);
-        k_gather<<<(unsigned)std::min<size_t>(pieces.size(), 65535), 256, 0, st>>>(dp, (int)pieces.size(), d_out);
-        FB2_CHECK_LAUNCH();
-        // the host vectors must outlive the async copies
-        FB2_CUDA(cudaStreamSynchronize(st));
-    }
-};
 
 // ------------------------------------------------------------------ FSE class blocks
 struct BlockJob {
@@ -231,13 +119,14 @@ __global__ void __launch_bounds__(128) k_fse_decode_blocks(const uint8_t *__rest
 }
 
 // Walks an fse_enc record sequence (host bytes) for n symbols starting at `off`; appends jobs.
-size_t parse_blocks(const uint8_t *h, size_t len, size_t off, unsigned long long n, unsigned long long dst_base,
+size_t parse_blocks(const ByteView &h, size_t off, unsigned long long n, unsigned long long dst_base,
                     std::vector<BlockJob> &jobs) {
+    const size_t len = h.len;
     unsigned long long done = 0;
     while (done < n) {
         const unsigned bn = (unsigned)std::min<unsigned long long>(n - done, FBLK);
         if (off >= len) throw std::invalid_argument("truncated FSE block stream");
-        const uint8_t flag = h[off++];
+        const uint8_t flag = h.at(off++);
         BlockJob j{dst_base + done, bn, flag, 0, 0};
         if (flag == 0) {
             if (off + bn > len) throw std::invalid_argument("truncated raw block");
@@ -251,9 +140,7 @@ size_t parse_blocks(const uint8_t *h, size_t len, size_t off, unsigned long long
             off += 1;
         } else if (flag == 1) {
             if (off + 4 > len) throw std::invalid_argument("truncated FSE block header");
-            uint32_t rr;
-            memcpy(&rr, h + off, 4);
-            off += 4;
+            const uint32_t rr = h.rd<uint32_t>(off);
             if (off + rr > len || bn < 3) throw std::invalid_argument("truncated FSE block");
             j.in = off;
             j.inlen = rr;
@@ -822,7 +709,7 @@ __global__ void k_sample_windows(const int16_t *__restrict__ q, const unsigned l
 
 // Decodes gamma groups whose class streams are fse_enc records in host-visible bytes `h`
 // (also present on the device at `d`).  vals must hold the group totals.
-void gamma_decode(Pool &pool, const uint8_t *d, const uint8_t *h, size_t len,
+void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
                   const std::vector<size_t> &cls_off, const std::vector<size_t> &man_off,
                   const std::vector<size_t> &man_len, const std::vector<unsigned long long> &gstart,
                   uint32_t *d_vals, int *d_err, cudaStream_t st) {
@@ -830,7 +717,7 @@ void gamma_decode(Pool &pool, const uint8_t *d, const uint8_t *h, size_t len,
     const long long T = (long long)gstart.back();
     if (T == 0) return;
     std::vector<BlockJob> jobs;
-    for (int g = 0; g < G; g++) parse_blocks(h, len, cls_off[g], gstart[g + 1] - gstart[g], gstart[g], jobs);
+    for (int g = 0; g < G; g++) parse_blocks(h, cls_off[g], gstart[g + 1] - gstart[g], gstart[g], jobs);
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
     k_fse_decode_blocks<<<(unsigned)jobs.size(), 128, 0, st>>>(d, dj, cls, d_err);
@@ -857,14 +744,6 @@ __global__ void k_ovf_convert(const uint32_t *gv, const unsigned long long *src,
             out[dst[g] + i] = (int16_t)unzz(gv[src[g] + i] - 1u);
 }
 
-template <class T>
-T rd(const uint8_t *h, size_t len, size_t &off) {
-    if (off + sizeof(T) > len) throw std::invalid_argument("truncated entropy stream");
-    T v;
-    memcpy(&v, h + off, sizeof(T));
-    off += sizeof(T);
-    return v;
-}
 
 }  // namespace
 
@@ -915,10 +794,8 @@ EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cud
     return ch;
 }
 
-size_t entropy_encode(Context &ctx, const int16_t *d_codes_in, size_t n, const EntropyChoice &ch, uint8_t *d_out,
-                      size_t cap, cudaStream_t st, const EntropyTuning &tune) {
-    (void)ctx;
-    Pool pool(st);
+void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, size_t n, const EntropyChoice &ch,
+                         cudaStream_t st, const EntropyTuning &tune) {
     const long long N = (long long)n;
     const int16_t *q = d_codes_in;
     if (ch.delta && N > 0) {
@@ -927,7 +804,6 @@ size_t entropy_encode(Context &ctx, const int16_t *d_codes_in, size_t n, const E
         FB2_CHECK_LAUNCH();
         q = dq;
     }
-    Assembler as;
     const uint8_t mb = (uint8_t)(ch.method | (ch.delta ? 0x80 : 0));
     as.val<uint8_t>(mb);
     as.val<uint16_t>(0);  // lo_
@@ -1082,39 +958,43 @@ size_t entropy_encode(Context &ctx, const int16_t *d_codes_in, size_t n, const E
             }
         }
     }
+}
+
+size_t entropy_encode(Context &ctx, const int16_t *d_codes, size_t n, const EntropyChoice &ch, uint8_t *d_out,
+                      size_t cap, cudaStream_t st, const EntropyTuning &tune) {
+    (void)ctx;
+    Pool pool(st);
+    Assembler as;
+    entropy_encode_into(pool, as, d_codes, n, ch, st, tune);
     if (as.pos > cap) throw std::length_error("The buffer for compressed data is not large enough.");
     as.run(pool, d_out, st);
     return (size_t)as.pos;
 }
 
-size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, size_t len, size_t n, int16_t *d_codes,
+size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size_t n, int16_t *d_codes,
                       cudaStream_t st) {
     (void)ctx;
     Pool pool(st);
-    std::vector<uint8_t> hcopy;
-    if (!h_in) {
-        hcopy = d2h(d_in, len, st);
-        h_in = hcopy.data();
-    }
+    const size_t len = h.len;
     size_t off = 0;
-    const uint8_t mb = rd<uint8_t>(h_in, len, off);
-    rd<uint16_t>(h_in, len, off);
-    rd<uint16_t>(h_in, len, off);
+    const uint8_t mb = h.rd<uint8_t>(off);
+    h.rd<uint16_t>(off);
+    h.rd<uint16_t>(off);
     const bool delta = (mb & 0x80) != 0;
     const int method = mb & 0x7F;
     const long long N = (long long)n;
     int *d_err = pool.get<int>(4);
     FB2_CUDA(cudaMemsetAsync(d_err, 0, 16, st));
     if (method == 0) {
-        const unsigned long long nr = rd<uint64_t>(h_in, len, off), nv = rd<uint64_t>(h_in, len, off);
-        const unsigned long long s_rcl = rd<uint64_t>(h_in, len, off), s_vcl = rd<uint64_t>(h_in, len, off);
-        const unsigned long long rbp = rd<uint64_t>(h_in, len, off), vbp = rd<uint64_t>(h_in, len, off);
+        const unsigned long long nr = h.rd<uint64_t>(off), nv = h.rd<uint64_t>(off);
+        const unsigned long long s_rcl = h.rd<uint64_t>(off), s_vcl = h.rd<uint64_t>(off);
+        const unsigned long long rbp = h.rd<uint64_t>(off), vbp = h.rd<uint64_t>(off);
         const size_t o_rcl = off, o_vcl = o_rcl + s_rcl, o_rman = o_vcl + s_vcl, o_vman = o_rman + rbp;
         const size_t end = o_vman + vbp;
         if (end > len || nv > (unsigned long long)N || nr > (unsigned long long)N + 1)
             throw std::invalid_argument("Invalid or truncated Falcons entropy payload");
         uint32_t *buf = pool.get<uint32_t>(nr + nv + 2);
-        gamma_decode(pool, d_in, h_in, len, {o_rcl, o_vcl}, {o_rman, o_vman}, {(size_t)rbp, (size_t)vbp},
+        gamma_decode(pool, d_in, h, {o_rcl, o_vcl}, {o_rman, o_vman}, {(size_t)rbp, (size_t)vbp},
                      {0ULL, nr, nr + nv}, buf, d_err, st);
         FB2_CUDA(cudaMemsetAsync(d_codes, 0, (size_t)N * 2, st));
         if (nv > 0) {
@@ -1127,7 +1007,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
         }
         off = end;
     } else if (method == 1) {
-        unsigned long long S = rd<uint64_t>(h_in, len, off);
+        unsigned long long S = h.rd<uint64_t>(off);
         if (S == 0) S = 1;
         if (S > (unsigned long long)std::max<long long>(N, 1)) throw std::invalid_argument("invalid segment count");
         const unsigned long long seg = ((unsigned long long)N + S - 1) / S;
@@ -1147,14 +1027,14 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
             unsigned long long hi = lo + seg;
             if (hi > (unsigned long long)N) hi = N;
             const unsigned long long ng = hi > lo ? hi - lo : 0;
-            rd<uint64_t>(h_in, len, off);  // stored N (the decoder uses the computed length)
-            const unsigned long long K = rd<uint64_t>(h_in, len, off);
+            h.rd<uint64_t>(off);  // stored N (the decoder uses the computed length)
+            const unsigned long long K = h.rd<uint64_t>(off);
             if (ng == 0) continue;
             if (K < 1 || K > (unsigned long long)kMaxK) throw std::invalid_argument("invalid tANS stream count");
             const unsigned long long cs = (ng + K - 1) / K;
             unsigned long long bl[kMaxK], nk[kMaxK];
-            for (unsigned long long k = 0; k < K; k++) bl[k] = rd<uint64_t>(h_in, len, off);
-            for (unsigned long long k = 0; k < K; k++) nk[k] = rd<uint64_t>(h_in, len, off);
+            for (unsigned long long k = 0; k < K; k++) bl[k] = h.rd<uint64_t>(off);
+            for (unsigned long long k = 0; k < K; k++) nk[k] = h.rd<uint64_t>(off);
             nf_off[g] = off;
             off += O1_NCTX * O1_NSYM * 2;
             unsigned long long sp = off, tot_ov = 0;
@@ -1170,15 +1050,15 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
             off = sp;
             if (off > len) throw std::invalid_argument("Invalid or truncated Falcons entropy payload");
             // escape block (decode_o1_ovf)
-            const uint8_t mode = rd<uint8_t>(h_in, len, off);
+            const uint8_t mode = h.rd<uint8_t>(off);
             if (tot_ov > 0) {
                 if (mode == 0) {
                     if (off + tot_ov * 2 > len) throw std::invalid_argument("truncated escape block");
                     raws.push_back(RawOvf{off, tot_ov, ovf_total});
                     off += tot_ov * 2;
                 } else {
-                    const unsigned long long s_vcl = rd<uint64_t>(h_in, len, off);
-                    const unsigned long long vbp = rd<uint64_t>(h_in, len, off);
+                    const unsigned long long s_vcl = h.rd<uint64_t>(off);
+                    const unsigned long long vbp = h.rd<uint64_t>(off);
                     cls_off.push_back(off);
                     man_off.push_back(off + s_vcl);
                     man_len.push_back(vbp);
@@ -1198,7 +1078,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
         int16_t *ovf = pool.get<int16_t>(ovf_total + 1);
         {
             uint32_t *gv = pool.get<uint32_t>(gstart.back() + 1);
-            gamma_decode(pool, d_in, h_in, len, cls_off, man_off, man_len, gstart, gv, d_err, st);
+            gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, gv, d_err, st);
             // place: raw blocks are copied, gamma groups converted
             std::vector<Piece> pcs;
             size_t gi = 0;
@@ -1213,12 +1093,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
                     gi++;
                 }
             }
-            if (!pcs.empty()) {
-                Piece *dp = h2d(pool, pcs, st);
-                k_gather<<<(unsigned)std::min<size_t>(pcs.size(), 65535), 256, 0, st>>>(dp, (int)pcs.size(),
-                                                                                       reinterpret_cast<uint8_t *>(ovf));
-                FB2_CHECK_LAUNCH();
-            }
+            launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(ovf), st);
             if (!conv_src.empty()) {
                 unsigned long long *d_cs = h2d(pool, conv_src, st), *d_cd = h2d(pool, conv_dst, st),
                                    *d_cn = h2d(pool, conv_n, st);
@@ -1234,10 +1109,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, si
             std::vector<Piece> pcs;
             for (unsigned long long g = 0; g < S; g++)
                 pcs.push_back(Piece{d_in + nf_off[g], g * O1_NCTX * O1_NSYM * 2, O1_NCTX * O1_NSYM * 2});
-            Piece *dp = h2d(pool, pcs, st);
-            k_gather<<<(unsigned)std::min<size_t>(pcs.size(), 65535), 256, 0, st>>>(dp, (int)pcs.size(),
-                                                                                   reinterpret_cast<uint8_t *>(nf));
-            FB2_CHECK_LAUNCH();
+            launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(nf), st);
         }
         fse::DEntry *dt = pool.get<fse::DEntry>((size_t)ntab * O1_M);
         uint8_t *spread = pool.get<uint8_t>((size_t)ntab * O1_M);

@@ -16,6 +16,7 @@
 
 #include <vector>
 
+#include "assemble.cuh"
 #include "context.cuh"
 
 namespace fb2 {
@@ -38,9 +39,14 @@ EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cud
 size_t entropy_encode(Context &ctx, const int16_t *d_codes, size_t n, const EntropyChoice &ch, uint8_t *d_out,
                       size_t cap, cudaStream_t st, const EntropyTuning &tune = EntropyTuning());
 
-// Decodes the encoder header + payload at d_in (device; h_in = optional host copy of the same bytes)
-// into n codes.  Returns the number of bytes consumed.
-size_t entropy_decode(Context &ctx, const uint8_t *d_in, const uint8_t *h_in, size_t len, size_t n, int16_t *d_codes,
+// Appends the encoder header + payload pieces to `as` (pieces reference scratch owned by `pool`).
+void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes, size_t n, const EntropyChoice &ch,
+                         cudaStream_t st, const EntropyTuning &tune = EntropyTuning());
+
+// Decodes the encoder header + payload into n codes.  d_in: the bytes on the device (flat);
+// h: the same bytes readable on the host (used to parse the block structure).  Returns the
+// number of bytes consumed.
+size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size_t n, int16_t *d_codes,
                       cudaStream_t st);
 
 }  // namespace fb2

@@ -200,9 +200,32 @@ struct Builder {
                 st[seq[i - 1]] = s;
                 generic_pass(level, s, seq[i], st);
             }
+        } else if (P.N == 2) {
+            const int d0 = seq[0], d1 = seq[1];
+            legacy_lines(level, s, d0, count_of(P.dims[d1], s2), s2 * P.off[d1]);
+            legacy_lines(level, s, d1, count_of(P.dims[d0], s), s * P.off[d0]);
         } else {
-            throw std::invalid_argument("tuning path for N<=2 is handled by the legacy line launcher");
+            legacy_lines(level, s, 0, 1, 0);
         }
+    }
+
+    // Legacy 1-D routine interpolation_1d (InterpolationDecomposition.hpp:371-419) on A lines.
+    void legacy_lines(int level, long long s, int pd, long long A, long long sa) {
+        const long long n = (P.dims[pd] - 1) / s + 1;
+        if (n <= 1) return;
+        PassLaunch L = blank();
+        L.kind = KIND_LEGACY;
+        L.cubic = prm.cubic != 0;
+        L.n = (int)n;
+        L.step = s * P.off[pd];
+        L.A = A;
+        L.sa = sa;
+        L.B = 1;
+        L.C = n / 2;
+        L.p_base = pos;
+        L.level = level;
+        P.passes.push_back(L);
+        pos += A * (n / 2);
     }
 };
 
@@ -220,7 +243,6 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
     if (p.direction < 0 || p.direction >= fact) throw std::invalid_argument("interpDirection out of range");
     if (!p.tuning && N >= 2 && N <= 3 && p.direction != 0 && p.direction != fact - 1)
         throw std::invalid_argument("interpDirection must be 0 or N!-1 for 2-D and 3-D fields");
-    if (p.tuning && N <= 2) throw std::invalid_argument("device tuning sweeps support N >= 3 only");
 
     InterpPlan P;
     P.N = N;
@@ -341,11 +363,32 @@ __global__ void __launch_bounds__(kPassThreads) k_pass(const PassLaunch L, T *__
                     } else {
                         r = mk_rule(F_LINEAR, t - 1, t + 1);
                     }
-                } else {  // KIND_LEGACY: one fixed target t per line
-                    t = L.g_t0;
+                } else {  // KIND_LEGACY: interpolation_1d on line a; its own visiting order
+                    t = 1 + 2 * (int)c;
                     line = a * L.sa;
-                    p = L.p_base + a;
-                    r = mk_rule(L.g_rule[0], L.g_rule[1], L.g_rule[2], L.g_rule[3], L.g_rule[4]);
+                    const int n = L.n;
+                    int rank = (int)c;
+                    if (!L.cubic || n < 5) {
+                        if (t + 1 < n) r = mk_rule(F_LINEAR, t - 1, t + 1);
+                        else r = n < 4 ? mk_rule(F_EQUAL, n - 2) : mk_rule(F_LINEAR1, n - 4, n - 2);
+                    } else {
+                        const int tf = (n & 1) ? n - 2 : n - 3;  // first odd t with t + 3 >= n
+                        const int mid = (tf - 3) / 2;
+                        if (t == 1) {
+                            r = mk_rule(F_QUAD1, 0, 2, 4);
+                            rank = mid;
+                        } else if (t == tf) {
+                            r = mk_rule(F_QUAD2, t - 3, t - 1, t + 1);
+                            rank = mid + 1;
+                        } else if (t > tf) {
+                            r = mk_rule(F_QUAD3, n - 6, n - 4, n - 2);
+                            rank = mid + 2;
+                        } else {
+                            r = mk_rule(F_CUBIC, t - 3, t - 1, t + 1, t + 3);
+                            rank = (t - 3) / 2;
+                        }
+                    }
+                    p = L.p_base + a * L.C + rank;
                 }
                 const long long st = L.step;
                 // Operands are never written by this launch: read them through the read-only path.

@@ -1,29 +1,392 @@
+// Full compress / decompress pipeline producing and consuming the reference's serial stream.
+//
+// Compress (reference call stack, api/falcons.hpp:54 -> FalconsDispatcher.hpp:16 ->
+// FalconsAlgoInterp.hpp:33 -> FalconsGenericCompressor.hpp:57):
+//   1. error-bound resolution        utils/Statistic.hpp:216-240   (device min/max)
+//   2. algorithm selection / tuning  FalconsAlgoInterp.hpp:273-544 (tuner.cu)
+//   3. interpolation decomposition   InterpolationDecomposition.hpp:131-239 (interp.cu)
+//   4. entropy coding                RleFseEncoder.hpp:850-982 (entropy.cu)
+//   5. trailing zstd stage           Lossless_zstd.hpp:29-46: written here as a zstd frame of raw
+//                                    blocks by the same gather kernel that assembles the payload
+//   6. dispatcher fallbacks          FalconsDispatcher.hpp:100-133 (lossless when the buffer is
+//                                    short or the ratio is below 3 and zstd of the field is smaller)
+//   7. Config header                 utils/Config.hpp:316-360, openmp bit cleared (serial format)
+#include <cmath>
+#include <cstring>
 #include <stdexcept>
+#include <vector>
 
+#include "assemble.cuh"
 #include "entropy.cuh"
+#include "interp.cuh"
 #include "pipeline.cuh"
+#include "stream.hpp"
+#include "tuner.cuh"
 
 namespace fb2 {
-size_t compress_size_bound(int, const falcons_config *) { throw std::runtime_error("not implemented"); }
-void compress_host(Context &, int, const falcons_config *, void *, uint32_t, void *, size_t, size_t *, falcons_config *) {
-    throw std::runtime_error("not implemented");
+
+namespace {
+
+long long default_anchor(int N) {
+    static const long long a[4] = {4096, 128, 32, 16};
+    return a[N - 1];
 }
-void read_config(const void *, size_t, falcons_config *) { throw std::runtime_error("not implemented"); }
-void decompress_host(Context &, int, const void *, size_t, void *, size_t, falcons_config *) {
-    throw std::runtime_error("not implemented");
+
+double psnr_to_abs(double psnr, double threshold, double range) {
+    // utils/Statistic.hpp computeABSErrBoundFromPSNR
+    const double v1 = psnr + 10 * std::log10(1 - 2.0 / 3.0 * threshold);
+    const double v2 = v1 / (-20);
+    const double v3 = std::pow(10, v2);
+    return range * v3;
 }
-void compress_device(Context &, int, const falcons_config *, void *, void *, size_t, size_t *, falcons_config *,
-                     cudaStream_t) {
-    throw std::runtime_error("not implemented");
+
+template <class T>
+double field_range(Context &ctx, const T *d_x, long long n, cudaStream_t st) {
+    Pool pool(st);
+    void *ws = pool.get<uint8_t>(range_workspace_bytes());
+    T *res = pool.get<T>(4);
+    device_range<T>(d_x, n, res, ws, st);
+    std::vector<T> h = d2h(res, 3, st);
+    return (double)h[0];
 }
-void decompress_device(Context &, int, const void *, size_t, void *, size_t, falcons_config *, cudaStream_t) {
-    throw std::runtime_error("not implemented");
+
+// calAbsErrorBound (utils/Statistic.hpp:216-240)
+template <class T>
+void resolve_error_bound(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st) {
+    if (c.errorBoundMode == EB_ABS) return;
+    auto range = [&]() { return field_range<T>(ctx, d_x, (long long)c.num, st); };
+    switch (c.errorBoundMode) {
+        case EB_REL: c.absErrorBound = c.relErrorBound * range(); break;
+        case EB_PSNR: c.absErrorBound = psnr_to_abs(c.psnrErrorBound, 0.99, range()); break;
+        case EB_L2NORM: c.absErrorBound = std::sqrt(3.0 / (double)c.num) * c.l2normErrorBound; break;
+        case EB_ABS_AND_REL: c.absErrorBound = std::min(c.absErrorBound, c.relErrorBound * range()); break;
+        case EB_ABS_OR_REL: c.absErrorBound = std::max(c.absErrorBound, c.relErrorBound * range()); break;
+        default: throw std::invalid_argument("Error bound mode not supported");
+    }
+    c.errorBoundMode = EB_ABS;
 }
+
+InterpParams interp_params_of(const falcons_config &c) {
+    InterpParams p;
+    p.eb = c.absErrorBound;
+    p.cubic = c.interpAlgo;
+    p.direction = c.interpDirection;
+    p.anchor = c.interpAnchorStride;
+    p.alpha = c.interpAlpha;
+    p.beta = c.interpBeta;
+    p.radius = c.quantbinCnt / 2;
+    p.tuning = 0;
+    return p;
+}
+
+struct LossyOut {
+    size_t payload = 0;  // [u64 len][zstd frame] bytes written at d_out
+};
+
+// Lossless-only payload: [u64 len][zstd raw-block frame of the field bytes] (device gather).
+size_t lossless_raw_frame(const void *d_x, size_t bytes, uint8_t *d_out, size_t cap, cudaStream_t st) {
+    Pool pool(st);
+    Assembler as;
+    as.dev(d_x, bytes);
+    const size_t need = as.framed_size();
+    if (need > cap) throw std::length_error("The buffer for compressed data is not large enough.");
+    return as.run_framed(pool, d_out, st);
+}
+
+template <class T>
+size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_t *d_out, size_t cap,
+                     falcons_config *conf_out, cudaStream_t st, const T *h_data) {
+    (void)h_data;
+    falcons_config c = in_conf;
+    normalize_dims(c);
+    c.openmp = 0;  // serial stream format
+    if (c.quantbinCnt <= 0 || c.quantbinCnt > 65536) throw std::invalid_argument("QuantizationBinTotal must be in [2, 65536]");
+    resolve_error_bound<T>(ctx, c, d_x, st);
+    if (c.absErrorBound == 0) c.cmprAlgo = ALGO_LOSSLESS;
+    if (c.cmprAlgo == ALGO_LORENZO_REG || c.cmprAlgo == ALGO_NOPRED)
+        throw std::invalid_argument("unsupported on GPU build: ALGO_LORENZO_REG and ALGO_NOPRED are not implemented");
+    const size_t hs = config_size(c);
+    if (cap < hs + 16) throw std::invalid_argument("The buffer for compressed data is not large enough.");
+    uint8_t *d_pay = d_out + hs;
+    const size_t pcap = cap - hs;
+    size_t payload = 0;
+    const size_t raw_bytes = (size_t)c.num * sizeof(T);
+    if (c.cmprAlgo != ALGO_LOSSLESS) {
+        try {
+            if (c.interpAnchorStride < 0) c.interpAnchorStride = (int)default_anchor(c.N);
+            if (c.cmprAlgo == ALGO_INTERP_LORENZO) {
+                tune_interp<T>(ctx, c, d_x, st);  // sets interpAlgo/direction/alpha/beta, cmprAlgo = ALGO_INTERP
+            }
+            if (c.cmprAlgo != ALGO_INTERP)
+                throw std::invalid_argument("unsupported on GPU build: the tuner chose a non-interpolation algorithm");
+            long long dims[4];
+            for (int i = 0; i < c.N; i++) dims[i] = (long long)c.dims[i];
+            const InterpParams prm = interp_params_of(c);
+            const InterpPlan plan = make_plan(dims, c.N, prm);
+            Pool pool(st);
+            int16_t *codes = pool.get<int16_t>((size_t)plan.n_codes + 16);
+            T *unpred = pool.get<T>((size_t)c.num + 16);
+            void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
+            unsigned long long *nesc = pool.get<unsigned long long>(2);
+            interp_compress<T>(plan, d_x, codes, unpred, ws, nesc, st);
+            const EntropyChoice ch = choose_entropy(ctx, codes, (size_t)plan.n_codes, st);  // syncs: nesc ready
+            unsigned long long h_nesc = 0;
+            FB2_CUDA(cudaMemcpyAsync(&h_nesc, nesc, 8, cudaMemcpyDeviceToHost, st));
+            FB2_CUDA(cudaStreamSynchronize(st));
+            const long long n_unpred = plan.n_anchor + (long long)h_nesc;
+            if (n_unpred > 0x7fffffffLL) throw std::length_error("The buffer for compressed data is not large enough.");
+            DecompHeader dh{};
+            dh.N = c.N;
+            for (int i = 0; i < c.N; i++) dh.dims[i] = c.dims[i];
+            long long maxd = 1;
+            for (int i = 0; i < c.N; i++) maxd = std::max<long long>(maxd, (long long)c.dims[i]);
+            dh.blocksize = (uint32_t)maxd;
+            dh.interp_id = c.interpAlgo;
+            dh.direction = c.interpDirection;
+            dh.anchor = (uint64_t)plan.anchor;
+            dh.alpha = c.interpAlpha;
+            dh.beta = c.interpBeta;
+            dh.quant_uid = 0b10;
+            dh.eb = c.absErrorBound;
+            dh.radius = c.quantbinCnt / 2;
+            dh.n_unpred = (int32_t)n_unpred;
+            std::vector<uint8_t> hdr;
+            decomp_header_write(dh, hdr);
+            Assembler as;
+            as.bytes(hdr.data(), hdr.size());
+            as.dev(unpred, (size_t)n_unpred * sizeof(T));
+            as.val<uint64_t>((uint64_t)plan.n_codes);
+            entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st);
+            if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
+            payload = as.run_framed(pool, d_pay, st);
+            c.cmprAlgo = ALGO_INTERP;
+        } catch (std::length_error &) {
+            // FalconsDispatcher.hpp:100-118: downgrade to lossless when the buffer is too small
+            c.cmprAlgo = ALGO_LOSSLESS;
+        }
+    }
+    if (c.cmprAlgo == ALGO_LOSSLESS) {
+        payload = lossless_raw_frame(d_x, raw_bytes, d_pay, pcap, st);
+    } else if ((double)raw_bytes / (double)payload < 3 && zstd_available()) {
+        // FalconsDispatcher.hpp:121-133: compare with zstd of the (in-place reconstructed) field
+        std::vector<uint8_t> host(raw_bytes);
+        FB2_CUDA(cudaMemcpyAsync(host.data(), d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+        std::vector<uint8_t> z(8 + zstd_compress_bound(raw_bytes));
+        const uint64_t L = raw_bytes;
+        memcpy(z.data(), &L, 8);
+        const size_t zs = 8 + zstd_compress(host.data(), raw_bytes, z.data() + 8, z.size() - 8, 3);
+        if (zs < payload && zs <= pcap) {
+            c.cmprAlgo = ALGO_LOSSLESS;
+            FB2_CUDA(cudaMemcpyAsync(d_pay, z.data(), zs, cudaMemcpyHostToDevice, st));
+            FB2_CUDA(cudaStreamSynchronize(st));
+            payload = zs;
+        }
+    }
+    std::vector<uint8_t> h(512);
+    const size_t hs2 = config_save(c, h.data());
+    if (hs2 != hs) throw std::logic_error("configuration header size changed");
+    FB2_CUDA(cudaMemcpyAsync(d_out, h.data(), hs2, cudaMemcpyHostToDevice, st));
+    FB2_CUDA(cudaStreamSynchronize(st));
+    if (conf_out) *conf_out = c;
+    return hs2 + payload;
+}
+
+// Parsed stream: where the payload's pieces live.
+struct Parsed {
+    falcons_config conf;
+    size_t hs = 0;
+};
+
+template <class T>
+void decompress_impl(Context &ctx, const uint8_t *h_stream, const uint8_t *d_stream, size_t len, T *d_out,
+                     size_t cap_elems, falcons_config *conf_out, cudaStream_t st) {
+    falcons_config c;
+    const size_t hs = config_load(h_stream, len, c);
+    if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
+    const uint8_t *hp = h_stream + hs;
+    const uint8_t *dp = d_stream + hs;
+    size_t plen = len - hs;
+    if (plen < 8) throw std::invalid_argument("Truncated Falcons lossless payload");
+    uint64_t L;
+    memcpy(&L, hp, 8);
+    const uint8_t *hf = hp + 8;
+    const size_t flen = plen - 8;
+    size_t fb = 0, content = 0;
+    const bool raw = parse_raw_frame(hf, flen, fb, content);
+    Pool pool(st);
+    uint8_t *d_flat = nullptr;
+    std::vector<uint8_t> host_flat;
+    ByteView view;
+    if (raw) {
+        if (content != L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
+        view.base = hf + fb;
+        view.len = L;
+        view.framed = true;
+        d_flat = pool.get<uint8_t>(L + 16);
+        std::vector<Piece> pcs;
+        logical_pieces(dp + 8 + fb, true, 0, L, 0, pcs);
+        launch_gather(pool, pcs, d_flat, st);
+    } else {
+        const unsigned long long fcs = zstd_frame_content_size(hf, flen);
+        if (fcs != 0xFFFFFFFFFFFFFFFFULL && fcs != L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
+        host_flat.resize(L + 16);
+        const size_t got = zstd_decompress(hf, flen, host_flat.data(), L);
+        if (got != L) throw std::invalid_argument("Invalid or truncated Falcons Zstd payload");
+        view.base = host_flat.data();
+        view.len = L;
+        d_flat = pool.get<uint8_t>(L + 16);
+        FB2_CUDA(cudaMemcpyAsync(d_flat, host_flat.data(), L, cudaMemcpyHostToDevice, st));
+    }
+    if (c.cmprAlgo == ALGO_LOSSLESS) {
+        if (L != c.num * sizeof(T)) throw std::runtime_error("Decompressed data size does not match the original data size");
+        FB2_CUDA(cudaMemcpyAsync(d_out, d_flat, L, cudaMemcpyDeviceToDevice, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+        if (conf_out) *conf_out = c;
+        return;
+    }
+    if (c.cmprAlgo != ALGO_INTERP)
+        throw std::invalid_argument("unsupported on GPU build: the stream uses a non-interpolation algorithm");
+    // decomposition header
+    size_t off = 0;
+    long long dims[4];
+    for (int i = 0; i < c.N; i++) {
+        dims[i] = (long long)view.rd<uint64_t>(off);
+        if ((uint64_t)dims[i] != c.dims[i]) throw std::invalid_argument("decomposition dims do not match the header");
+    }
+    view.rd<uint32_t>(off);  // blocksize
+    InterpParams p;
+    p.cubic = view.rd<int32_t>(off);
+    p.direction = view.rd<int32_t>(off);
+    p.anchor = (long long)view.rd<uint64_t>(off);
+    p.alpha = view.rd<double>(off);
+    p.beta = view.rd<double>(off);
+    const uint8_t uid = view.rd<uint8_t>(off);
+    if (uid != 0b10) throw std::invalid_argument("LinearQuantizer uid mismatch");
+    p.eb = view.rd<double>(off);
+    p.radius = view.rd<int32_t>(off);
+    const int32_t n_unpred = view.rd<int32_t>(off);
+    p.tuning = 0;
+    if (n_unpred < 0 || off + (size_t)n_unpred * sizeof(T) > L) throw std::invalid_argument("Truncated Falcons payload");
+    const InterpPlan plan = make_plan(dims, c.N, p);
+    if (n_unpred < plan.n_anchor) throw std::invalid_argument("Truncated Falcons payload");
+    T *unpred = pool.get<T>((size_t)n_unpred + 16);
+    {
+        std::vector<Piece> pcs;
+        if (n_unpred) pcs.push_back(Piece{d_flat + off, 0, (unsigned long long)n_unpred * sizeof(T)});
+        launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(unpred), st);
+    }
+    off += (size_t)n_unpred * sizeof(T);
+    const uint64_t n_codes = view.rd<uint64_t>(off);
+    if ((long long)n_codes != plan.n_codes) throw std::invalid_argument("code count does not match the field");
+    int16_t *codes = pool.get<int16_t>((size_t)n_codes + 16);
+    entropy_decode(ctx, d_flat + off, view.sub(off), (size_t)n_codes, codes, st);
+    void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
+    interp_decompress<T>(plan, codes, unpred, d_out, ws, st);
+    FB2_CUDA(cudaStreamSynchronize(st));
+    if (conf_out) *conf_out = c;
+}
+
+}  // namespace
+
+size_t compress_size_bound(int elem, const falcons_config *conf) {
+    if (!conf) throw std::invalid_argument("null config");
+    falcons_config c = *conf;
+    normalize_dims(c);
+    // FalconsImpl.hpp:44-55 (serial): 4096 + header + ZSTD_compressBound(num * sizeof(T))
+    return 4096 + config_size(c) + zstd_compress_bound((size_t)c.num * elem);
+}
+
+void read_config(const void *bytes, size_t len, falcons_config *conf_out) {
+    falcons_config c;
+    config_load(static_cast<const uint8_t *>(bytes), len, c);
+    if (conf_out) *conf_out = c;
+}
+
+void compress_device(Context &ctx, int elem, const falcons_config *conf, void *d_data, void *d_out, size_t cap,
+                     size_t *out_len, falcons_config *conf_out, cudaStream_t st) {
+    if (!conf || !d_data || !d_out) throw std::invalid_argument("null pointer");
+    if (cap < compress_size_bound(elem, conf)) throw std::invalid_argument("The buffer for compressed data is not large enough.");
+    size_t n;
+    if (elem == 4)
+        n = compress_impl<float>(ctx, *conf, static_cast<float *>(d_data), static_cast<uint8_t *>(d_out), cap, conf_out,
+                                 st, nullptr);
+    else
+        n = compress_impl<double>(ctx, *conf, static_cast<double *>(d_data), static_cast<uint8_t *>(d_out), cap,
+                                  conf_out, st, nullptr);
+    if (out_len) *out_len = n;
+}
+
+void compress_host(Context &ctx, int elem, const falcons_config *conf, void *data, uint32_t flags, void *out,
+                   size_t cap, size_t *out_len, falcons_config *conf_out) {
+    if (!conf || !data || !out) throw std::invalid_argument("null pointer");
+    if (cap < compress_size_bound(elem, conf)) throw std::invalid_argument("The buffer for compressed data is not large enough.");
+    falcons_config c = *conf;
+    normalize_dims(c);
+    const size_t bytes = (size_t)c.num * elem;
+    cudaStream_t st = ctx.stream;
+    void *d_x = ctx.field.get(bytes + 64);
+    FB2_CUDA(cudaMemcpyAsync(d_x, data, bytes, cudaMemcpyHostToDevice, st));
+    uint8_t *d_out = static_cast<uint8_t *>(ctx.out.get(cap + 64));
+    size_t n;
+    if (elem == 4)
+        n = compress_impl<float>(ctx, *conf, static_cast<float *>(d_x), d_out, cap, conf_out, st,
+                                 static_cast<const float *>(data));
+    else
+        n = compress_impl<double>(ctx, *conf, static_cast<double *>(d_x), d_out, cap, conf_out, st,
+                                  static_cast<const double *>(data));
+    FB2_CUDA(cudaMemcpyAsync(out, d_out, n, cudaMemcpyDeviceToHost, st));
+    if (flags & FALCONS_FLAG_WRITEBACK) FB2_CUDA(cudaMemcpyAsync(data, d_x, bytes, cudaMemcpyDeviceToHost, st));
+    FB2_CUDA(cudaStreamSynchronize(st));
+    if (out_len) *out_len = n;
+}
+
+void decompress_host(Context &ctx, int elem, const void *bytes, size_t len, void *out, size_t cap_elems,
+                     falcons_config *conf_out) {
+    if (!bytes || !out) throw std::invalid_argument("The decompression buffer is too small");
+    cudaStream_t st = ctx.stream;
+    falcons_config c;
+    config_load(static_cast<const uint8_t *>(bytes), len, c);
+    if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
+    uint8_t *d_stream = static_cast<uint8_t *>(ctx.codes.get(len + 64));
+    FB2_CUDA(cudaMemcpyAsync(d_stream, bytes, len, cudaMemcpyHostToDevice, st));
+    void *d_x = ctx.field.get((size_t)c.num * elem + 64);
+    if (elem == 4)
+        decompress_impl<float>(ctx, static_cast<const uint8_t *>(bytes), d_stream, len, static_cast<float *>(d_x),
+                               cap_elems, conf_out, st);
+    else
+        decompress_impl<double>(ctx, static_cast<const uint8_t *>(bytes), d_stream, len, static_cast<double *>(d_x),
+                                cap_elems, conf_out, st);
+    FB2_CUDA(cudaMemcpyAsync(out, d_x, (size_t)c.num * elem, cudaMemcpyDeviceToHost, st));
+    FB2_CUDA(cudaStreamSynchronize(st));
+}
+
+void decompress_device(Context &ctx, int elem, const void *d_stream, size_t len, void *d_out, size_t cap_elems,
+                       falcons_config *conf_out, cudaStream_t st) {
+    if (!d_stream || !d_out) throw std::invalid_argument("null pointer");
+    // The block structure is parsed on the host: bring the stream bytes over once.
+    std::vector<uint8_t> h(len);
+    FB2_CUDA(cudaMemcpyAsync(h.data(), d_stream, len, cudaMemcpyDeviceToHost, st));
+    FB2_CUDA(cudaStreamSynchronize(st));
+    if (elem == 4)
+        decompress_impl<float>(ctx, h.data(), static_cast<const uint8_t *>(d_stream), len, static_cast<float *>(d_out),
+                               cap_elems, conf_out, st);
+    else
+        decompress_impl<double>(ctx, h.data(), static_cast<const uint8_t *>(d_stream), len,
+                                static_cast<double *>(d_out), cap_elems, conf_out, st);
+}
+
 size_t encode_codes(Context &ctx, const int16_t *d_codes, size_t n, uint8_t *d_out, size_t cap, cudaStream_t st) {
     const EntropyChoice ch = choose_entropy(ctx, d_codes, n, st);
     return entropy_encode(ctx, d_codes, n, ch, d_out, cap, st);
 }
+
 void decode_codes(Context &ctx, const uint8_t *d_in, size_t len, size_t n, int16_t *d_codes, cudaStream_t st) {
-    entropy_decode(ctx, d_in, nullptr, len, n, d_codes, st);
+    std::vector<uint8_t> h = d2h(d_in, len, st);
+    ByteView v;
+    v.base = h.data();
+    v.len = len;
+    entropy_decode(ctx, d_in, v, n, d_codes, st);
 }
+
 }  // namespace fb2
