@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Falcons path on the single-large-field workload.
+
+Workload: one 3-D float32 field 512 x 512 x 512 (512 MiB), a Gaussian random field with power
+spectrum P(k) ~ k^-11/3 (seeded synthetic data: the reference's SDRBench fields are not available
+offline), compressed with ALGO_INTERP at EB_REL 1e-4 and decompressed.  A step is one compress
+plus one decompress of the field.
+
+  value  device-resident throughput: the field and the compressed stream stay in HBM
+         (falcons_compress_device / falcons_decompress_device), 2 x field bytes per step.
+  e2e    the same through the host-buffer C ABI (falcons_compress / falcons_decompress) from
+         pinned host memory, host<->device copies inside the timed region.
+  --impl reference  times the reference's own CPU build (AVX2 + OpenMP, all host cores).
+
+Multi-GPU (torchrun): every rank compresses its own field (independent replicas, weak scaling);
+the throughput is the sum over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "compress/decompress GB/s at rel EB 1e-4 vs plain GPU and CPU; p50/p99 latency"
+UNIT = "GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="falcons", choices=["falcons", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--rel", type=float, default=1e-4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4)
+                          if r[5 + i].lower() in ("active", "1")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_config(api, shape, rel):
+    c = api.falconsConfig(*shape)
+    c.cmprAlgo = api.falconsAlgorithm.INTERP
+    c.errorBoundMode = api.falconsErrorBoundMode.REL
+    c.relErrorBound = rel
+    return c
+
+
+def cpu_reference_run(x_host, rel, steps, warmup):
+    """Times the reference AVX2 + OpenMP build on the host cores; returns (GB/s, cores, kind, sample, ratio)."""
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    import oracle
+    if oracle.reference_available(omp=True):
+        R = oracle.Reference(omp=True)
+        conf = oracle.ref_conf(algo=oracle.ALGO_INTERP, eb_mode=oracle.EB_REL, rel_eb=rel, openmp=True)
+        best = None
+        ratio = None
+        for it in range(warmup + steps):
+            w = x_host.copy()
+            t0 = time.perf_counter()
+            s = R.compress(w, conf, mutate=True)
+            t1 = time.perf_counter()
+            R.decompress(s, np.float32, x_host.size)
+            t2 = time.perf_counter()
+            ratio = x_host.nbytes / len(s)
+            if it >= warmup:
+                best = (t1 - t0, t2 - t1) if best is None else (min(best[0], t1 - t0), min(best[1], t2 - t1))
+        gbs = 2 * x_host.nbytes / (best[0] + best[1]) / 1e9
+        return gbs, cores, "reference", (f"full {x_host.shape} field, AVX2+OpenMP build with openmp=true, "
+                                         f"{warmup} warm-up + best of {steps}; compress {x_host.nbytes / best[0] / 1e9:.3f} "
+                                         f"GB/s, decompress {x_host.nbytes / best[1] / 1e9:.3f} GB/s"), ratio
+    # Fallback: the oracle's C restatement (interpolation stage only, single thread) on a sub-block
+    O = oracle.Restatement()
+    sub = np.ascontiguousarray(x_host[:128, :128, :128])
+    eb = rel * float(x_host.max() - x_host.min())
+    t0 = time.perf_counter()
+    r = O.compress(sub, eb)
+    t1 = time.perf_counter()
+    return (2 * sub.nbytes / (t1 - t0) / 1e9, 1, "port",
+            "128^3 sub-block, oracle C restatement of the interpolation stage (compress+decompress), 1 thread", None)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import torch
+    from falcons_b200 import synth
+    shape = (args.size,) * 3
+    if torch.cuda.is_available():
+        x = synth.spectral_field_torch(shape, seed=1, device="cuda:0").cpu().numpy()
+    else:
+        x = synth.spectral_field(shape, seed=1)
+    t0 = time.perf_counter()
+    gbs, cores, kind, sample, ratio = cpu_reference_run(x, args.rel, max(1, args.steps), max(0, args.warmup))
+    line = {"impl": "reference", "metric": METRIC, "value": round(gbs, 4), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded spectral k^-11/3 field)",
+            "config": {"workload": f"single field {args.size}^3 float32, ALGO_INTERP, EB_REL {args.rel}",
+                       "ratio": ratio},
+            "cpu_baseline": {"value": round(gbs, 4), "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": round(gbs, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": round(time.perf_counter() - t0, 2)}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    from falcons_b200 import _lib, api
+    from falcons_b200 import device as D
+    from falcons_b200 import synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    shape = (args.size,) * 3
+    x0 = synth.spectral_field_torch(shape, seed=1 + rank, device=dev)
+    nbytes = x0.numel() * 4
+    xw = torch.empty_like(x0)
+    rec = torch.empty_like(x0)
+    conf = make_config(api, shape, args.rel)
+    ctx = _lib.default_context(local)
+    st = torch.cuda.current_stream()
+    out = None
+
+    def step(times=None):
+        nonlocal out
+        xw.copy_(x0)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        s, _ = D.compress(xw, conf, out=out, ctx=ctx)
+        out_buf = s
+        e1.record()
+        D.decompress(out_buf, torch.float32, out=rec.view(-1), ctx=ctx)
+        e2.record()
+        if times is not None:
+            times.append((e0, e1, e2, s.numel()))
+        return s
+
+    s = step()
+    torch.cuda.synchronize()
+    out = torch.empty(int(api.size_bound(conf, np.float32)), dtype=torch.uint8, device=dev)
+    err = float((rec.view(shape).double() - x0.double()).abs().max())
+    eb = args.rel * float(x0.max() - x0.min())
+    assert err <= eb * (1 + 1e-12), f"error bound violated: {err} > {eb}"
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = _lib.lib().falcons_kernel_launches()
+    times = []
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record()
+    for _ in range(args.steps):
+        step(times)
+    t_end.record()
+    torch.cuda.synchronize()
+    launches = _lib.lib().falcons_kernel_launches() - l0
+    ck = clocks.stop()
+    if dist:
+        dist.barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    tc = [a.elapsed_time(b) for a, b, c, n in times]
+    td = [b.elapsed_time(c) for a, b, c, n in times]
+    stream_len = times[-1][3]
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = 2 * nbytes * args.steps * world / (total_ms / 1e3) / 1e9
+
+    # ---- live roofline of the prediction + quantization stage (interpolation kernels)
+    eb_abs = args.rel * float(x0.max() - x0.min())
+    p = D.interp_params(eb_abs, 1, 0, None, 3)
+    pq = []
+    pqd = []
+    for it in range(4):
+        xw.copy_(x0)
+        a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a.record()
+        codes, unpred = D.interp_compress(xw, p, ctx=ctx)
+        b.record()
+        D.interp_decompress(shape, torch.float32, codes, unpred, p, out=rec, ctx=ctx)
+        c.record()
+        torch.cuda.synchronize()
+        if it:
+            pq.append(a.elapsed_time(b))
+            pqd.append(b.elapsed_time(c))
+    pq_ms = float(np.mean(pq))
+    pqd_ms = float(np.mean(pqd))
+    alg_bytes = x0.numel() * (4 + 2)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = alg_bytes / (pq_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("interp_compress_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the host-buffer C ABI (pinned memory)
+    e2e = None
+    if rank == 0 or True:
+        hx = torch.empty(x0.shape, dtype=torch.float32, pin_memory=True)
+        hx.copy_(x0.cpu())
+        hout = torch.empty(int(api.size_bound(conf, np.float32)), dtype=torch.uint8, pin_memory=True)
+        hrec = torch.empty(x0.numel(), dtype=torch.float32, pin_memory=True)
+        import ctypes
+        L = _lib.lib()
+        n = ctypes.c_size_t(0)
+        co = _lib.Config()
+
+        def e2e_step():
+            _lib.check(L.falcons_compress(ctx.ptr, _lib.F32, ctypes.byref(conf.conf), ctypes.c_void_p(hx.data_ptr()),
+                                          ctypes.c_uint32(0), ctypes.c_void_p(hout.data_ptr()),
+                                          ctypes.c_size_t(hout.numel()), ctypes.byref(n), ctypes.byref(co)))
+            _lib.check(L.falcons_decompress(ctx.ptr, _lib.F32, ctypes.c_void_p(hout.data_ptr()), n,
+                                            ctypes.c_void_p(hrec.data_ptr()), ctypes.c_size_t(hrec.numel()),
+                                            ctypes.byref(co)))
+            return n.value
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            m = e2e_step()
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.e2e_steps
+        e2e = {"value": round(2 * nbytes / dt / 1e9, 3), "unit": UNIT, "h2d_bytes_per_step": int(nbytes + m),
+               "d2h_bytes_per_step": int(m + nbytes), "ms_per_step": round(dt * 1e3, 3)}
+        if dist:
+            t = torch.tensor([e2e["value"]], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            e2e["value"] = round(float(t.item()), 3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        gbs, cores, kind, sample, ratio_ref = cpu_reference_run(x0.cpu().numpy(), args.rel, 1, 1)
+        cpu = {"value": round(gbs, 4), "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+               "ratio": ratio_ref}
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded spectral k^-11/3 Gaussian random field, generated on the device)",
+        "config": {"workload": f"single field {args.size}^3 float32, ALGO_INTERP (cubic, direction 0), EB_REL {args.rel}",
+                   "step": "one compress + one decompress, field and stream resident in HBM",
+                   "l2": "inputs (512 MiB) larger than L2 (126 MB), no flush",
+                   "ratio": round(nbytes / stream_len, 4), "stream_bytes": int(stream_len),
+                   "compress_GBps": round(nbytes / (np.median(tc) / 1e3) / 1e9, 3),
+                   "decompress_GBps": round(nbytes / (np.median(td) / 1e3) / 1e9, 3),
+                   "compress_ms_p50": round(float(np.median(tc)), 4), "decompress_ms_p50": round(float(np.median(td)), 4),
+                   "compress_ms_p99": round(float(np.percentile(tc, 99)), 4),
+                   "decompress_ms_p99": round(float(np.percentile(td, 99)), 4),
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "kernel": "prediction+quantization stage (interpolation pass kernels + escape scan), "
+                               f"algorithmic bytes num*(4+2) = {alg_bytes}; decompress stage "
+                               f"{alg_bytes / (pqd_ms / 1e3) / 1e9:.1f} GB/s",
+                     "peak_source": f"{peak_src} hbm_gbs", "stage_ms": round(pq_ms, 4)},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

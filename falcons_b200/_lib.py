@@ -45,7 +45,7 @@ _lib = None
 _lock = threading.Lock()
 
 EXPORTS = [
-    "falcons_ctx_create", "falcons_ctx_destroy", "falcons_last_error", "falcons_version",
+    "falcons_ctx_create", "falcons_ctx_destroy", "falcons_last_error", "falcons_version", "falcons_kernel_launches",
     "falcons_compress_size_bound", "falcons_compress", "falcons_read_config", "falcons_decompress",
     "falcons_compress_device", "falcons_decompress_device", "falcons_interp_compress",
     "falcons_interp_decompress", "falcons_device_range", "falcons_encode_codes", "falcons_decode_codes",
@@ -62,6 +62,7 @@ def lib() -> ctypes.CDLL:
             L = ctypes.CDLL(LIB_PATH)
             L.falcons_last_error.restype = ctypes.c_char_p
             L.falcons_version.restype = ctypes.c_char_p
+            L.falcons_kernel_launches.restype = ctypes.c_uint64
             L.falcons_compress_size_bound.restype = ctypes.c_size_t
             L.falcons_compress_size_bound.argtypes = [ctypes.c_int, ctypes.POINTER(Config)]
             for name in EXPORTS:

@@ -104,6 +104,71 @@ void Assembler::run(Pool &pool, uint8_t *d_out, cudaStream_t st) {
     FB2_CUDA(cudaStreamSynchronize(st));  // the host vectors must outlive the async copies
 }
 
+bool SparseIndex::read(void *dst, unsigned long long o, size_t n) const {
+    // last entry with off <= o
+    size_t lo = 0, hi = off.size();
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (off[mid] <= o) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo == 0) return false;
+    const size_t e = lo - 1;
+    if (o + n > off[e] + len[e]) return false;
+    memcpy(dst, bytes.data() + pos[e] + (o - off[e]), n);
+    return true;
+}
+
+bool SparseIndex::parse(const uint8_t *c, size_t size, SparseIndex &out) {
+    if (size < 12) return false;
+    uint32_t tag, count;
+    memcpy(&tag, c, 4);
+    memcpy(&count, c + 4, 4);
+    if (tag != kIndexTag) return false;
+    size_t p = 8;
+    for (uint32_t i = 0; i < count; i++) {
+        if (p + 12 > size) return false;
+        unsigned long long o;
+        uint32_t l;
+        memcpy(&o, c + p, 8);
+        memcpy(&l, c + p + 8, 4);
+        p += 12;
+        if (p + l > size) return false;
+        out.off.push_back(o);
+        out.len.push_back(l);
+        out.pos.push_back(out.bytes.size());
+        out.bytes.insert(out.bytes.end(), c + p, c + p + l);
+        p += l;
+    }
+    for (size_t i = 1; i < out.off.size(); i++)
+        if (out.off[i] < out.off[i - 1]) return false;
+    return true;
+}
+
+std::vector<uint8_t> Assembler::index_frame() const {
+    std::vector<std::pair<unsigned long long, std::pair<const uint8_t *, size_t>>> e;
+    for (auto &r : host_refs) e.push_back({pieces[r.first].dst, {host.data() + r.second, (size_t)pieces[r.first].len}});
+    for (auto &sh : shadows) e.push_back({sh.first, {sh.second.data(), sh.second.size()}});
+    std::sort(e.begin(), e.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    std::vector<uint8_t> c(16);
+    const uint32_t magic = kSkippableMagic, tag = kIndexTag, count = (uint32_t)e.size();
+    memcpy(c.data() + 8, &tag, 4);
+    memcpy(c.data() + 12, &count, 4);
+    for (auto &x : e) {
+        const unsigned long long o = x.first;
+        const uint32_t l = (uint32_t)x.second.second;
+        const size_t at = c.size();
+        c.resize(at + 12 + l);
+        memcpy(c.data() + at, &o, 8);
+        memcpy(c.data() + at + 8, &l, 4);
+        memcpy(c.data() + at + 12, x.second.first, l);
+    }
+    const uint32_t fsz = (uint32_t)(c.size() - 8);
+    memcpy(c.data(), &magic, 4);
+    memcpy(c.data() + 4, &fsz, 4);
+    return c;
+}
+
 size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
     const size_t L = pos;
     std::vector<uint8_t> hb = host;  // extra host bytes: length word, frame header, block headers
@@ -155,11 +220,18 @@ size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
             rem -= c;
         }
     }
+    size_t total = 8 + zstd_raw_frame_size(L);
+    if (with_index) {
+        const std::vector<uint8_t> idx = index_frame();
+        host_pieces.push_back(out.size());
+        add_host(idx.data(), idx.size(), total);
+        total += idx.size();
+    }
     uint8_t *dh = h2d(pool, hb, st);
     for (size_t i : host_pieces) out[i].src = dh + reinterpret_cast<uintptr_t>(out[i].src);
     launch_gather(pool, out, d_out, st);
     FB2_CUDA(cudaStreamSynchronize(st));
-    return 8 + zstd_raw_frame_size(L);
+    return total;
 }
 
 void logical_pieces(const uint8_t *d_base, bool framed, size_t off, size_t n, unsigned long long dst,

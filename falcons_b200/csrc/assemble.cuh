@@ -69,11 +69,35 @@ size_t zstd_raw_frame_size(size_t content);
 // Frame header bytes (magic + descriptor + content size); returns its length.
 size_t zstd_raw_frame_header(uint8_t *out, size_t content);
 
+// Header index carried in a zstd skippable frame after the payload frame (RFC 8878 section 3.1.2;
+// decoders, the reference's included, skip it).  It holds every header byte of the payload
+// (logical offset + bytes), so a decoder whose stream sits in device memory can parse the block
+// structure without copying the stream to the host.
+constexpr uint32_t kSkippableMagic = 0x184D2A5Bu;
+constexpr uint32_t kIndexTag = 0x49324246u;  // "FB2I"
+
+struct SparseIndex {
+    std::vector<unsigned long long> off;   // sorted logical offsets
+    std::vector<uint32_t> len;
+    std::vector<size_t> pos;               // into bytes
+    std::vector<uint8_t> bytes;
+    // Returns false when [o, o+n) is not fully covered by one entry.
+    bool read(void *dst, unsigned long long o, size_t n) const;
+    static bool parse(const uint8_t *content, size_t size, SparseIndex &out);
+};
+
 struct Assembler {
     std::vector<Piece> pieces;                         // logical layout
     std::vector<uint8_t> host;                         // host-built bytes
     std::vector<std::pair<size_t, size_t>> host_refs;  // (piece index, host offset)
+    std::vector<std::pair<unsigned long long, std::vector<uint8_t>>> shadows;  // header bytes of device pieces
     unsigned long long pos = 0;
+    bool with_index = true;
+    // Records that the next device piece starts with these (host-known) header bytes.
+    void shadow(const void *b, size_t n) {
+        shadows.push_back({pos, std::vector<uint8_t>(static_cast<const uint8_t *>(b), static_cast<const uint8_t *>(b) + n)});
+    }
+    std::vector<uint8_t> index_frame() const;
     void dev(const void *src, size_t len) {
         if (!len) return;
         pieces.push_back(Piece{static_cast<const uint8_t *>(src), pos, len});
@@ -95,11 +119,12 @@ struct Assembler {
     void run(Pool &pool, uint8_t *d_out, cudaStream_t st);
     // Writes [u64 pos][zstd raw-block frame of the layout] to d_out; returns the bytes written.
     size_t run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st);
-    size_t framed_size() const { return 8 + zstd_raw_frame_size(pos); }
+    size_t framed_size() const { return 8 + zstd_raw_frame_size(pos) + (with_index ? index_frame().size() : 0); }
 };
 
 // Logical bytes [0, len) stored either flat or as the content of a raw-block zstd frame.
 struct ByteView {
+    const SparseIndex *sparse = nullptr;  // when set, reads are served from the header index
     const uint8_t *base = nullptr;   // host pointer (flat bytes or the frame's first block header)
     size_t len = 0;                  // logical length (from origin)
     bool framed = false;
@@ -117,11 +142,20 @@ struct ByteView {
     }
     uint8_t at(size_t i) const {
         if (i >= len) throw std::invalid_argument("Invalid or truncated Falcons payload");
+        if (sparse) {
+            uint8_t b;
+            read(&b, i, 1);
+            return b;
+        }
         return base[phys(i)];
     }
     void read(void *dst, size_t off, size_t n) const {
         if (off + n > len || off + n < off) throw std::invalid_argument("Invalid or truncated Falcons payload");
         uint8_t *d = static_cast<uint8_t *>(dst);
+        if (sparse) {
+            if (!sparse->read(d, origin + off, n)) throw std::out_of_range("header index does not cover the read");
+            return;
+        }
         if (!framed) {
             memcpy(d, base + origin + off, n);
             return;

@@ -1,6 +1,7 @@
 // extern "C" boundary of libfalcons_b200.so (declared in include/falcons_b200.h).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -71,9 +72,15 @@ void check_dtype(int dtype) {
 }
 }  // namespace
 
+namespace fb2 {
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long count_launch() { return ++g_launches; }
+}  // namespace fb2
+
 extern "C" {
 
 const char *falcons_last_error(void) { return g_last_error.c_str(); }
+uint64_t falcons_kernel_launches(void) { return fb2::g_launches.load(); }
 const char *falcons_version(void) { return "falcons_b200 1.0.0 (stream format Falcons data version 1.0.0)"; }
 
 int falcons_ctx_create(falcons_ctx **out, int device) {

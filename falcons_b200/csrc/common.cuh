@@ -28,7 +28,13 @@ struct cuda_error : std::runtime_error {
                                     __FILE__ + ":" + std::to_string(__LINE__));                         \
     } while (0)
 
-#define FB2_CHECK_LAUNCH() FB2_CUDA(cudaGetLastError())
+// Every kernel launch of the library is followed by FB2_CHECK_LAUNCH(), which also counts it.
+unsigned long long count_launch();
+#define FB2_CHECK_LAUNCH()      \
+    do {                        \
+        ::fb2::count_launch();  \
+        FB2_CUDA(cudaGetLastError()); \
+    } while (0)
 
 // ---------------------------------------------------------------- predictor formulas
 enum Formula : int { F_EQUAL = 0, F_LINEAR, F_LINEAR1, F_QUAD1, F_QUAD2, F_QUAD3, F_CUBIC };

@@ -158,6 +158,7 @@ size_t parse_blocks(const ByteView &h, size_t off, unsigned long long n, unsigne
 // vals (u32, >= 1) of all groups concatenated; gstart has G+1 entries.
 struct GammaOut {
     std::vector<std::vector<std::pair<const uint8_t *, size_t>>> cls_pieces;  // per group
+    std::vector<std::vector<unsigned>> cls_n;                                  // symbols per block
     std::vector<size_t> cls_bytes;                                             // per group
     std::vector<const uint8_t *> man_ptr;                                      // per group
     std::vector<size_t> man_bytes;                                             // per group
@@ -204,6 +205,7 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     const long long T = (long long)gstart.back();
     GammaOut out;
     out.cls_pieces.resize(G);
+    out.cls_n.resize(G);
     out.cls_bytes.assign(G, 0);
     out.man_ptr.assign(G, nullptr);
     out.man_bytes.assign(G, 0);
@@ -257,9 +259,30 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     for (size_t j = 0; j < jobs.size(); j++) {
         const int g = job_group[j];
         out.cls_pieces[g].push_back({slots + j * kBlockSlot, (size_t)hs[j]});
+        out.cls_n[g].push_back(jobs[j].n);
         out.cls_bytes[g] += (size_t)hs[j];
     }
     return out;
+}
+
+// Adds the fse_enc records of group g, recording each record's header bytes for the index.
+void add_class_pieces(Assembler &as, const GammaOut &go, int g) {
+    for (size_t b = 0; b < go.cls_pieces[g].size(); b++) {
+        const auto &p = go.cls_pieces[g][b];
+        const unsigned n = go.cls_n[g][b];
+        uint8_t h[5];
+        size_t hl;
+        if (p.second == 1 + (size_t)n) { h[0] = 0; hl = 1; }
+        else if (p.second == 2) { h[0] = 2; hl = 1; }
+        else {
+            h[0] = 1;
+            const uint32_t r = (uint32_t)(p.second - 5);
+            memcpy(h + 1, &r, 4);
+            hl = 5;
+        }
+        as.shadow(h, hl);
+        as.dev(p.first, p.second);
+    }
 }
 
 __global__ void k_gamma_unpack(const uint8_t *__restrict__ cls, const unsigned long long *__restrict__ boff,
@@ -848,8 +871,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         as.val<uint64_t>(go.cls_bytes[1]);
         as.val<uint64_t>(go.man_bytes[0]);
         as.val<uint64_t>(go.man_bytes[1]);
-        for (auto &p : go.cls_pieces[0]) as.dev(p.first, p.second);
-        for (auto &p : go.cls_pieces[1]) as.dev(p.first, p.second);
+        add_class_pieces(as, go, 0);
+        add_class_pieces(as, go, 1);
         as.dev(go.man_ptr[0], go.man_bytes[0]);
         as.dev(go.man_ptr[1], go.man_bytes[1]);
     } else {
@@ -952,7 +975,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
                     as.val<uint8_t>(1);
                     as.val<uint64_t>(go.cls_bytes[g]);
                     as.val<uint64_t>(go.man_bytes[g]);
-                    for (auto &p : go.cls_pieces[g]) as.dev(p.first, p.second);
+                    add_class_pieces(as, go, (int)g);
                     as.dev(go.man_ptr[g], go.man_bytes[g]);
                 }
             }

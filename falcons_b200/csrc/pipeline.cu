@@ -87,6 +87,7 @@ struct LossyOut {
 size_t lossless_raw_frame(const void *d_x, size_t bytes, uint8_t *d_out, size_t cap, cudaStream_t st) {
     Pool pool(st);
     Assembler as;
+    as.with_index = false;
     as.dev(d_x, bytes);
     const size_t need = as.framed_size();
     if (need > cap) throw std::length_error("The buffer for compressed data is not large enough.");
@@ -192,62 +193,36 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     return hs2 + payload;
 }
 
-// Parsed stream: where the payload's pieces live.
-struct Parsed {
-    falcons_config conf;
-    size_t hs = 0;
+// Where the logical payload (frame content) lives.
+struct Payload {
+    uint64_t L = 0;                  // content length
+    bool raw = false;                // zstd frame of raw blocks (content addressable in place)
+    const uint8_t *d_blocks = nullptr;  // device address of the first block header (raw frames)
+    ByteView view;                   // host-readable view of the content (framed, flat or sparse)
+    std::vector<uint8_t> flat;       // host copy of the content (non-raw frames)
 };
 
 template <class T>
-void decompress_impl(Context &ctx, const uint8_t *h_stream, const uint8_t *d_stream, size_t len, T *d_out,
-                     size_t cap_elems, falcons_config *conf_out, cudaStream_t st) {
-    falcons_config c;
-    const size_t hs = config_load(h_stream, len, c);
-    if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
-    const uint8_t *hp = h_stream + hs;
-    const uint8_t *dp = d_stream + hs;
-    size_t plen = len - hs;
-    if (plen < 8) throw std::invalid_argument("Truncated Falcons lossless payload");
-    uint64_t L;
-    memcpy(&L, hp, 8);
-    const uint8_t *hf = hp + 8;
-    const size_t flen = plen - 8;
-    size_t fb = 0, content = 0;
-    const bool raw = parse_raw_frame(hf, flen, fb, content);
+void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_out, cudaStream_t st) {
     Pool pool(st);
-    uint8_t *d_flat = nullptr;
-    std::vector<uint8_t> host_flat;
-    ByteView view;
-    if (raw) {
-        if (content != L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
-        view.base = hf + fb;
-        view.len = L;
-        view.framed = true;
-        d_flat = pool.get<uint8_t>(L + 16);
+    const uint64_t L = pl.L;
+    const ByteView &view = pl.view;
+    uint8_t *d_flat = pool.get<uint8_t>(L + 16);
+    if (pl.raw) {
         std::vector<Piece> pcs;
-        logical_pieces(dp + 8 + fb, true, 0, L, 0, pcs);
+        logical_pieces(pl.d_blocks, true, 0, L, 0, pcs);
         launch_gather(pool, pcs, d_flat, st);
     } else {
-        const unsigned long long fcs = zstd_frame_content_size(hf, flen);
-        if (fcs != 0xFFFFFFFFFFFFFFFFULL && fcs != L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
-        host_flat.resize(L + 16);
-        const size_t got = zstd_decompress(hf, flen, host_flat.data(), L);
-        if (got != L) throw std::invalid_argument("Invalid or truncated Falcons Zstd payload");
-        view.base = host_flat.data();
-        view.len = L;
-        d_flat = pool.get<uint8_t>(L + 16);
-        FB2_CUDA(cudaMemcpyAsync(d_flat, host_flat.data(), L, cudaMemcpyHostToDevice, st));
+        FB2_CUDA(cudaMemcpyAsync(d_flat, pl.flat.data(), L, cudaMemcpyHostToDevice, st));
     }
     if (c.cmprAlgo == ALGO_LOSSLESS) {
         if (L != c.num * sizeof(T)) throw std::runtime_error("Decompressed data size does not match the original data size");
         FB2_CUDA(cudaMemcpyAsync(d_out, d_flat, L, cudaMemcpyDeviceToDevice, st));
         FB2_CUDA(cudaStreamSynchronize(st));
-        if (conf_out) *conf_out = c;
         return;
     }
     if (c.cmprAlgo != ALGO_INTERP)
         throw std::invalid_argument("unsupported on GPU build: the stream uses a non-interpolation algorithm");
-    // decomposition header
     size_t off = 0;
     long long dims[4];
     for (int i = 0; i < c.N; i++) {
@@ -284,7 +259,31 @@ void decompress_impl(Context &ctx, const uint8_t *h_stream, const uint8_t *d_str
     void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
     interp_decompress<T>(plan, codes, unpred, d_out, ws, st);
     FB2_CUDA(cudaStreamSynchronize(st));
-    if (conf_out) *conf_out = c;
+}
+
+// Lossless payload [u64 L][zstd frame(s)] held in host memory at hp (plen bytes).
+void payload_from_host(const uint8_t *hp, const uint8_t *dp, size_t plen, Payload &pl) {
+    if (plen < 8) throw std::invalid_argument("Truncated Falcons lossless payload");
+    memcpy(&pl.L, hp, 8);
+    const uint8_t *hf = hp + 8;
+    const size_t flen = plen - 8;
+    size_t fb = 0, content = 0;
+    pl.raw = parse_raw_frame(hf, flen, fb, content);
+    if (pl.raw) {
+        if (content != pl.L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
+        pl.view.base = hf + fb;
+        pl.view.len = pl.L;
+        pl.view.framed = true;
+        pl.d_blocks = dp + 8 + fb;
+    } else {
+        const unsigned long long fcs = zstd_frame_content_size(hf, flen);
+        if (fcs != 0xFFFFFFFFFFFFFFFFULL && fcs != pl.L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
+        pl.flat.resize(pl.L + 16);
+        const size_t got = zstd_decompress(hf, flen, pl.flat.data(), pl.L);
+        if (got != pl.L) throw std::invalid_argument("Invalid or truncated Falcons Zstd payload");
+        pl.view.base = pl.flat.data();
+        pl.view.len = pl.L;
+    }
 }
 
 }  // namespace
@@ -345,35 +344,92 @@ void decompress_host(Context &ctx, int elem, const void *bytes, size_t len, void
                      falcons_config *conf_out) {
     if (!bytes || !out) throw std::invalid_argument("The decompression buffer is too small");
     cudaStream_t st = ctx.stream;
+    const uint8_t *hb = static_cast<const uint8_t *>(bytes);
     falcons_config c;
-    config_load(static_cast<const uint8_t *>(bytes), len, c);
+    const size_t hs = config_load(hb, len, c);
     if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
     uint8_t *d_stream = static_cast<uint8_t *>(ctx.codes.get(len + 64));
     FB2_CUDA(cudaMemcpyAsync(d_stream, bytes, len, cudaMemcpyHostToDevice, st));
+    Payload pl;
+    payload_from_host(hb + hs, d_stream + hs, len - hs, pl);
     void *d_x = ctx.field.get((size_t)c.num * elem + 64);
-    if (elem == 4)
-        decompress_impl<float>(ctx, static_cast<const uint8_t *>(bytes), d_stream, len, static_cast<float *>(d_x),
-                               cap_elems, conf_out, st);
-    else
-        decompress_impl<double>(ctx, static_cast<const uint8_t *>(bytes), d_stream, len, static_cast<double *>(d_x),
-                                cap_elems, conf_out, st);
+    if (elem == 4) decompress_core<float>(ctx, c, pl, static_cast<float *>(d_x), st);
+    else decompress_core<double>(ctx, c, pl, static_cast<double *>(d_x), st);
     FB2_CUDA(cudaMemcpyAsync(out, d_x, (size_t)c.num * elem, cudaMemcpyDeviceToHost, st));
     FB2_CUDA(cudaStreamSynchronize(st));
+    if (conf_out) *conf_out = c;
 }
 
-void decompress_device(Context &ctx, int elem, const void *d_stream, size_t len, void *d_out, size_t cap_elems,
+void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t len, void *d_out, size_t cap_elems,
                        falcons_config *conf_out, cudaStream_t st) {
-    if (!d_stream || !d_out) throw std::invalid_argument("null pointer");
-    // The block structure is parsed on the host: bring the stream bytes over once.
+    if (!d_stream_v || !d_out) throw std::invalid_argument("null pointer");
+    const uint8_t *d_stream = static_cast<const uint8_t *>(d_stream_v);
+    // Only the headers are needed on the host: the stream prefix and the header index frame.
+    std::vector<uint8_t> pre(std::min<size_t>(len, 4096));
+    FB2_CUDA(cudaMemcpyAsync(pre.data(), d_stream, pre.size(), cudaMemcpyDeviceToHost, st));
+    FB2_CUDA(cudaStreamSynchronize(st));
+    falcons_config c;
+    const size_t hs = config_load(pre.data(), len, c);
+    if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
+    Payload pl;
+    SparseIndex idx;
+    bool fast = false;
+    if (pre.size() >= hs + 8 + 14) {
+        memcpy(&pl.L, pre.data() + hs, 8);
+        const uint8_t *hf = pre.data() + hs + 8;
+        uint32_t magic;
+        memcpy(&magic, hf, 4);
+        const uint8_t fhd = hf[4];
+        if (magic == kZstdMagic && fhd == (uint8_t)(((fhd >> 6) << 6) | 0x20)) {
+            static const int fcs_sizes[4] = {1, 2, 4, 8};
+            const int fb = 5 + fcs_sizes[fhd >> 6];
+            uint64_t v = 0;
+            for (int i = 0; i < fcs_sizes[fhd >> 6]; i++) v |= (uint64_t)hf[5 + i] << (8 * i);
+            if ((fhd >> 6) == 1) v += 256;
+            if (v == pl.L) {
+                const size_t frame = zstd_raw_frame_size(pl.L);
+                const size_t ipos = hs + 8 + frame;
+                uint8_t ih[8];
+                if (ipos + 8 <= len) {
+                    FB2_CUDA(cudaMemcpyAsync(ih, d_stream + ipos, 8, cudaMemcpyDeviceToHost, st));
+                    FB2_CUDA(cudaStreamSynchronize(st));
+                    uint32_t m, sz;
+                    memcpy(&m, ih, 4);
+                    memcpy(&sz, ih + 4, 4);
+                    if (m == kSkippableMagic && ipos + 8 + sz <= len) {
+                        std::vector<uint8_t> content(sz);
+                        FB2_CUDA(cudaMemcpyAsync(content.data(), d_stream + ipos + 8, sz, cudaMemcpyDeviceToHost, st));
+                        FB2_CUDA(cudaStreamSynchronize(st));
+                        if (SparseIndex::parse(content.data(), sz, idx)) {
+                            pl.raw = true;
+                            pl.d_blocks = d_stream + hs + 8 + fb;
+                            pl.view.sparse = &idx;
+                            pl.view.len = pl.L;
+                            fast = true;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (fast) {
+        try {
+            if (elem == 4) decompress_core<float>(ctx, c, pl, static_cast<float *>(d_out), st);
+            else decompress_core<double>(ctx, c, pl, static_cast<double *>(d_out), st);
+            if (conf_out) *conf_out = c;
+            return;
+        } catch (const std::out_of_range &) {
+            // the index does not cover a header: fall back to the full host copy below
+        }
+    }
     std::vector<uint8_t> h(len);
     FB2_CUDA(cudaMemcpyAsync(h.data(), d_stream, len, cudaMemcpyDeviceToHost, st));
     FB2_CUDA(cudaStreamSynchronize(st));
-    if (elem == 4)
-        decompress_impl<float>(ctx, h.data(), static_cast<const uint8_t *>(d_stream), len, static_cast<float *>(d_out),
-                               cap_elems, conf_out, st);
-    else
-        decompress_impl<double>(ctx, h.data(), static_cast<const uint8_t *>(d_stream), len,
-                                static_cast<double *>(d_out), cap_elems, conf_out, st);
+    Payload p2;
+    payload_from_host(h.data() + hs, d_stream + hs, len - hs, p2);
+    if (elem == 4) decompress_core<float>(ctx, c, p2, static_cast<float *>(d_out), st);
+    else decompress_core<double>(ctx, c, p2, static_cast<double *>(d_out), st);
+    if (conf_out) *conf_out = c;
 }
 
 size_t encode_codes(Context &ctx, const int16_t *d_codes, size_t n, uint8_t *d_out, size_t cap, cudaStream_t st) {

@@ -103,3 +103,45 @@ def decode_codes(payload: torch.Tensor, n: int, ctx=None, stream=None) -> torch.
                                                ctypes.c_size_t(payload.numel()), ctypes.c_size_t(n),
                                                ctypes.c_void_p(out.data_ptr()), _stream_ptr(stream)), "decode_codes")
     return out[:n]
+
+
+def compress(x: torch.Tensor, config, out: torch.Tensor | None = None, ctx=None, stream=None):
+    """Falcons_compress on a device-resident field; returns (uint8 stream tensor on the device, config).
+
+    `x` is overwritten with the reference's partial reconstruction (the in-place compressor).
+    `config` is a falcons_b200.api.falconsConfig.
+    """
+    assert x.is_cuda and x.is_contiguous()
+    ctx = ctx or _lib.default_context(x.device.index or 0)
+    if config.num_elements != x.numel():
+        config.setDims(*x.shape)
+    cap = int(_lib.lib().falcons_compress_size_bound(_dtype_code(x), ctypes.byref(config.conf)))
+    if out is None or out.numel() < cap:
+        out = torch.empty(cap, dtype=torch.uint8, device=x.device)
+    n = ctypes.c_size_t(0)
+    conf_out = _lib.Config()
+    _lib.check(_lib.lib().falcons_compress_device(ctx.ptr, _dtype_code(x), ctypes.byref(config.conf),
+                                                  ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                                  ctypes.c_size_t(out.numel()), ctypes.byref(n),
+                                                  ctypes.byref(conf_out), _stream_ptr(stream)), "compress_device")
+    return out[:n.value], conf_out
+
+
+def decompress(stream_bytes: torch.Tensor, dtype, out: torch.Tensor | None = None, ctx=None, stream=None):
+    """Falcons_decompress of a device-resident stream into a device tensor (flat)."""
+    assert stream_bytes.is_cuda and stream_bytes.dtype == torch.uint8
+    ctx = ctx or _lib.default_context(stream_bytes.device.index or 0)
+    head = stream_bytes[:256].cpu().numpy()
+    c = _lib.Config()
+    # the header (at most 255 bytes) is inside the first 256 bytes of the stream
+    buf = bytearray(head.tobytes())
+    _lib.check(_lib.lib().falcons_read_config((ctypes.c_char * len(buf)).from_buffer(buf), ctypes.c_size_t(len(buf)),
+                                              ctypes.byref(c)), "read_config")
+    if out is None:
+        out = torch.empty(int(c.num), dtype=dtype, device=stream_bytes.device)
+    conf_out = _lib.Config()
+    _lib.check(_lib.lib().falcons_decompress_device(ctx.ptr, _dtype_code(out), ctypes.c_void_p(stream_bytes.data_ptr()),
+                                                    ctypes.c_size_t(stream_bytes.numel()),
+                                                    ctypes.c_void_p(out.data_ptr()), ctypes.c_size_t(out.numel()),
+                                                    ctypes.byref(conf_out), _stream_ptr(stream)), "decompress_device")
+    return out, conf_out

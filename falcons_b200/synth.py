@@ -89,3 +89,35 @@ def latlon_field(shape=(1800, 3600), seed=3, n_waves=16, noise=1e-3, dtype=np.fl
     out *= np.cos(lat)
     out += rng.normal(0.0, noise, size=shape)
     return out.astype(dtype)
+
+
+def spectral_field_torch(shape=(512, 512, 512), seed=1, device="cuda", dtype=None):
+    """The spectral (k^-11/3) Gaussian random field generated on a CUDA device with torch.
+
+    Same construction as spectral_field (complex white noise shaped by k^-11/6, inverse real FFT,
+    zero mean / unit variance), with torch's generator, so it is fast at 512^3.
+    """
+    import torch
+    dtype = dtype or torch.float32
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    rshape = list(shape[:-1]) + [shape[-1] // 2 + 1]
+    re = torch.randn(rshape, generator=g, device=device, dtype=torch.float32)
+    im = torch.randn(rshape, generator=g, device=device, dtype=torch.float32)
+    k2 = torch.zeros(rshape, device=device, dtype=torch.float32)
+    for d, s in enumerate(shape):
+        f = torch.fft.rfftfreq(s, device=device) if d == len(shape) - 1 else torch.fft.fftfreq(s, device=device)
+        sh = [1] * len(shape)
+        sh[d] = -1
+        k2 = k2 + (f.float() * s).reshape(sh) ** 2
+    k = torch.sqrt(k2)
+    k.view(-1)[0] = 1.0
+    amp = k ** (-11.0 / 6.0)
+    amp.view(-1)[0] = 0.0
+    spec = torch.complex(re * amp, im * amp)
+    del re, im, k2, k, amp
+    x = torch.fft.irfftn(spec, s=shape)
+    del spec
+    x = x.double() if dtype == torch.float64 else x
+    x = (x - x.mean(dtype=torch.float64)) / x.std()
+    return x.to(dtype).contiguous()

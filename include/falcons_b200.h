@@ -90,6 +90,8 @@ int falcons_ctx_create(falcons_ctx **out, int device);
 int falcons_ctx_destroy(falcons_ctx *ctx);
 const char *falcons_last_error(void);
 const char *falcons_version(void);
+/* Number of CUDA kernels this library has launched in the process (all contexts). */
+uint64_t falcons_kernel_launches(void);
 
 /* ---- drop-in API (host buffers) ---- */
 size_t falcons_compress_size_bound(int dtype, const falcons_config *conf);

@@ -15,7 +15,7 @@ def _declared():
     names = []
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
         txt = open(h).read()
-        names += re.findall(r"^\s*(?:int|size_t|const char \*)\s*(falcons_\w+)\s*\(", txt, re.M)
+        names += re.findall(r"^\s*(?:int|size_t|uint64_t|const char \*)\s*(falcons_\w+)\s*\(", txt, re.M)
     return sorted(set(names))
 
 

@@ -171,3 +171,23 @@ def test_degenerate_shapes(cuda, reference, shape):
     y, _ = api.falcons.decompress(buf, np.float32, shape)
     np.testing.assert_array_equal(y.ravel(), reference.decompress(buf.tobytes(), np.float32, x.size).ravel())
     assert np.abs(y.astype(np.float64) - x).max() <= 1e-3
+
+
+@pytest.mark.parametrize("rel", [1e-4, 1e-2])
+def test_device_resident_path_uses_header_index(cuda, reference, rel):
+    """compress_device / decompress_device on HBM-resident data, against the host API and the reference."""
+    import torch
+    from falcons_b200 import api, device as D, synth
+    x = synth.spectral_field((96, 100, 104), seed=4)
+    conf = _conf(api, x.shape, mode="REL", rel=rel)
+    xd = torch.from_numpy(x.copy()).to(cuda)
+    s, c = D.compress(xd, conf)
+    host_buf, _ = api.falcons.compress(x.copy(), conf, copy=True)
+    np.testing.assert_array_equal(s.cpu().numpy(), host_buf)      # same bytes from both entry points
+    y, _ = D.decompress(s, torch.float32)
+    torch.cuda.synchronize()
+    y_ref = reference.decompress(host_buf.tobytes(), np.float32, x.size).ravel()
+    np.testing.assert_array_equal(y.cpu().numpy(), y_ref)
+    before = __import__("falcons_b200")._lib.lib().falcons_kernel_launches()
+    D.decompress(s, torch.float32)
+    assert __import__("falcons_b200")._lib.lib().falcons_kernel_launches() > before
