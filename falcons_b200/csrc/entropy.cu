@@ -10,6 +10,7 @@
 //   encode_o1_ovf     :483-575   escape side stream (gamma + FSE, or raw int16)
 //   decode            :984-1070, decode_o1tans :753-843
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <vector>
@@ -30,15 +31,11 @@ constexpr int O1_NSYM = 256;
 constexpr int kMaxK = 16;
 
 __host__ __device__ __forceinline__ int o1_ctx(int code) {
+    // magnitude buckets 1,2,3,4 | 5-7 | 8-11 | >= 12, doubled for the sign (RleFseEncoder.hpp:354-384)
     const int sgn = code < 0;
     const int a = sgn ? -code : code;
-    if (a == 0) return 0;
-    int m;
-    if (a <= 4) m = a - 1;
-    else if (a <= 7) m = 4;
-    else if (a <= 11) m = 5;
-    else m = 6;
-    return 1 + m * 2 + sgn;
+    const int m = min(a - 1, 3 + (a > 4) + (a > 7) + (a > 11));
+    return a == 0 ? 0 : 1 + m * 2 + sgn;
 }
 
 __host__ __device__ __forceinline__ int o1_sym(int code) {
@@ -61,22 +58,94 @@ struct BlockJob {
 
 constexpr size_t kBlockSlot = FBLK + 64;
 
-// One CTA per 64 Ki block: parallel histogram, then the sequential FSE coder in thread 0.
+// FSE_compress on the device: header, tables and the 2-state reverse coding of one 64 Ki block
+// (zfse/fse_compress.c FSE_compress_wksp).  The two state chains are interleaved and the symbol
+// loads are issued ahead of the dependent table lookups.
+__device__ size_t fse_block_encode(uint8_t *dst, size_t cap, const uint8_t *__restrict__ src, size_t n,
+                                   fse::BlockScratch &w, uint8_t *__restrict__ bits, size_t &hdr_out,
+                                   size_t &body_out) {
+    if (n <= 2) return 0;
+    unsigned maxSV = 255;
+    while (maxSV > 0 && w.count[maxSV] == 0) maxSV--;
+    uint32_t maxCount = 0;
+    for (unsigned s2 = 0; s2 <= maxSV; s2++) maxCount = w.count[s2] > maxCount ? w.count[s2] : maxCount;
+    if (maxCount == n) return 1;
+    if (maxCount == 1) return 0;
+    if (maxCount < (n >> 7)) return 0;
+    const unsigned tl = fse::optimal_table_log(fse::kDefaultTableLog, n, maxSV);
+    if (fse::normalize_count(w.norm, tl, w.count, n, maxSV) != tl) return 0;
+    if (cap < fse::ncount_bound(maxSV, tl) + 16) return 0;
+    const size_t hdr = fse::write_ncount(dst, w.norm, maxSV, tl);
+    if (hdr == 0) return 0;
+    if (!fse::build_ctable(w.state_table, w.sym_tt, w.sym, w.norm, maxSV, tl)) return 0;
+    fse::Writer32 bw;
+    bw.init(bits, cap - hdr);
+    uint32_t st[2];
+    for (int k = 0; k < 2; k++) {
+        const size_t i = ((n - 1) % 2 == (size_t)k) ? n - 1 : n - 2;
+        const fse::SymTT t = w.sym_tt[src[i]];
+        const uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
+        const uint32_t v = (nb << 16) - t.deltaNbBits;
+        st[k] = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
+    }
+    // symbols n-3 .. 0 in that order; index parity selects the state
+    long long ii = (long long)n - 3;
+    uint8_t sa = ii >= 1 ? src[ii] : 0, sb = ii >= 1 ? src[ii - 1] : 0;
+    while (ii >= 1) {
+        const uint8_t na = ii >= 3 ? src[ii - 2] : 0, nbs = ii >= 3 ? src[ii - 3] : 0;  // next pair, early
+        const fse::SymTT ta = w.sym_tt[sa], tb = w.sym_tt[sb];
+        const int ka = (int)(ii & 1), kb = ka ^ 1;
+        const uint32_t nba = (st[ka] + ta.deltaNbBits) >> 16;
+        const uint32_t nbb = (st[kb] + tb.deltaNbBits) >> 16;
+        bw.add(st[ka], nba);
+        bw.add(st[kb], nbb);
+        st[ka] = w.state_table[(int32_t)(st[ka] >> nba) + ta.deltaFindState];
+        st[kb] = w.state_table[(int32_t)(st[kb] >> nbb) + tb.deltaFindState];
+        sa = na;
+        sb = nbs;
+        ii -= 2;
+    }
+    if (ii == 0) {
+        const fse::SymTT t = w.sym_tt[src[0]];
+        const uint32_t nb = (st[0] + t.deltaNbBits) >> 16;
+        bw.add(st[0], nb);
+        st[0] = w.state_table[(int32_t)(st[0] >> nb) + t.deltaFindState];
+    }
+    bw.add(st[1], tl);
+    bw.add(st[0], tl);
+    const size_t body = bw.close();
+    if (bw.overflow || body + 8 > cap - hdr) return 0;
+    const size_t total = hdr + body;
+    if (total >= n - 1) return 0;
+    hdr_out = hdr;
+    body_out = body;
+    return total;
+}
+
+// One CTA per 64 Ki block: parallel histogram, then the sequential FSE coder in thread 0 writing
+// the bitstream to an aligned scratch area, then a cooperative move into the record.
 // Writes the complete fse_enc record ([flag][u32 len][data] | [0][raw] | [2][sym]) to its slot.
 __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__restrict__ cls,
                                                           const BlockJob *__restrict__ jobs,
                                                           uint8_t *__restrict__ slots,
-                                                          unsigned long long *__restrict__ sizes) {
+                                                          unsigned long long *__restrict__ sizes,
+                                                          uint8_t *__restrict__ scratch) {
     __shared__ fse::BlockScratch w;
     const BlockJob jb = jobs[blockIdx.x];
     const uint8_t *src = cls + jb.src;
     uint8_t *out = slots + (size_t)blockIdx.x * kBlockSlot;
+    uint8_t *bits = scratch + (size_t)blockIdx.x * kBlockSlot;
     for (int s = threadIdx.x; s < 256; s += blockDim.x) w.count[s] = 0;
     __syncthreads();
     for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) atomicAdd(&w.count[src[i]], 1u);
     __syncthreads();
-    __shared__ unsigned long long r_sh;
-    if (threadIdx.x == 0) r_sh = fse::compress_block_counted(out + 5, kBlockSlot - 5, src, jb.n, w);
+    __shared__ unsigned long long r_sh, hdr_sh, body_sh;
+    if (threadIdx.x == 0) {
+        size_t h = 0, b = 0;
+        r_sh = fse_block_encode(out + 5, kBlockSlot - 5, src, jb.n, w, bits, h, b);
+        hdr_sh = h;
+        body_sh = b;
+    }
     __syncthreads();
     const unsigned long long r = r_sh;
     if (r == 0 || r >= jb.n) {  // raw
@@ -89,20 +158,26 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             out[1] = src[0];
             sizes[blockIdx.x] = 2;
         }
-    } else if (threadIdx.x == 0) {
-        out[0] = 1;
-        const uint32_t rr = (uint32_t)r;
-        out[1] = (uint8_t)rr;
-        out[2] = (uint8_t)(rr >> 8);
-        out[3] = (uint8_t)(rr >> 16);
-        out[4] = (uint8_t)(rr >> 24);
-        sizes[blockIdx.x] = 5 + r;
+    } else {
+        uint8_t *d = out + 5 + hdr_sh;
+        for (unsigned long long i = threadIdx.x; i < body_sh; i += blockDim.x) d[i] = bits[i];
+        if (threadIdx.x == 0) {
+            out[0] = 1;
+            const uint32_t rr = (uint32_t)r;
+            out[1] = (uint8_t)rr;
+            out[2] = (uint8_t)(rr >> 8);
+            out[3] = (uint8_t)(rr >> 16);
+            out[4] = (uint8_t)(rr >> 24);
+            sizes[blockIdx.x] = 5 + r;
+        }
     }
 }
 
-__global__ void __launch_bounds__(128) k_fse_decode_blocks(const uint8_t *__restrict__ in,
-                                                          const BlockJob *__restrict__ jobs,
-                                                          uint8_t *__restrict__ cls, int *__restrict__ err) {
+// One warp per 64 Ki block: the decode table lives in shared memory and lane 0 runs the two
+// interleaved state chains (zfse/fse_decompress.c FSE_decompress_usingDTable_generic).
+__global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restrict__ in,
+                                                         const BlockJob *__restrict__ jobs,
+                                                         uint8_t *__restrict__ cls, int *__restrict__ err) {
     __shared__ fse::DEntry dt[1 << fse::kMaxTableLog];
     __shared__ uint8_t sym[1 << fse::kMaxTableLog];
     const BlockJob jb = jobs[blockIdx.x];
@@ -110,12 +185,39 @@ __global__ void __launch_bounds__(128) k_fse_decode_blocks(const uint8_t *__rest
     const uint8_t *p = in + jb.in;
     if (jb.flag == 0) {
         for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) dst[i] = p[i];
-    } else if (jb.flag == 2) {
+        return;
+    }
+    if (jb.flag == 2) {
         const uint8_t v = p[0];
         for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) dst[i] = v;
-    } else if (threadIdx.x == 0) {
-        if (!fse::decompress_block(dst, jb.n, p, (size_t)jb.inlen, dt, sym)) atomicExch(err, 1);
+        return;
     }
+    if (threadIdx.x != 0) return;
+    int16_t norm[256];
+    unsigned maxSV = 255, tl = 0;
+    const size_t size = (size_t)jb.inlen;
+    const size_t hdr = fse::read_ncount(norm, &maxSV, &tl, p, size);
+    if (hdr == 0 || hdr >= size || tl > (unsigned)fse::kMaxTableLog || !fse::build_dtable(dt, norm, maxSV, tl, sym)) {
+        atomicExch(err, 1);
+        return;
+    }
+    fse::Reader32 br;
+    if (!br.init(p + hdr, (uint32_t)(size - hdr))) {
+        atomicExch(err, 1);
+        return;
+    }
+    uint32_t s0 = br.read(tl), s1 = br.read(tl);
+    const unsigned n = jb.n;
+    unsigned i = 0;
+    for (; i + 1 < n; i += 2) {
+        const fse::DEntry e0 = dt[s0];
+        const fse::DEntry e1 = dt[s1];
+        dst[i] = e0.symbol;
+        dst[i + 1] = e1.symbol;
+        s0 = e0.newState + br.read(e0.nbBits);
+        s1 = e1.newState + br.read(e1.nbBits);
+    }
+    if (i < n) dst[i] = dt[s0].symbol;
 }
 
 // Walks an fse_enc record sequence (host bytes) for n symbols starting at `off`; appends jobs.
@@ -252,8 +354,9 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     }
     BlockJob *d_jobs = h2d(pool, jobs, st);
     uint8_t *slots = pool.get<uint8_t>(jobs.size() * kBlockSlot);
+    uint8_t *bits = pool.get<uint8_t>(jobs.size() * kBlockSlot);
     unsigned long long *sizes = pool.get<unsigned long long>(jobs.size());
-    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, 0, st>>>(cls, d_jobs, slots, sizes);
+    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, 0, st>>>(cls, d_jobs, slots, sizes, bits);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
     for (size_t j = 0; j < jobs.size(); j++) {
@@ -563,26 +666,45 @@ __global__ void k_o1_norm(const uint32_t *__restrict__ hist, int total_tables, u
 __global__ void __launch_bounds__(32) k_o1_ctable(const uint16_t *__restrict__ nf, uint16_t *__restrict__ stab,
                                                  fse::SymTT *__restrict__ stt, uint8_t *__restrict__ scratch,
                                                  int *__restrict__ err) {
+    (void)scratch;
+    __shared__ uint8_t sym[O1_M];
     if (threadIdx.x != 0) return;
     const size_t t = blockIdx.x;
     int16_t norm[O1_NSYM];
     for (int s = 0; s < O1_NSYM; s++) norm[s] = (int16_t)nf[t * O1_NSYM + s];
-    if (!fse::build_ctable(stab + t * O1_M, stt + t * O1_NSYM, scratch + t * O1_M, norm, O1_NSYM - 1, O1_PB))
-        atomicExch(err, 4);
+    if (!fse::build_ctable(stab + t * O1_M, stt + t * O1_NSYM, sym, norm, O1_NSYM - 1, O1_PB)) atomicExch(err, 4);
 }
 
-__global__ void __launch_bounds__(32) k_o1_dtable(const uint16_t *__restrict__ nf, fse::DEntry *__restrict__ dt,
+// Decode table of one context with everything a decode step needs in one 32-bit word:
+//   bits 0-12 next state base, 13-16 bits to read, 17-20 context of the decoded code,
+//   bit 21 escape (value from the side stream), bits 22-31 the decoded code (signed).
+__global__ void __launch_bounds__(128) k_o1_dtable(const uint16_t *__restrict__ nf, uint32_t *__restrict__ dt,
                                                  uint8_t *__restrict__ scratch, int *__restrict__ err) {
-    if (threadIdx.x != 0) return;
+    (void)scratch;
+    __shared__ uint8_t sym[O1_M];
+    __shared__ fse::DEntry e[O1_M];
     const size_t t = blockIdx.x;
-    int16_t norm[O1_NSYM];
-    for (int s = 0; s < O1_NSYM; s++) norm[s] = (int16_t)nf[t * O1_NSYM + s];
-    if (!fse::build_dtable(dt + t * O1_M, norm, O1_NSYM - 1, O1_PB, scratch + t * O1_M)) atomicExch(err, 5);
+    if (threadIdx.x == 0) {
+        int16_t norm[O1_NSYM];
+        for (int s = 0; s < O1_NSYM; s++) norm[s] = (int16_t)nf[t * O1_NSYM + s];
+        if (!fse::build_dtable(e, norm, O1_NSYM - 1, O1_PB, sym)) atomicExch(err, 5);
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < O1_M; u += blockDim.x) {
+        const fse::DEntry d = e[u];
+        const bool esc = d.symbol == O1_NSYM - 1;
+        const int code = esc ? 0 : unzz(d.symbol);
+        const int ctx = esc ? 0 : o1_ctx(code);
+        dt[t * O1_M + u] = (uint32_t)d.newState | ((uint32_t)d.nbBits << 13) | ((uint32_t)ctx << 17) |
+                           ((uint32_t)esc << 21) | ((uint32_t)(code & 0x3FF) << 22);
+    }
 }
 
-// One thread per (segment, chunk) chain: reverse tANS encode with per-symbol context tables.
-__global__ void __launch_bounds__(128) k_o1_encode(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
-                                                  int nseg, const uint16_t *__restrict__ stab,
+// One thread per (segment, chunk) chain: reverse tANS encode with per-symbol context tables
+// (RleFseEncoder.hpp:671-707).  tab[g] selects the table set of segment g.
+__global__ void __launch_bounds__(32) k_o1_encode(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
+                                                  int nseg, const int *__restrict__ tab,
+                                                  const uint16_t *__restrict__ stab,
                                                   const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
                                                   const unsigned long long *__restrict__ slot_off,
                                                   unsigned long long *__restrict__ blen) {
@@ -598,35 +720,63 @@ __global__ void __launch_bounds__(128) k_o1_encode(const int16_t *__restrict__ q
         blen[chain] = 0;
         return;
     }
-    const size_t tb = (size_t)g * O1_NCTX;
-    fse::BitWriter bw;
+    const size_t tb = (size_t)tab[g] * O1_NCTX;
+    const uint16_t *__restrict__ S = stab + tb * O1_M;
+    const fse::SymTT *__restrict__ T = stt + tb * O1_NSYM;
+    fse::Writer32 bw;
     const unsigned long long cap = slot_off[chain + 1] - slot_off[chain];
     bw.init(slots + slot_off[chain], (size_t)cap);
-    // initial state from the last symbol of the chunk (FSE_initCState2)
     unsigned long long idx = hi - 1;
-    int prevc = idx > lo ? (int)q[idx - 1] : 0;
-    int c = o1_ctx(prevc);
-    int s = o1_sym(q[idx]);
-    fse::SymTT t = stt[(tb + c) * O1_NSYM + s];
+    int cur = q[idx];
+    int prev = idx > lo ? (int)__ldg(q + idx - 1) : 0;
+    fse::SymTT t = T[o1_ctx(prev) * O1_NSYM + o1_sym(cur)];
     uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
     uint32_t v = (nb << 16) - t.deltaNbBits;
-    uint32_t state = stab[(tb + c) * O1_M + (int32_t)(v >> nb) + t.deltaFindState];
+    uint32_t state = S[o1_ctx(prev) * O1_M + (int32_t)(v >> nb) + t.deltaFindState];
+    // walk down: the symbol at idx-1 becomes current, its predecessor is loaded one step ahead
+    int nxt = (idx >= lo + 2) ? (int)__ldg(q + idx - 2) : 0;
     while (idx > lo) {
         idx--;
-        const int cur = (int)q[idx];
-        prevc = idx > lo ? (int)q[idx - 1] : 0;
-        c = o1_ctx(prevc);
-        s = o1_sym(cur);
-        t = stt[(tb + c) * O1_NSYM + s];
+        cur = prev;
+        prev = idx > lo ? nxt : 0;
+        if (idx >= lo + 2) nxt = (int)__ldg(q + idx - 2);
+        const int c = o1_ctx(prev);
+        t = T[c * O1_NSYM + o1_sym(cur)];
         nb = (state + t.deltaNbBits) >> 16;
         bw.add(state, nb);
-        state = stab[(tb + c) * O1_M + (int32_t)(state >> nb) + t.deltaFindState];
-        bw.flush();
+        state = S[c * O1_M + (int32_t)(state >> nb) + t.deltaFindState];
     }
     bw.add(state, O1_PB);
-    bw.flush();
     const size_t len = bw.close();
     blen[chain] = bw.overflow ? ~0ULL : len;
+}
+
+// Sum of the per-segment histograms of each table region (segments [rs[r], rs[r+1])).
+__global__ void k_region_hist(const uint32_t *__restrict__ seg_hist, const int *__restrict__ rs,
+                              uint32_t *__restrict__ reg_hist) {
+    const int r = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O1_NCTX * O1_NSYM) return;
+    uint32_t s = 0;
+    for (int g = rs[r]; g < rs[r + 1]; g++) s += seg_hist[(size_t)g * O1_NCTX * O1_NSYM + i];
+    reg_hist[(size_t)r * O1_NCTX * O1_NSYM + i] = s;
+}
+
+// Flags segments whose 15 x 256 table equals the previous segment's (decode-side deduplication).
+__global__ void k_table_same(const uint8_t *__restrict__ in, const unsigned long long *__restrict__ nf_off,
+                             int nseg, int *__restrict__ same) {
+    const int g = blockIdx.x;
+    if (g >= nseg) return;
+    __shared__ int diff;
+    if (threadIdx.x == 0) diff = (g == 0);
+    __syncthreads();
+    if (g > 0) {
+        const uint8_t *a = in + nf_off[g], *b = in + nf_off[g - 1];
+        for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM * 2; i += blockDim.x)
+            if (a[i] != b[i]) diff = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) same[g] = !diff;
 }
 
 // Escape (|code| >= 128) extraction in index order: tile count + scan + scatter of zz+1 values.
@@ -679,40 +829,41 @@ struct DecChain {
     int pad;
 };
 
-__global__ void __launch_bounds__(128) k_o1_decode(const uint8_t *__restrict__ in, const DecChain *__restrict__ chains,
-                                                  int nchains, const fse::DEntry *__restrict__ dt,
-                                                  const int16_t *__restrict__ ovf, unsigned long long n_ovf,
-                                                  int16_t *__restrict__ out, int *__restrict__ err) {
+__global__ void __launch_bounds__(32) k_o1_decode(const uint8_t *__restrict__ in, const DecChain *__restrict__ chains,
+                                                 int nchains, const uint32_t *__restrict__ dt,
+                                                 const int16_t *__restrict__ ovf, unsigned long long n_ovf,
+                                                 int16_t *__restrict__ out, int *__restrict__ err) {
     const int ci = blockIdx.x * blockDim.x + threadIdx.x;
     if (ci >= nchains) return;
     const DecChain ch = chains[ci];
     if (ch.n == 0) return;
-    fse::BitReader br;
-    if (ch.inlen == 0 || !br.init(in + ch.in, (size_t)ch.inlen)) {
+    fse::Reader32 br;
+    if (ch.inlen == 0 || ch.inlen >= (1ull << 28) || !br.init(in + ch.in, (uint32_t)ch.inlen)) {
         atomicExch(err, 6);
         return;
     }
-    const fse::DEntry *tb = dt + (size_t)ch.table * O1_NCTX * O1_M;
+    const uint32_t *__restrict__ tb = dt + (size_t)ch.table * O1_NCTX * O1_M;
     uint32_t state = br.read(O1_PB);
-    int prev = 0;
-    unsigned long long oi = ch.ovf;
-    for (unsigned long long j = 0; j < ch.n; j++) {
-        const fse::DEntry e = tb[(size_t)o1_ctx(prev) * O1_M + state];
-        int code;
-        if (e.symbol == O1_NSYM - 1) {
-            if (oi >= n_ovf) {
-                atomicExch(err, 7);
-                return;
-            }
-            code = ovf[oi++];
-        } else {
-            code = unzz(e.symbol);
-        }
-        out[ch.lo + j] = (int16_t)code;
-        prev = code;
-        if (j + 1 < ch.n) state = e.newState + br.read(e.nbBits);
+    uint32_t ctx = 0;
+    const int16_t *__restrict__ ov = ovf + ch.ovf;
+    const uint32_t nov = (uint32_t)min((unsigned long long)0x7fffffff, n_ovf - ch.ovf);
+    int16_t *o = out + ch.lo;
+    const uint32_t n = (uint32_t)ch.n;
+    uint32_t oi = 0;
+    int next_ov = nov ? (int)__ldg(ov) : 0;  // escape value prefetched one step ahead
+    for (uint32_t j = 0; j < n; j++) {
+        const uint32_t e = __ldg(tb + ctx * O1_M + state);
+        const bool esc = (e >> 21) & 1u;
+        const int code = esc ? next_ov : ((int)e >> 22);
+        ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
+        oi += esc;
+        if (esc) next_ov = oi < nov ? (int)__ldg(ov + oi) : 0;
+        o[j] = (int16_t)code;
+        state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
     }
-    if (br.bitpos < 0) atomicExch(err, 8);
+    if (oi > nov) atomicExch(err, 7);
+    // the step after the last symbol reads at most 13 bits below the stream start
+    if (br.pos < -16) atomicExch(err, 8);
 }
 
 __global__ void k_m0_scatter(const uint32_t *__restrict__ runs, const uint32_t *__restrict__ vals,
@@ -743,7 +894,7 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     for (int g = 0; g < G; g++) parse_blocks(h, cls_off[g], gstart[g + 1] - gstart[g], gstart[g], jobs);
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
-    k_fse_decode_blocks<<<(unsigned)jobs.size(), 128, 0, st>>>(d, dj, cls, d_err);
+    k_fse_decode_blocks<<<(unsigned)jobs.size(), 32, 0, st>>>(d, dj, cls, d_err);
     FB2_CHECK_LAUNCH();
     unsigned long long *boff = pool.get<unsigned long long>(T + 1);
     void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
@@ -879,7 +1030,11 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         // ---- segmentation: K chains per segment, S segments (decoder reads S and K from the stream)
         const int K = std::max(1, std::min(kMaxK, tune.o1_streams));
         long long seg_target = tune.o1_segment;
-        if (seg_target <= 0) seg_target = 1LL << 18;  // 256 Ki symbols -> 16 Ki per chain
+        if (seg_target <= 0) {
+            const char *env = getenv("FALCONS_O1_SEGMENT");
+            seg_target = env ? atoll(env) : (1LL << 18);  // 256 Ki symbols -> 16 Ki per chain
+            if (seg_target < 1024) seg_target = 1024;
+        }
         long long S = std::max<long long>(1, (N + seg_target - 1) / seg_target);
         if (S > N) S = std::max<long long>(1, N);
         // every segment must be non-empty: an empty one ends after its N and K words
@@ -898,9 +1053,36 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint32_t *nvk = pool.get<uint32_t>((size_t)S * kMaxK);
         k_o1_hist<<<(unsigned)S, 1024, 0, st>>>(q, d_segs, hist, nvk);
         FB2_CHECK_LAUNCH();
-        const int ntab = (int)(S * O1_NCTX);
+        // table regions: segments whose statistics come from the same part of the code stream
+        // share one table set (tune.regions holds the code positions where statistics change)
+        std::vector<int> seg_region(S, 0), rs{0};
+        if (tune.per_segment_tables) {
+            for (long long g = 0; g < S; g++) seg_region[g] = (int)g;
+            for (long long g = 1; g <= S; g++) rs.push_back((int)g);
+        } else {
+            int prev_rr = -1;
+            for (long long g = 0; g < S; g++) {
+                int rr = 0;
+                for (long long b : tune.regions)
+                    if (b > 0 && (unsigned long long)b <= segs[g].lo) rr++;
+                if (g > 0 && rr != prev_rr) rs.push_back((int)g);
+                seg_region[g] = (int)rs.size() - 1;
+                prev_rr = rr;
+            }
+            rs.push_back((int)S);
+        }
+        const int R = (int)rs.size() - 1;
+        uint32_t *rhist = hist;
+        if (!tune.per_segment_tables) {
+            rhist = pool.get<uint32_t>((size_t)R * O1_NCTX * O1_NSYM);
+            int *d_rs = h2d(pool, rs, st);
+            k_region_hist<<<dim3((O1_NCTX * O1_NSYM + 255) / 256, R), 256, 0, st>>>(hist, d_rs, rhist);
+            FB2_CHECK_LAUNCH();
+        }
+        int *d_tab = h2d(pool, seg_region, st);
+        const int ntab = R * O1_NCTX;
         uint16_t *nf = pool.get<uint16_t>((size_t)ntab * O1_NSYM);
-        k_o1_norm<<<(ntab + 63) / 64, 64, 0, st>>>(hist, ntab, nf);
+        k_o1_norm<<<(ntab + 63) / 64, 64, 0, st>>>(rhist, ntab, nf);
         FB2_CHECK_LAUNCH();
         uint16_t *stab = pool.get<uint16_t>((size_t)ntab * O1_M);
         fse::SymTT *stt = pool.get<fse::SymTT>((size_t)ntab * O1_NSYM);
@@ -920,8 +1102,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         unsigned long long *d_soff = h2d(pool, soff, st);
         uint8_t *slots = pool.get<uint8_t>(soff.back() + 16);
         unsigned long long *blen = pool.get<unsigned long long>(nchains);
-        k_o1_encode<<<(unsigned)((nchains + 127) / 128), 128, 0, st>>>(q, d_segs, (int)S, stab, stt, slots, d_soff,
-                                                                      blen);
+        k_o1_encode<<<(unsigned)((nchains + 31) / 32), 32, 0, st>>>(q, d_segs, (int)S, d_tab, stab, stt, slots,
+                                                                      d_soff, blen);
         FB2_CHECK_LAUNCH();
         // escapes in index order
         const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
@@ -960,7 +1142,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             as.val<uint64_t>((uint64_t)K);
             for (int k = 0; k < K; k++) as.val<uint64_t>(h_blen[g * kMaxK + k]);
             for (int k = 0; k < K; k++) as.val<uint64_t>(h_nvk[g * kMaxK + k]);
-            as.dev(nf + (size_t)g * O1_NCTX * O1_NSYM, O1_NCTX * O1_NSYM * 2);
+            as.dev(nf + (size_t)seg_region[g] * O1_NCTX * O1_NSYM, O1_NCTX * O1_NSYM * 2);
             for (int k = 0; k < K; k++) as.dev(slots + soff[g * kMaxK + k], h_blen[g * kMaxK + k]);
             const unsigned long long ne = gstart[g + 1] - gstart[g];
             if (ne == 0) {
@@ -1125,21 +1307,37 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 FB2_CHECK_LAUNCH();
             }
         }
-        // decode tables
-        const int ntab = (int)(S * O1_NCTX);
+        // decode tables: consecutive segments with identical tables share one decode table set
+        std::vector<int> uid(S, 0);
+        std::vector<unsigned long long> lead;
+        {
+            std::vector<unsigned long long> nfo(nf_off.begin(), nf_off.end());
+            unsigned long long *d_nfo = h2d(pool, nfo, st);
+            int *d_same = pool.get<int>(S);
+            k_table_same<<<(unsigned)S, 256, 0, st>>>(d_in, d_nfo, (int)S, d_same);
+            FB2_CHECK_LAUNCH();
+            std::vector<int> same = d2h(d_same, (size_t)S, st);
+            for (unsigned long long g = 0; g < S; g++) {
+                if (g == 0 || !same[g]) lead.push_back(nf_off[g]);
+                uid[g] = (int)lead.size() - 1;
+            }
+        }
+        const int U = (int)lead.size();
+        const int ntab = U * O1_NCTX;
         uint16_t *nf = pool.get<uint16_t>((size_t)ntab * O1_NSYM);
         {
             std::vector<Piece> pcs;
-            for (unsigned long long g = 0; g < S; g++)
-                pcs.push_back(Piece{d_in + nf_off[g], g * O1_NCTX * O1_NSYM * 2, O1_NCTX * O1_NSYM * 2});
+            for (int u = 0; u < U; u++)
+                pcs.push_back(Piece{d_in + lead[u], (unsigned long long)u * O1_NCTX * O1_NSYM * 2, O1_NCTX * O1_NSYM * 2});
             launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(nf), st);
         }
-        fse::DEntry *dt = pool.get<fse::DEntry>((size_t)ntab * O1_M);
-        uint8_t *spread = pool.get<uint8_t>((size_t)ntab * O1_M);
-        k_o1_dtable<<<ntab, 32, 0, st>>>(nf, dt, spread, d_err);
+        uint32_t *dt = pool.get<uint32_t>((size_t)ntab * O1_M);
+        uint8_t *spread = pool.get<uint8_t>(16);
+        k_o1_dtable<<<ntab, 128, 0, st>>>(nf, dt, spread, d_err);
         FB2_CHECK_LAUNCH();
+        for (auto &c : chains) c.table = uid[c.table];
         DecChain *dch = h2d(pool, chains, st);
-        k_o1_decode<<<(unsigned)((chains.size() + 127) / 128), 128, 0, st>>>(d_in, dch, (int)chains.size(), dt, ovf,
+        k_o1_decode<<<(unsigned)((chains.size() + 31) / 32), 32, 0, st>>>(d_in, dch, (int)chains.size(), dt, ovf,
                                                                             ovf_total, d_codes, d_err);
         FB2_CHECK_LAUNCH();
     } else {

@@ -28,8 +28,11 @@ struct EntropyChoice {
 
 // Encoder-side tunables (chosen by the autotuner; defaults give ~2% table overhead).
 struct EntropyTuning {
-    long long o1_segment = 0;   // symbols per method-1 segment (0 = automatic)
-    int o1_streams = 16;        // K, 1..16
+    long long o1_segment = 0;          // symbols per method-1 segment (0 = automatic)
+    int o1_streams = 16;               // K, 1..16
+    bool per_segment_tables = false;   // one table set per segment (the reference's choice)
+    std::vector<long long> regions;    // code positions where the statistics change (level starts);
+                                       // segments of one region share a table set
 };
 
 EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cudaStream_t st);

@@ -474,6 +474,145 @@ struct BitReader {
     }
 };
 
+// Backward bit reader with a 64-bit register window, refilled by aligned 32-bit word loads
+// (fast path for device streams; same semantics as BitReader).
+struct FastReader {
+    const uint8_t *base;
+    int64_t size;      // bytes
+    int64_t pos;       // bits below the read position
+    int64_t lo;        // bit offset of win's bit 0 (multiple of 8)
+    uint64_t win;
+    __host__ __device__ __forceinline__ uint64_t load8(int64_t byte) const {
+#ifdef __CUDA_ARCH__
+        if (byte >= 0 && byte + 8 <= size) {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(base + byte);
+            const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+            const int sh = (int)(a & 3) * 8;
+            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1);
+            const uint32_t w2 = sh ? __ldg(w + 2) : 0u;
+            const uint32_t l = __funnelshift_r(w0, w1, sh), h = __funnelshift_r(w1, w2, sh);
+            return (uint64_t)l | ((uint64_t)h << 32);
+        }
+#endif
+        uint64_t v = 0;
+        for (int i = 0; i < 8; i++) {
+            const int64_t b = byte + i;
+            if (b >= 0 && b < size) v |= (uint64_t)base[b] << (8 * i);
+        }
+        return v;
+    }
+    // Loads the 64-bit window that ends at the byte boundary at or above bit p + n.
+    __host__ __device__ __forceinline__ void refill(int64_t p, unsigned n) {
+        const int64_t top = (p + (int64_t)n + 7) >> 3;
+        lo = (top - 8) * 8;
+        win = load8(top - 8);
+    }
+    __host__ __device__ bool init(const uint8_t *b, size_t sz) {
+        base = b;
+        size = (int64_t)sz;
+        lo = INT64_MAX;
+        win = 0;
+        if (sz < 1) return false;
+        const uint8_t last = b[sz - 1];
+        if (last == 0) return false;
+        pos = (int64_t)(sz - 1) * 8 + highbit32(last);
+        return true;
+    }
+    __host__ __device__ __forceinline__ uint32_t read(unsigned n) {
+        pos -= n;
+        if (pos < lo) refill(pos, n);
+        return (uint32_t)((win >> (pos - lo)) & ((1ull << n) - 1));
+    }
+};
+
+// Backward bit reader over one stream with 32-bit positions (streams shorter than 256 MiB).
+struct Reader32 {
+    const uint8_t *base;
+    int32_t size;
+    int32_t pos;
+    int32_t lo;
+    uint64_t win;
+    __device__ __forceinline__ uint64_t load8(int32_t byte) const {
+        if (byte >= 0 && byte + 8 <= size) {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(base + byte);
+            const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+            const int sh = (int)(a & 3) * 8;
+            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1);
+            const uint32_t w2 = sh ? __ldg(w + 2) : 0u;
+            return (uint64_t)__funnelshift_r(w0, w1, sh) | ((uint64_t)__funnelshift_r(w1, w2, sh) << 32);
+        }
+        uint64_t v = 0;
+        for (int i = 0; i < 8; i++) {
+            const int32_t b = byte + i;
+            if (b >= 0 && b < size) v |= (uint64_t)base[b] << (8 * i);
+        }
+        return v;
+    }
+    __device__ bool init(const uint8_t *b, uint32_t sz) {
+        base = b;
+        size = (int32_t)sz;
+        lo = 0x7fffffff;
+        win = 0;
+        if (sz < 1) return false;
+        const uint8_t last = b[sz - 1];
+        if (last == 0) return false;
+        pos = (int32_t)(sz - 1) * 8 + (int32_t)highbit32(last);
+        return true;
+    }
+    __device__ __forceinline__ uint32_t read(unsigned n) {
+        pos -= (int32_t)n;
+        if (pos < lo) {
+            const int32_t top = (pos + (int32_t)n + 7) >> 3;
+            lo = (top - 8) * 8;
+            win = load8(top - 8);
+        }
+        return (uint32_t)(win >> (pos - lo)) & ((1u << n) - 1u);
+    }
+};
+
+// Forward bit writer that stores whole little-endian 32-bit words to a 4-byte aligned buffer.
+struct Writer32 {
+    uint32_t *out;
+    uint32_t cap_words;
+    uint32_t nw;        // words stored
+    uint64_t acc;
+    uint32_t nb;
+    bool overflow;
+    __device__ void init(uint8_t *b, size_t cap) {
+        out = reinterpret_cast<uint32_t *>(b);
+        cap_words = (uint32_t)(cap / 4);
+        nw = 0;
+        acc = 0;
+        nb = 0;
+        overflow = false;
+    }
+    __device__ __forceinline__ void add(uint32_t v, unsigned n) {
+        acc |= (uint64_t)(v & ((n >= 32) ? 0xffffffffu : ((1u << n) - 1u))) << nb;
+        nb += n;
+        if (nb >= 32) {
+            if (nw < cap_words) out[nw] = (uint32_t)acc;
+            else overflow = true;
+            nw++;
+            acc >>= 32;
+            nb -= 32;
+        }
+    }
+    // Appends the end mark; returns the byte length (BIT_closeCStream).
+    __device__ size_t close() {
+        add(1, 1);
+        size_t bytes = (size_t)nw * 4;
+        uint8_t *ob = reinterpret_cast<uint8_t *>(out);
+        while (nb > 0) {
+            if (bytes < (size_t)cap_words * 4) ob[bytes] = (uint8_t)acc;
+            else overflow = true;
+            bytes++;
+            acc >>= 8;
+            nb = nb > 8 ? nb - 8 : 0;
+        }
+        return bytes;
+    }
+};
+
 }  // namespace fse
 }  // namespace fb2
 

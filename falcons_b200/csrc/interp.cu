@@ -294,6 +294,7 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
         }
         const int li = (int)P.levels.size();
         P.levels.push_back(QParams{cur, 2 * cur, 1.0 / (2 * cur), p.radius});
+        P.level_starts.push_back(b.pos);
         const long long s = 1LL << (level - 1);
         if (p.tuning || N == 4) b.tuning_level(li, s);
         else b.disabled_level(li, s, level == 1);

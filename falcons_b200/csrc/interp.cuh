@@ -57,6 +57,7 @@ struct InterpPlan {
     int first_point;        // anchor-free field: element 0 is quantized against 0 first
     std::vector<QParams> levels;      // index 0: first point (constructor reciprocal), then one per level
     std::vector<PassLaunch> passes;   // in stream order
+    std::vector<long long> level_starts;  // first code position of every level (statistics change there)
 };
 
 // Builds the pass plan; throws std::invalid_argument for unsupported parameters.

@@ -157,7 +157,9 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             as.bytes(hdr.data(), hdr.size());
             as.dev(unpred, (size_t)n_unpred * sizeof(T));
             as.val<uint64_t>((uint64_t)plan.n_codes);
-            entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st);
+            EntropyTuning tune;
+            tune.regions = plan.level_starts;
+            entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st, tune);
             if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
             payload = as.run_framed(pool, d_pay, st);
             c.cmprAlgo = ALGO_INTERP;
