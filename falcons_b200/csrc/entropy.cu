@@ -751,6 +751,228 @@ __global__ void __launch_bounds__(32) k_o1_encode(const int16_t *__restrict__ q,
     blen[chain] = bw.overflow ? ~0ULL : len;
 }
 
+struct DecChain {
+    unsigned long long in;      // stream byte offset
+    unsigned long long inlen;   // stream length (0 = empty chunk)
+    unsigned long long lo, n;   // output range
+    unsigned long long ovf;     // first escape value of this chunk
+    int table;                  // segment index (tables at table * 15)
+    int pad;
+};
+
+// ---- shared-memory resident context tables
+// A CTA encodes or decodes chains that share one table set; the tables of the contexts that carry
+// most symbols are staged in shared memory (the rest are read from global memory).  `map` packs,
+// per context, its shared-memory slot (4 bits, 15 = not resident); `rev` packs the context of
+// every slot.
+constexpr int kEncSlots = 13;  // 13 x 8192 x u16 encode state tables = 208 KiB
+constexpr int kDecSlots = 7;   // 7 x 8192 x u32 decode tables = 224 KiB
+struct ChainCta {
+    int table;
+    int first;
+    int count;
+    int pad;
+    unsigned long long map, rev;
+};
+
+__global__ void __launch_bounds__(64) k_o1_encode_smem(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
+                                                      const ChainCta *__restrict__ ctas,
+                                                      const uint16_t *__restrict__ stab,
+                                                      const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
+                                                      const unsigned long long *__restrict__ slot_off,
+                                                      unsigned long long *__restrict__ blen) {
+    extern __shared__ uint4 smem_raw[];
+    uint16_t *sst = reinterpret_cast<uint16_t *>(smem_raw);
+    const ChainCta w = ctas[blockIdx.x];
+    const size_t tb = (size_t)w.table * O1_NCTX;
+    const uint16_t *__restrict__ S = stab + tb * O1_M;
+    const fse::SymTT *__restrict__ T = stt + tb * O1_NSYM;
+    for (int j = 0; j < kEncSlots; j++) {
+        const int c = (int)((w.rev >> (4 * j)) & 15);
+        if (c >= O1_NCTX) continue;
+        const uint4 *src = reinterpret_cast<const uint4 *>(S + (size_t)c * O1_M);
+        uint4 *dst = reinterpret_cast<uint4 *>(sst + (size_t)j * O1_M);
+        for (int i = threadIdx.x; i < O1_M * 2 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x >= w.count) return;
+    const int chain = w.first + threadIdx.x;
+    const int g = chain / kMaxK, k = chain % kMaxK;
+    const SegInfo sg = segs[g];
+    if (k >= sg.K) return;
+    const unsigned long long lo = sg.lo + (unsigned long long)k * sg.cs;
+    unsigned long long hi = lo + sg.cs;
+    if (hi > sg.lo + sg.n) hi = sg.lo + sg.n;
+    if (lo >= hi) {
+        blen[chain] = 0;
+        return;
+    }
+    const unsigned long long map = w.map;
+    fse::Writer32 bw;
+    const unsigned long long cap = slot_off[chain + 1] - slot_off[chain];
+    bw.init(slots + slot_off[chain], (size_t)cap);
+    auto stlookup = [&](int c, int idx) -> uint32_t {
+        const int sl = (int)((map >> (4 * c)) & 15);
+        return sl < kEncSlots ? sst[sl * O1_M + idx] : __ldg(S + (size_t)c * O1_M + idx);
+    };
+    // codes are read through a 6-deep register queue (Q[i] = q[idx - i]) and the symbol transform
+    // of the next step is loaded during the current one, so no step waits on global memory
+    const long long L0 = (long long)lo;
+    long long idx = (long long)hi - 1;
+    auto ld = [&](long long i) -> int { return i >= L0 ? (int)__ldg(q + i) : 0; };
+    int Q0 = ld(idx), Q1 = ld(idx - 1), Q2 = ld(idx - 2), Q3 = ld(idx - 3), Q4 = ld(idx - 4), Q5 = ld(idx - 5);
+    int c = o1_ctx(idx > L0 ? Q1 : 0);
+    fse::SymTT t = T[c * O1_NSYM + o1_sym(Q0)];
+    uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
+    uint32_t v = (nb << 16) - t.deltaNbBits;
+    uint32_t state = stlookup(c, (int32_t)(v >> nb) + t.deltaFindState);
+    // advance to idx - 1
+    Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
+    idx--;
+    int cn = o1_ctx(idx > L0 ? Q1 : 0);
+    fse::SymTT tn = idx >= L0 ? T[cn * O1_NSYM + o1_sym(Q0)] : t;
+    while (idx >= L0) {
+        c = cn;
+        t = tn;
+        // prefetch for idx - 1
+        const int n0 = Q1, n1 = Q2;
+        cn = o1_ctx(idx - 1 > L0 ? n1 : 0);
+        if (idx - 1 >= L0) tn = T[cn * O1_NSYM + o1_sym(n0)];
+        nb = (state + t.deltaNbBits) >> 16;
+        bw.add(state, nb);
+        state = stlookup(c, (int32_t)(state >> nb) + t.deltaFindState);
+        Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
+        idx--;
+    }
+    bw.add(state, O1_PB);
+    const size_t len = bw.close();
+    blen[chain] = bw.overflow ? ~0ULL : len;
+}
+
+__global__ void __launch_bounds__(64) k_o1_decode_smem(const uint8_t *__restrict__ in,
+                                                      const DecChain *__restrict__ chains,
+                                                      const ChainCta *__restrict__ ctas,
+                                                      const uint32_t *__restrict__ dt,
+                                                      const int16_t *__restrict__ ovf, unsigned long long n_ovf,
+                                                      int16_t *__restrict__ out, int *__restrict__ err) {
+    extern __shared__ uint4 smem_raw[];
+    uint32_t *sdt = reinterpret_cast<uint32_t *>(smem_raw);
+    const ChainCta w = ctas[blockIdx.x];
+    const uint32_t *__restrict__ tb = dt + (size_t)w.table * O1_NCTX * O1_M;
+    for (int j = 0; j < kDecSlots; j++) {
+        const int c = (int)((w.rev >> (4 * j)) & 15);
+        if (c >= O1_NCTX) continue;
+        const uint4 *src = reinterpret_cast<const uint4 *>(tb + (size_t)c * O1_M);
+        uint4 *dst = reinterpret_cast<uint4 *>(sdt + (size_t)j * O1_M);
+        for (int i = threadIdx.x; i < O1_M * 4 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x >= w.count) return;
+    const DecChain ch = chains[w.first + threadIdx.x];
+    if (ch.n == 0) return;
+    fse::ReaderPF br;
+    const uint8_t *sb = in + ch.in;
+    if (ch.inlen == 0 || ch.inlen >= (1ull << 28) || !br.init(sb, (uint32_t)ch.inlen)) {
+        atomicExch(err, 6);
+        return;
+    }
+    const unsigned long long map = w.map;
+    uint32_t state = br.read(O1_PB);
+    uint32_t ctx = 0;
+    const int16_t *__restrict__ ov = ovf + ch.ovf;
+    const uint32_t nov = (uint32_t)min((unsigned long long)0x7fffffff, n_ovf - ch.ovf);
+    int16_t *o = out + ch.lo;
+    const uint32_t n = (uint32_t)ch.n;
+    uint32_t oi = 0;
+    // escape values queued two deep, so each load has several steps to arrive
+    int q0 = nov > 0 ? (int)__ldg(ov) : 0;
+    int q1 = nov > 1 ? (int)__ldg(ov + 1) : 0;
+    for (uint32_t j = 0; j < n; j++) {
+        const uint32_t sl = (uint32_t)(map >> (4 * ctx)) & 15u;
+        const uint32_t e = sl < (uint32_t)kDecSlots ? sdt[sl * O1_M + state] : __ldg(tb + ctx * O1_M + state);
+        const bool esc = (e >> 21) & 1u;
+        const int code = esc ? q0 : ((int)e >> 22);
+        ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
+        if (esc) {
+            oi++;
+            q0 = q1;
+            q1 = oi + 1 < nov ? (int)__ldg(ov + oi + 1) : 0;
+        }
+        o[j] = (int16_t)code;
+        state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
+    }
+    if (oi > nov) atomicExch(err, 7);
+    if (br.pos < br.start_bit(sb) - 16) atomicExch(err, 8);
+}
+
+// Context frequencies of one table set: the stationary distribution of the context chain implied
+// by the normalized tables (the next context is a function of the decoded code; escapes split
+// between the two large-magnitude contexts).  Returns (map, rev) for `slots` resident tables.
+std::pair<unsigned long long, unsigned long long> hot_contexts(const uint16_t *nf, int slots) {
+    double P[O1_NCTX][O1_NCTX] = {};
+    for (int c = 0; c < O1_NCTX; c++) {
+        for (int s = 0; s < O1_NSYM; s++) {
+            int f = (int16_t)nf[c * O1_NSYM + s];
+            if (f < 0) f = 1;
+            if (f == 0) continue;
+            const double pr = f / (double)O1_M;
+            if (s == O1_NSYM - 1) {
+                P[c][13] += pr / 2;
+                P[c][14] += pr / 2;
+            } else {
+                P[c][o1_ctx(unzz(s))] += pr;
+            }
+        }
+    }
+    double pi[O1_NCTX], nx[O1_NCTX];
+    for (int c = 0; c < O1_NCTX; c++) pi[c] = 1.0 / O1_NCTX;
+    for (int it = 0; it < 200; it++) {
+        for (int c = 0; c < O1_NCTX; c++) nx[c] = 0;
+        for (int a = 0; a < O1_NCTX; a++)
+            for (int b = 0; b < O1_NCTX; b++) nx[b] += pi[a] * P[a][b];
+        double sum = 0;
+        for (int c = 0; c < O1_NCTX; c++) sum += nx[c];
+        for (int c = 0; c < O1_NCTX; c++) pi[c] = sum > 0 ? nx[c] / sum : 1.0 / O1_NCTX;
+    }
+    int order[O1_NCTX];
+    for (int c = 0; c < O1_NCTX; c++) order[c] = c;
+    std::sort(order, order + O1_NCTX, [&](int a, int b) { return pi[a] > pi[b]; });
+    unsigned long long map = ~0ULL, rev = ~0ULL;
+    for (int j = 0; j < slots && j < O1_NCTX; j++) {
+        const int c = order[j];
+        map &= ~(15ULL << (4 * c));
+        map |= (unsigned long long)j << (4 * c);
+        rev &= ~(15ULL << (4 * j));
+        rev |= (unsigned long long)c << (4 * j);
+    }
+    return {map, rev};
+}
+
+// CTAs of up to 64 consecutive chains that share a table set.
+std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std::vector<unsigned long long> &maps,
+                                 const std::vector<unsigned long long> &revs) {
+    std::vector<ChainCta> out;
+    size_t i = 0;
+    while (i < chain_table.size()) {
+        const int t = chain_table[i];
+        size_t j = i;
+        while (j < chain_table.size() && chain_table[j] == t && j - i < 64) j++;
+        out.push_back(ChainCta{t, (int)i, (int)(j - i), 0, maps[t], revs[t]});
+        i = j;
+    }
+    return out;
+}
+
+void enable_big_smem() {
+    static bool done = false;
+    if (done) return;
+    FB2_CUDA(cudaFuncSetAttribute(k_o1_encode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kEncSlots * O1_M * 2));
+    FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kDecSlots * O1_M * 4));
+    done = true;
+}
+
 // Sum of the per-segment histograms of each table region (segments [rs[r], rs[r+1])).
 __global__ void k_region_hist(const uint32_t *__restrict__ seg_hist, const int *__restrict__ rs,
                               uint32_t *__restrict__ reg_hist) {
@@ -820,14 +1042,7 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_extract(const int16_t *__r
     }
 }
 
-struct DecChain {
-    unsigned long long in;      // stream byte offset
-    unsigned long long inlen;   // stream length (0 = empty chunk)
-    unsigned long long lo, n;   // output range
-    unsigned long long ovf;     // first escape value of this chunk
-    int table;                  // segment index (tables at table * 15)
-    int pad;
-};
+
 
 __global__ void __launch_bounds__(32) k_o1_decode(const uint8_t *__restrict__ in, const DecChain *__restrict__ chains,
                                                  int nchains, const uint32_t *__restrict__ dt,
@@ -1102,9 +1317,23 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         unsigned long long *d_soff = h2d(pool, soff, st);
         uint8_t *slots = pool.get<uint8_t>(soff.back() + 16);
         unsigned long long *blen = pool.get<unsigned long long>(nchains);
-        k_o1_encode<<<(unsigned)((nchains + 31) / 32), 32, 0, st>>>(q, d_segs, (int)S, d_tab, stab, stt, slots,
-                                                                      d_soff, blen);
-        FB2_CHECK_LAUNCH();
+        {
+            std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
+            std::vector<unsigned long long> maps(R), revs(R);
+            for (int r = 0; r < R; r++) {
+                auto mr = hot_contexts(hnf.data() + (size_t)r * O1_NCTX * O1_NSYM, kEncSlots);
+                maps[r] = mr.first;
+                revs[r] = mr.second;
+            }
+            std::vector<int> chain_table((size_t)nchains);
+            for (long long ch = 0; ch < nchains; ch++) chain_table[ch] = seg_region[ch / kMaxK];
+            std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
+            ChainCta *d_ctas = h2d(pool, ctas, st);
+            enable_big_smem();
+            k_o1_encode_smem<<<(unsigned)ctas.size(), 64, kEncSlots * O1_M * 2, st>>>(q, d_segs, d_ctas, stab, stt, slots,
+                                                                                   d_soff, blen);
+            FB2_CHECK_LAUNCH();
+        }
         // escapes in index order
         const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
         uint32_t *tcnt = pool.get<uint32_t>(tiles + 2);
@@ -1337,9 +1566,23 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         FB2_CHECK_LAUNCH();
         for (auto &c : chains) c.table = uid[c.table];
         DecChain *dch = h2d(pool, chains, st);
-        k_o1_decode<<<(unsigned)((chains.size() + 31) / 32), 32, 0, st>>>(d_in, dch, (int)chains.size(), dt, ovf,
-                                                                            ovf_total, d_codes, d_err);
-        FB2_CHECK_LAUNCH();
+        {
+            std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
+            std::vector<unsigned long long> maps(U), revs(U);
+            for (int u = 0; u < U; u++) {
+                auto mr = hot_contexts(hnf.data() + (size_t)u * O1_NCTX * O1_NSYM, kDecSlots);
+                maps[u] = mr.first;
+                revs[u] = mr.second;
+            }
+            std::vector<int> chain_table(chains.size());
+            for (size_t i = 0; i < chains.size(); i++) chain_table[i] = chains[i].table;
+            std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
+            ChainCta *d_ctas = h2d(pool, ctas, st);
+            enable_big_smem();
+            k_o1_decode_smem<<<(unsigned)ctas.size(), 64, kDecSlots * O1_M * 4, st>>>(d_in, dch, d_ctas, dt, ovf,
+                                                                                   ovf_total, d_codes, d_err);
+            FB2_CHECK_LAUNCH();
+        }
     } else {
         throw std::invalid_argument("unsupported entropy method");
     }

@@ -570,6 +570,46 @@ struct Reader32 {
     }
 };
 
+// Backward bit reader for long-running chains: the stream is read as aligned 32-bit words
+// (words sharing bytes with neighbouring data are harmless: those bits are never returned for a
+// valid stream) and the next two words are prefetched, so a refill never waits on memory.
+struct ReaderPF {
+    const uint32_t *w;   // aligned word base
+    int32_t pos;         // bit position (relative to w) below which bits are unread
+    int32_t lo;          // bit offset of win's bit 0 (multiple of 32)
+    uint64_t win;
+    uint32_t p1, p2;     // words lo/32 - 1 and lo/32 - 2
+    __device__ __forceinline__ uint32_t word(int32_t i) const { return i >= 0 ? __ldg(w + i) : 0u; }
+    __device__ bool init(const uint8_t *b, uint32_t sz) {
+        if (sz < 1) return false;
+        const uint8_t last = b[sz - 1];
+        if (last == 0) return false;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(b);
+        w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+        pos = (int32_t)(a & 3) * 8 + (int32_t)(sz - 1) * 8 + (int32_t)highbit32(last);
+        const int32_t top = pos >> 5;
+        lo = (top - 1) * 32;
+        win = ((uint64_t)word(top) << 32) | word(top - 1);
+        p1 = word(top - 2);
+        p2 = word(top - 3);
+        return true;
+    }
+    __device__ __forceinline__ uint32_t read(unsigned n) {
+        pos -= (int32_t)n;
+        if (pos < lo) {
+            win = (win << 32) | p1;
+            lo -= 32;
+            p1 = p2;
+            p2 = word((lo >> 5) - 2);
+        }
+        return (uint32_t)(win >> (pos - lo)) & ((1u << n) - 1u);
+    }
+    // bits consumed beyond the stream start (0 for a fully consumed valid stream)
+    __device__ __forceinline__ int32_t start_bit(const uint8_t *b) const {
+        return (int32_t)(reinterpret_cast<uintptr_t>(b) & 3) * 8;
+    }
+};
+
 // Forward bit writer that stores whole little-endian 32-bit words to a 4-byte aligned buffer.
 struct Writer32 {
     uint32_t *out;
