@@ -49,6 +49,7 @@ EXPORTS = [
     "falcons_compress_size_bound", "falcons_compress", "falcons_read_config", "falcons_decompress",
     "falcons_compress_device", "falcons_decompress_device", "falcons_interp_compress",
     "falcons_interp_decompress", "falcons_device_range", "falcons_encode_codes", "falcons_decode_codes",
+    "falcons_interp_decompress_noalloc",
 ]
 
 

@@ -11,6 +11,7 @@
 #include "context.cuh"
 #include "interp.cuh"
 #include "pipeline.cuh"
+#include "static_scratch.cuh"
 
 struct falcons_ctx {
     fb2::Context c;
@@ -159,6 +160,36 @@ int falcons_interp_decompress(falcons_ctx *ctx, int dtype, const size_t *dims, i
             fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred),
                                            static_cast<double *>(d_out), ws, st);
         if (!stream) FB2_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int falcons_interp_decompress_noalloc(int dtype, const size_t *dims, int N, const falcons_interp_params *p,
+                                      const int16_t *d_codes, size_t n_codes, const void *d_unpred,
+                                      size_t n_unpred, void *d_out, void *stream) {
+    return guarded([&] {
+        check_dtype(dtype);
+        if (!dims || !d_out || !d_codes) throw std::invalid_argument("null pointer");
+        long long d[4];
+        for (int i = 0; i < N && i < 4; i++) d[i] = (long long)dims[i];
+        const fb2::InterpPlan plan = fb2::make_plan(d, N, to_params(p));
+        if ((long long)n_codes != plan.n_codes) throw std::invalid_argument("code count does not match the field");
+        if ((long long)n_unpred < plan.n_anchor) throw std::invalid_argument("unpredictable list too short");
+        const int es = dtype == FALCONS_DTYPE_F32 ? 4 : 8;
+        const size_t need = fb2::interp_workspace_bytes(plan, es);
+        if (need > (size_t)FALCONS_NOALLOC_SCRATCH_BYTES)
+            throw std::invalid_argument("falcons_interp_decompress_noalloc: this field needs " + std::to_string(need) +
+                                        " bytes of scratch, more than the " +
+                                        std::to_string((size_t)FALCONS_NOALLOC_SCRATCH_BYTES) +
+                                        " static bytes (FALCONS_NOALLOC_SCRATCH_BYTES); use "
+                                        "falcons_interp_decompress for fields this large");
+        void *ws = fb2::static_scratch_current_device();
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        if (dtype == FALCONS_DTYPE_F32)
+            fb2::interp_decompress<float>(plan, d_codes, static_cast<const float *>(d_unpred),
+                                          static_cast<float *>(d_out), ws, st);
+        else
+            fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred),
+                                           static_cast<double *>(d_out), ws, st);
     });
 }
 

@@ -738,6 +738,37 @@ void device_range(const T *d_x, long long n, T *d_out, void *d_ws, cudaStream_t 
     FB2_CHECK_LAUNCH();
 }
 
+namespace {
+template <class T>
+cudaError_t preload_decompress_kernels() {
+    const void *fns[] = {
+        reinterpret_cast<const void *>(&k_anchors<T, true>),
+        reinterpret_cast<const void *>(&k_esc_scatter<T, true>),
+        reinterpret_cast<const void *>(&k_first_point<T, true>),
+        reinterpret_cast<const void *>(&k_pass<T, KIND_ROW, true>),
+        reinterpret_cast<const void *>(&k_pass<T, KIND_LINE, true>),
+        reinterpret_cast<const void *>(&k_pass<T, KIND_GENERIC, true>),
+        reinterpret_cast<const void *>(&k_pass<T, KIND_LEGACY, true>),
+    };
+    for (const void *f : fns) {
+        cudaFuncAttributes a;
+        const cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t interp_decompress_preload() {
+    for (const void *f : {reinterpret_cast<const void *>(&k_esc_count), reinterpret_cast<const void *>(&k_scan_u32)}) {
+        cudaFuncAttributes a;
+        const cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+    }
+    const cudaError_t e = preload_decompress_kernels<float>();
+    return e != cudaSuccess ? e : preload_decompress_kernels<double>();
+}
+
 template void interp_compress<float>(const InterpPlan &, float *, int16_t *, float *, void *, unsigned long long *,
                                      cudaStream_t);
 template void interp_compress<double>(const InterpPlan &, double *, int16_t *, double *, void *,

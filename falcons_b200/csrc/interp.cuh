@@ -74,6 +74,11 @@ template <class T>
 void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, T *d_x, void *d_ws,
                        cudaStream_t st);
 
+// Loads, on the current device, every kernel interp_decompress can launch (float and double).
+// Under lazy module loading a kernel is otherwise loaded at its first launch, which can allocate
+// device memory for its code; calling this once up front moves that cost out of later calls.
+cudaError_t interp_decompress_preload();
+
 // max - min over a device array, result left on the device (T) and optionally returned.
 template <class T>
 void device_range(const T *d_x, long long n, T *d_out_range, void *d_ws, cudaStream_t st);

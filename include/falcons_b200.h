@@ -119,6 +119,36 @@ int falcons_encode_codes(falcons_ctx *ctx, const int16_t *d_codes, size_t n, voi
                          size_t *out_len, void *stream);
 int falcons_decode_codes(falcons_ctx *ctx, const void *d_in, size_t len, size_t n, int16_t *d_codes, void *stream);
 
+/* ---- allocation-free decompress (no counterpart in the reference) ----
+ *
+ * falcons_interp_decompress without a context and without any device allocation: the same
+ * kernels, with their scratch in a static device region of FALCONS_NOALLOC_SCRATCH_BYTES per
+ * device instead of the context's work buffers.  It is for callers that cannot let a library
+ * allocate device memory: an application that hands nearly all of HBM to its own pool at
+ * start-up leaves cudaMalloc nothing to give, and a latency-bound decode thread cannot absorb
+ * cudaFree's implicit device-wide synchronisation or a work buffer's first-use growth.
+ *
+ * - Limit: the field's scratch (about 4 bytes per code for float, 8 for double, plus 12 bytes per
+ *   4096 codes) must fit in FALCONS_NOALLOC_SCRATCH_BYTES (64 MiB: about 16.7 million float or
+ *   8.3 million double codes).  Larger fields are rejected with FALCONS_EINVAL and a message
+ *   giving the size needed; use falcons_interp_decompress for them.
+ * - Device and stream: works on the CURRENT device; `stream` is a cudaStream_t of that device
+ *   (NULL: the default stream).  The call is asynchronous: d_out is complete when the stream's
+ *   work is.
+ * - Set-up: the first call on a device (with that device current) resolves the scratch address
+ *   and loads the decompress kernels there, which reserves the region; make that first call
+ *   before any stream capture begins.  Later calls allocate nothing.
+ * - Nothing in the scratch has to start at zero: every word the call reads, it wrote earlier in
+ *   the same call.
+ * - Overlapping calls race: all calls on a device share the one region, so two calls whose work
+ *   overlaps in time (on different streams, or from different threads) corrupt each other's
+ *   scratch.  Issue them on one stream, or make each call's stream wait for the previous call.
+ * Arguments and results are those of falcons_interp_decompress. */
+#define FALCONS_NOALLOC_SCRATCH_BYTES (64u << 20)
+int falcons_interp_decompress_noalloc(int dtype, const size_t *dims, int N, const falcons_interp_params *p,
+                                      const int16_t *d_codes, size_t n_codes, const void *d_unpred,
+                                      size_t n_unpred, void *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
