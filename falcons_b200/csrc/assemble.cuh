@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <stdexcept>
 #include <vector>
@@ -53,6 +54,21 @@ T *h2d(Pool &pool, const std::vector<T> &h, cudaStream_t st) {
 
 inline unsigned grid_for(long long n, int threads, long long cap = 1 << 20) {
     return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, cap));
+}
+
+// Number of SMs of the current device (cached per device).
+inline int sm_count() {
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    FB2_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return 148;
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        FB2_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        if (v <= 0) v = 148;
+        cache[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
 }
 
 struct Piece {

@@ -2,6 +2,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <stdexcept>
@@ -76,6 +79,21 @@ void check_dtype(int dtype) {
 namespace fb2 {
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long count_launch() { return ++g_launches; }
+
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+Trace::Trace(const char *w) : what(w), t0(0), l0(0), on(std::getenv("FALCONS_TRACE") != nullptr) {
+    if (on) {
+        t0 = now_ms();
+        l0 = g_launches.load();
+    }
+}
+void Trace::mark(const char *label) {
+    if (on)
+        std::fprintf(stderr, "[falcons trace] %s %-28s +%8.3f ms  launches %llu\n", what, label, now_ms() - t0,
+                     g_launches.load() - l0);
+}
 }  // namespace fb2
 
 extern "C" {

@@ -30,6 +30,18 @@ struct cuda_error : std::runtime_error {
 
 // Every kernel launch of the library is followed by FB2_CHECK_LAUNCH(), which also counts it.
 unsigned long long count_launch();
+
+// Host-side phase trace, on when the environment variable FALCONS_TRACE is set: each mark()
+// prints to stderr the host time since the traced call began and the kernel launches so far.
+// A long gap between two marks with few launches is host work the GPU waited for.
+struct Trace {
+    const char *what;
+    double t0;
+    unsigned long long l0;
+    bool on;
+    explicit Trace(const char *w);
+    void mark(const char *label);
+};
 #define FB2_CHECK_LAUNCH()      \
     do {                        \
         ::fb2::count_launch();  \

@@ -301,6 +301,13 @@ __global__ void k_gamma_pack(const uint32_t *__restrict__ v, const uint8_t *__re
     }
 }
 
+// out[i] = src[idx[i]]
+__global__ void k_pick_u64(const unsigned long long *__restrict__ src, const unsigned long long *__restrict__ idx,
+                           long long n, unsigned long long *__restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = src[idx[i]];
+}
+
 GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
                       cudaStream_t st) {
     const int G = (int)gstart.size() - 1;
@@ -318,16 +325,12 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     unsigned long long *boff = pool.get<unsigned long long>(T + 1);
     void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
     exclusive_scan<uint8_t, unsigned long long>(cls, T, boff, sc, st);
-    // per-group bit totals
-    std::vector<unsigned long long> gb(G + 1);
-    {
-        std::vector<unsigned long long> hb(G + 1);
-        for (int g = 0; g <= G; g++) {
-            FB2_CUDA(cudaMemcpyAsync(&hb[g], boff + gstart[g], 8, cudaMemcpyDeviceToHost, st));
-        }
-        FB2_CUDA(cudaStreamSynchronize(st));
-        gb = hb;
-    }
+    // per-group bit totals: the scan at every group start, gathered on the device, one copy back
+    unsigned long long *d_gstart = h2d(pool, gstart, st);
+    unsigned long long *d_gb = pool.get<unsigned long long>(G + 1);
+    k_pick_u64<<<grid_for(G + 1, 256), 256, 0, st>>>(boff, d_gstart, G + 1, d_gb);
+    FB2_CHECK_LAUNCH();
+    const std::vector<unsigned long long> gb = d2h(d_gb, (size_t)G + 1, st);
     std::vector<unsigned long long> gword(G);
     unsigned long long words = 0;
     for (int g = 0; g < G; g++) {
@@ -338,7 +341,6 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     }
     uint32_t *wbuf = pool.get<uint32_t>(words + 4);
     FB2_CUDA(cudaMemsetAsync(wbuf, 0, (words + 4) * 4, st));
-    unsigned long long *d_gstart = h2d(pool, gstart, st);
     unsigned long long *d_gword = h2d(pool, gword, st);
     k_gamma_pack<<<grid_for(T, 256), 256, 0, st>>>(d_vals, cls, boff, T, d_gstart, G, d_gword, wbuf);
     FB2_CHECK_LAUNCH();
@@ -765,6 +767,15 @@ struct DecChain {
 // most symbols are staged in shared memory (the rest are read from global memory).  `map` packs,
 // per context, its shared-memory slot (4 bits, 15 = not resident); `rev` packs the context of
 // every slot.
+// A chain CTA holds up to 64 chains that share one table set (kept in shared memory, so one CTA
+// fills an SM).  The chains are spread over all 8 warps, 8 lanes each, so that every scheduler of
+// the SM has two warps of independent chain steps to interleave.
+constexpr int kChainThreads = 256;
+constexpr int kMaxChainsPerCta = 64;
+__device__ __forceinline__ int chain_slot() {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    return lane < kMaxChainsPerCta / (kChainThreads / 32) ? lane * (kChainThreads / 32) + warp : -1;
+}
 constexpr int kEncSlots = 13;  // 13 x 8192 x u16 encode state tables = 208 KiB
 constexpr int kDecSlots = 7;   // 7 x 8192 x u32 decode tables = 224 KiB
 struct ChainCta {
@@ -775,7 +786,7 @@ struct ChainCta {
     unsigned long long map, rev;
 };
 
-__global__ void __launch_bounds__(64) k_o1_encode_smem(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
+__global__ void __launch_bounds__(kChainThreads) k_o1_encode_smem(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
                                                       const ChainCta *__restrict__ ctas,
                                                       const uint16_t *__restrict__ stab,
                                                       const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
@@ -795,8 +806,9 @@ __global__ void __launch_bounds__(64) k_o1_encode_smem(const int16_t *__restrict
         for (int i = threadIdx.x; i < O1_M * 2 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
     }
     __syncthreads();
-    if ((int)threadIdx.x >= w.count) return;
-    const int chain = w.first + threadIdx.x;
+    const int lc = chain_slot();
+    if (lc < 0 || lc >= w.count) return;
+    const int chain = w.first + lc;
     const int g = chain / kMaxK, k = chain % kMaxK;
     const SegInfo sg = segs[g];
     if (k >= sg.K) return;
@@ -849,7 +861,7 @@ __global__ void __launch_bounds__(64) k_o1_encode_smem(const int16_t *__restrict
     blen[chain] = bw.overflow ? ~0ULL : len;
 }
 
-__global__ void __launch_bounds__(64) k_o1_decode_smem(const uint8_t *__restrict__ in,
+__global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t *__restrict__ in,
                                                       const DecChain *__restrict__ chains,
                                                       const ChainCta *__restrict__ ctas,
                                                       const uint32_t *__restrict__ dt,
@@ -867,8 +879,9 @@ __global__ void __launch_bounds__(64) k_o1_decode_smem(const uint8_t *__restrict
         for (int i = threadIdx.x; i < O1_M * 4 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
     }
     __syncthreads();
-    if ((int)threadIdx.x >= w.count) return;
-    const DecChain ch = chains[w.first + threadIdx.x];
+    const int lc = chain_slot();
+    if (lc < 0 || lc >= w.count) return;
+    const DecChain ch = chains[w.first + lc];
     if (ch.n == 0) return;
     fse::ReaderPF br;
     const uint8_t *sb = in + ch.in;
@@ -949,14 +962,18 @@ std::pair<unsigned long long, unsigned long long> hot_contexts(const uint16_t *n
 }
 
 // CTAs of up to 64 consecutive chains that share a table set.
+// Groups consecutive chains of one table into CTAs of at most `per` chains; `per` is chosen so
+// that the CTAs cover the SMs once (one chain CTA fills an SM).
 std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std::vector<unsigned long long> &maps,
                                  const std::vector<unsigned long long> &revs) {
     std::vector<ChainCta> out;
+    const size_t sms = (size_t)sm_count();
+    const size_t per = std::max<size_t>(8, std::min<size_t>(kMaxChainsPerCta, (chain_table.size() + sms - 1) / sms));
     size_t i = 0;
     while (i < chain_table.size()) {
         const int t = chain_table[i];
         size_t j = i;
-        while (j < chain_table.size() && chain_table[j] == t && j - i < 64) j++;
+        while (j < chain_table.size() && chain_table[j] == t && j - i < per) j++;
         out.push_back(ChainCta{t, (int)i, (int)(j - i), 0, maps[t], revs[t]});
         i = j;
     }
@@ -1185,6 +1202,7 @@ EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cud
 
 void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, size_t n, const EntropyChoice &ch,
                          cudaStream_t st, const EntropyTuning &tune) {
+    Trace tr("encode");
     const long long N = (long long)n;
     const int16_t *q = d_codes_in;
     if (ch.delta && N > 0) {
@@ -1319,6 +1337,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         unsigned long long *blen = pool.get<unsigned long long>(nchains);
         {
             std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
+            tr.mark("tables normalized");
             std::vector<unsigned long long> maps(R), revs(R);
             for (int r = 0; r < R; r++) {
                 auto mr = hot_contexts(hnf.data() + (size_t)r * O1_NCTX * O1_NSYM, kEncSlots);
@@ -1330,9 +1349,10 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
             ChainCta *d_ctas = h2d(pool, ctas, st);
             enable_big_smem();
-            k_o1_encode_smem<<<(unsigned)ctas.size(), 64, kEncSlots * O1_M * 2, st>>>(q, d_segs, d_ctas, stab, stt, slots,
+            k_o1_encode_smem<<<(unsigned)ctas.size(), kChainThreads, kEncSlots * O1_M * 2, st>>>(q, d_segs, d_ctas, stab, stt, slots,
                                                                                    d_soff, blen);
             FB2_CHECK_LAUNCH();
+            tr.mark("chains launched");
         }
         // escapes in index order
         const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
@@ -1348,6 +1368,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         std::vector<unsigned long long> h_blen = d2h(blen, (size_t)nchains, st);
         std::vector<int> h_err = d2h(d_err, 1, st);
         if (h_err[0]) throw std::runtime_error("tANS table construction failed");
+        tr.mark("chains done");
         unsigned long long E = 0;
         std::vector<unsigned long long> gstart(S + 1, 0);
         for (long long g = 0; g < S; g++) {
@@ -1363,6 +1384,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             FB2_CHECK_LAUNCH();
         }
         GammaOut go = gamma_encode(pool, evals, gstart, st);
+        tr.mark("escapes coded");
         for (auto b : h_blen)
             if (b == ~0ULL) throw std::runtime_error("tANS chain overflow");
         as.val<uint64_t>((uint64_t)S);
@@ -1408,6 +1430,7 @@ size_t entropy_encode(Context &ctx, const int16_t *d_codes, size_t n, const Entr
 size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size_t n, int16_t *d_codes,
                       cudaStream_t st) {
     (void)ctx;
+    Trace tr("decode");
     Pool pool(st);
     const size_t len = h.len;
     size_t off = 0;
@@ -1508,6 +1531,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         }
         for (unsigned long long g = 0; g < S; g++)
             if (nf_off[g] + O1_NCTX * O1_NSYM * 2 > len) throw std::invalid_argument("truncated tANS tables");
+        tr.mark("segments parsed");
         // escape values
         int16_t *ovf = pool.get<int16_t>(ovf_total + 1);
         {
@@ -1536,6 +1560,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 FB2_CHECK_LAUNCH();
             }
         }
+        tr.mark("escapes launched");
         // decode tables: consecutive segments with identical tables share one decode table set
         std::vector<int> uid(S, 0);
         std::vector<unsigned long long> lead;
@@ -1568,6 +1593,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         DecChain *dch = h2d(pool, chains, st);
         {
             std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
+            tr.mark("decode tables built");
             std::vector<unsigned long long> maps(U), revs(U);
             for (int u = 0; u < U; u++) {
                 auto mr = hot_contexts(hnf.data() + (size_t)u * O1_NCTX * O1_NSYM, kDecSlots);
@@ -1579,15 +1605,17 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
             std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
             ChainCta *d_ctas = h2d(pool, ctas, st);
             enable_big_smem();
-            k_o1_decode_smem<<<(unsigned)ctas.size(), 64, kDecSlots * O1_M * 4, st>>>(d_in, dch, d_ctas, dt, ovf,
+            k_o1_decode_smem<<<(unsigned)ctas.size(), kChainThreads, kDecSlots * O1_M * 4, st>>>(d_in, dch, d_ctas, dt, ovf,
                                                                                    ovf_total, d_codes, d_err);
             FB2_CHECK_LAUNCH();
         }
     } else {
         throw std::invalid_argument("unsupported entropy method");
     }
+    tr.mark("chains launched");
     if (delta) undelta(pool, d_codes, N, st);
     std::vector<int> he = d2h(d_err, 1, st);
+    tr.mark("chains done");
     if (he[0]) throw std::invalid_argument("Invalid or corrupted Falcons entropy payload");
     return off;
 }

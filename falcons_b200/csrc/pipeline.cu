@@ -99,10 +99,12 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
                      falcons_config *conf_out, cudaStream_t st, const T *h_data) {
     (void)h_data;
     falcons_config c = in_conf;
+    Trace tr("compress");
     normalize_dims(c);
     c.openmp = 0;  // serial stream format
     if (c.quantbinCnt <= 0 || c.quantbinCnt > 65536) throw std::invalid_argument("QuantizationBinTotal must be in [2, 65536]");
     resolve_error_bound<T>(ctx, c, d_x, st);
+    tr.mark("error bound resolved");
     if (c.absErrorBound == 0) c.cmprAlgo = ALGO_LOSSLESS;
     if (c.cmprAlgo == ALGO_LORENZO_REG || c.cmprAlgo == ALGO_NOPRED)
         throw std::invalid_argument("unsupported on GPU build: ALGO_LORENZO_REG and ALGO_NOPRED are not implemented");
@@ -130,7 +132,9 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
             unsigned long long *nesc = pool.get<unsigned long long>(2);
             interp_compress<T>(plan, d_x, codes, unpred, ws, nesc, st);
+            tr.mark("interpolation launched");
             const EntropyChoice ch = choose_entropy(ctx, codes, (size_t)plan.n_codes, st);  // syncs: nesc ready
+            tr.mark("entropy method chosen");
             unsigned long long h_nesc = 0;
             FB2_CUDA(cudaMemcpyAsync(&h_nesc, nesc, 8, cudaMemcpyDeviceToHost, st));
             FB2_CUDA(cudaStreamSynchronize(st));
@@ -160,8 +164,10 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             EntropyTuning tune;
             tune.regions = plan.level_starts;
             entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st, tune);
+            tr.mark("entropy stage launched");
             if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
             payload = as.run_framed(pool, d_pay, st);
+            tr.mark("payload assembled");
             c.cmprAlgo = ALGO_INTERP;
         } catch (std::length_error &) {
             // FalconsDispatcher.hpp:100-118: downgrade to lossless when the buffer is too small
@@ -206,6 +212,7 @@ struct Payload {
 
 template <class T>
 void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_out, cudaStream_t st) {
+    Trace tr("decompress");
     Pool pool(st);
     const uint64_t L = pl.L;
     const ByteView &view = pl.view;
@@ -257,10 +264,13 @@ void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_ou
     const uint64_t n_codes = view.rd<uint64_t>(off);
     if ((long long)n_codes != plan.n_codes) throw std::invalid_argument("code count does not match the field");
     int16_t *codes = pool.get<int16_t>((size_t)n_codes + 16);
+    tr.mark("headers parsed");
     entropy_decode(ctx, d_flat + off, view.sub(off), (size_t)n_codes, codes, st);
+    tr.mark("entropy stage launched");
     void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
     interp_decompress<T>(plan, codes, unpred, d_out, ws, st);
     FB2_CUDA(cudaStreamSynchronize(st));
+    tr.mark("reconstructed");
 }
 
 // Lossless payload [u64 L][zstd frame(s)] held in host memory at hp (plen bytes).
