@@ -262,8 +262,9 @@ def main():
         peak, peak_src = 6650.0, "fallback"
     achieved = alg_bytes / (pq_ms / 1e3) / 1e9
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(tpath):
+    # DRAM bytes of one prediction + quantization stage, from an ncu capture of the same workload
+    tpath = os.path.join(ROOT, "profiles", f"pq_stage_{args.size}cube_f32_traffic.json")
+    if os.path.exists(tpath) and args.rel == 1e-4:
         try:
             traffic = json.load(open(tpath)).get("interp_compress_bytes_per_launch")
         except Exception:

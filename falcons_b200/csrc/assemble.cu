@@ -226,6 +226,15 @@ size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
         host_pieces.push_back(out.size());
         add_host(idx.data(), idx.size(), total);
         total += idx.size();
+        for (size_t i = 0; i < tail.size(); i++) {
+            if (tail[i].src == nullptr) {
+                host_pieces.push_back(out.size());
+                add_host(tail_host.data() + tail_off[i], tail[i].len, total + tail[i].dst);
+            } else {
+                out.push_back(Piece{tail[i].src, total + tail[i].dst, tail[i].len});
+            }
+        }
+        total += tail_len;
     }
     uint8_t *dh = h2d(pool, hb, st);
     for (size_t i : host_pieces) out[i].src = dh + reinterpret_cast<uintptr_t>(out[i].src);

@@ -131,11 +131,31 @@ struct Assembler {
     void val(T v) {
         bytes(&v, sizeof(T));
     }
+    // Bytes written after the index frame (further skippable frames): host bytes or device pieces.
+    std::vector<Piece> tail;                 // src == nullptr: host bytes at tail_host + tail_off
+    std::vector<uint8_t> tail_host;
+    std::vector<size_t> tail_off;
+    unsigned long long tail_len = 0;
+    void tail_bytes(const void *p, size_t n) {
+        if (!n) return;
+        tail_off.push_back(tail_host.size());
+        tail_host.insert(tail_host.end(), static_cast<const uint8_t *>(p), static_cast<const uint8_t *>(p) + n);
+        tail.push_back(Piece{nullptr, tail_len, n});
+        tail_len += n;
+    }
+    void tail_dev(const void *src, size_t n) {
+        if (!n) return;
+        tail_off.push_back(0);
+        tail.push_back(Piece{static_cast<const uint8_t *>(src), tail_len, n});
+        tail_len += n;
+    }
     // Copies the logical layout to d_out[0, pos).  Synchronizes the stream.
     void run(Pool &pool, uint8_t *d_out, cudaStream_t st);
     // Writes [u64 pos][zstd raw-block frame of the layout] to d_out; returns the bytes written.
     size_t run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st);
-    size_t framed_size() const { return 8 + zstd_raw_frame_size(pos) + (with_index ? index_frame().size() : 0); }
+    size_t framed_size() const {
+        return 8 + zstd_raw_frame_size(pos) + (with_index ? index_frame().size() + tail_len : 0);
+    }
 };
 
 // Logical bytes [0, len) stored either flat or as the content of a raw-block zstd frame.

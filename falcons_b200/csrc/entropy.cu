@@ -54,6 +54,8 @@ struct BlockJob {
     unsigned flag;            // decode side: 0 raw, 1 FSE, 2 RLE
     unsigned long long in;    // decode side: offset of the payload (after flag / length)
     unsigned long long inlen; // decode side: payload length
+    unsigned ck = 0xFFFFFFFFu; // decode side: first checkpoint of the block (none: all ones)
+    unsigned pad = 0;
 };
 
 constexpr size_t kBlockSlot = FBLK + 64;
@@ -61,106 +63,269 @@ constexpr size_t kBlockSlot = FBLK + 64;
 // FSE_compress on the device: header, tables and the 2-state reverse coding of one 64 Ki block
 // (zfse/fse_compress.c FSE_compress_wksp).  The two state chains are interleaved and the symbol
 // loads are issued ahead of the dependent table lookups.
-__device__ size_t fse_block_encode(uint8_t *dst, size_t cap, const uint8_t *__restrict__ src, size_t n,
-                                   fse::BlockScratch &w, uint8_t *__restrict__ bits, size_t &hdr_out,
-                                   size_t &body_out) {
-    if (n <= 2) return 0;
-    unsigned maxSV = 255;
-    while (maxSV > 0 && w.count[maxSV] == 0) maxSV--;
-    uint32_t maxCount = 0;
-    for (unsigned s2 = 0; s2 <= maxSV; s2++) maxCount = w.count[s2] > maxCount ? w.count[s2] : maxCount;
-    if (maxCount == n) return 1;
-    if (maxCount == 1) return 0;
-    if (maxCount < (n >> 7)) return 0;
-    const unsigned tl = fse::optimal_table_log(fse::kDefaultTableLog, n, maxSV);
-    if (fse::normalize_count(w.norm, tl, w.count, n, maxSV) != tl) return 0;
-    if (cap < fse::ncount_bound(maxSV, tl) + 16) return 0;
-    const size_t hdr = fse::write_ncount(dst, w.norm, maxSV, tl);
-    if (hdr == 0) return 0;
-    if (!fse::build_ctable(w.state_table, w.sym_tt, w.sym, w.norm, maxSV, tl)) return 0;
-    fse::Writer32 bw;
-    bw.init(bits, cap - hdr);
-    uint32_t st[2];
-    for (int k = 0; k < 2; k++) {
-        const size_t i = ((n - 1) % 2 == (size_t)k) ? n - 1 : n - 2;
-        const fse::SymTT t = w.sym_tt[src[i]];
-        const uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
-        const uint32_t v = (nb << 16) - t.deltaNbBits;
-        st[k] = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
-    }
-    // symbols n-3 .. 0 in that order; index parity selects the state
-    long long ii = (long long)n - 3;
-    uint8_t sa = ii >= 1 ? src[ii] : 0, sb = ii >= 1 ? src[ii - 1] : 0;
-    while (ii >= 1) {
-        const uint8_t na = ii >= 3 ? src[ii - 2] : 0, nbs = ii >= 3 ? src[ii - 3] : 0;  // next pair, early
-        const fse::SymTT ta = w.sym_tt[sa], tb = w.sym_tt[sb];
-        const int ka = (int)(ii & 1), kb = ka ^ 1;
-        const uint32_t nba = (st[ka] + ta.deltaNbBits) >> 16;
-        const uint32_t nbb = (st[kb] + tb.deltaNbBits) >> 16;
-        bw.add(st[ka], nba);
-        bw.add(st[kb], nbb);
-        st[ka] = w.state_table[(int32_t)(st[ka] >> nba) + ta.deltaFindState];
-        st[kb] = w.state_table[(int32_t)(st[kb] >> nbb) + tb.deltaFindState];
-        sa = na;
-        sb = nbs;
-        ii -= 2;
-    }
-    if (ii == 0) {
-        const fse::SymTT t = w.sym_tt[src[0]];
-        const uint32_t nb = (st[0] + t.deltaNbBits) >> 16;
-        bw.add(st[0], nb);
-        st[0] = w.state_table[(int32_t)(st[0] >> nb) + t.deltaFindState];
-    }
-    bw.add(st[1], tl);
-    bw.add(st[0], tl);
-    const size_t body = bw.close();
-    if (bw.overflow || body + 8 > cap - hdr) return 0;
-    const size_t total = hdr + body;
-    if (total >= n - 1) return 0;
-    hdr_out = hdr;
-    body_out = body;
-    return total;
+// Decode checkpoint of an FSE block (two interleaved states): the decoder's bit position and both
+// states just before it decodes symbol q * part (q >= 1).  Recorded by the encoder, stored in the
+// stream's checkpoint frame, so that one block decodes as independent parts.
+struct FseCkpt {
+    uint32_t bitpos;
+    uint16_t s0, s1;
+};
+
+// Decode checkpoint of a tANS chain: before the decoder decodes index lo + q * part (q >= 1), its
+// bit position in the chain's stream, its state, the context (of the previous code) and the number
+// of escapes the chain has consumed.  Recorded by the encoder into the stream's checkpoint frame.
+struct O1Ckpt {
+    uint32_t bitpos;
+    uint32_t esc;
+    uint16_t state;
+    uint16_t ctx;
+};
+
+// Checkpoints of an n-symbol FSE block: one before every symbol q * part <= n - 3, q >= 1 (the
+// last two symbols only initialise the encoder states).
+__host__ __device__ __forceinline__ uint32_t fse_ckpt_count(uint32_t n, uint32_t part) {
+    return n >= 3 ? (n - 3) / part : 0;
 }
 
-// One CTA per 64 Ki block: parallel histogram, then the sequential FSE coder in thread 0 writing
-// the bitstream to an aligned scratch area, then a cooperative move into the record.
-// Writes the complete fse_enc record ([flag][u32 len][data] | [0][raw] | [2][sym]) to its slot.
+// FSE class block encoder (zfse/fse_compress.c FSE_compress), one CTA per 64 Ki-symbol block.
+// The histogram is parallel; thread 0 normalizes and writes the table header; the CTA builds the
+// coding tables in shared memory (the state table with warp match ranks, the symbol transforms
+// per symbol); thread 0 then runs the two interleaved state chains (symbols
+// n-3 .. 0, each coded by the state of its index parity), recording for every symbol its emitted
+// bits and their count instead of packing them; the CTA then packs in parallel: a block scan of
+// the bit counts gives every symbol its bit position, each thread writes the bits of one run of
+// symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends the two final
+// states and the end mark.  (The chains of these skewed class streams converge too slowly for a
+// speculative split.)  Writes the complete fse_enc record ([1][u32 len][data] | [0][raw] |
+// [2][sym]) to the block's slot; the record flag goes into bits 56-63 of `sizes`.  `recs` is
+// scratch of FBLK words per block.
+constexpr unsigned kFseMaxLog = 11;               // the block coder's table log never exceeds 11
+struct FseSmem {
+    uint32_t count[256];
+    uint32_t cumul[257];
+    uint32_t scan[256];
+    fse::SymTT sym_tt[256];
+    int16_t norm[256];
+    uint16_t state_table[1 << kFseMaxLog];
+    uint8_t sym[1 << kFseMaxLog];
+};
+
 __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__restrict__ cls,
                                                           const BlockJob *__restrict__ jobs,
                                                           uint8_t *__restrict__ slots,
                                                           unsigned long long *__restrict__ sizes,
-                                                          uint8_t *__restrict__ scratch) {
-    __shared__ fse::BlockScratch w;
+                                                          uint8_t *__restrict__ scratch, uint32_t part,
+                                                          FseCkpt *__restrict__ cks, uint32_t *__restrict__ recs) {
+    __shared__ FseSmem w;
+    __shared__ int s_mode;  // 0 raw, 1 RLE, 2 FSE
+    __shared__ unsigned s_tl, s_hdr, s_s0, s_s1, s_maxsv, s_i0, s_i1;
+    uint32_t *s_scan = w.scan;
     const BlockJob jb = jobs[blockIdx.x];
     const uint8_t *src = cls + jb.src;
     uint8_t *out = slots + (size_t)blockIdx.x * kBlockSlot;
-    uint8_t *bits = scratch + (size_t)blockIdx.x * kBlockSlot;
+    uint32_t *bw = reinterpret_cast<uint32_t *>(scratch + (size_t)blockIdx.x * kBlockSlot);
+    uint32_t *rec = recs + (size_t)blockIdx.x * FBLK;
+    FseCkpt *ck = cks ? cks + (size_t)blockIdx.x * (FBLK / part) : nullptr;
+    const unsigned n = jb.n;
     for (int s = threadIdx.x; s < 256; s += blockDim.x) w.count[s] = 0;
     __syncthreads();
-    for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) atomicAdd(&w.count[src[i]], 1u);
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&w.count[src[i]], 1u);
     __syncthreads();
-    __shared__ unsigned long long r_sh, hdr_sh, body_sh;
     if (threadIdx.x == 0) {
-        size_t h = 0, b = 0;
-        r_sh = fse_block_encode(out + 5, kBlockSlot - 5, src, jb.n, w, bits, h, b);
-        hdr_sh = h;
-        body_sh = b;
+        int mode = 0;
+        unsigned tl = 0, hdr = 0, maxSV = 255;
+        if (n > 2) {
+            while (maxSV > 0 && w.count[maxSV] == 0) maxSV--;
+            uint32_t maxCount = 0;
+            for (unsigned s2 = 0; s2 <= maxSV; s2++) maxCount = w.count[s2] > maxCount ? w.count[s2] : maxCount;
+            if (maxCount == n) {
+                mode = 1;
+            } else if (maxCount > 1 && maxCount >= (n >> 7)) {
+                tl = fse::optimal_table_log(fse::kDefaultTableLog, n, maxSV);
+                if (tl <= kFseMaxLog && fse::normalize_count(w.norm, tl, w.count, n, maxSV) == tl &&
+                    kBlockSlot - 5 >= fse::ncount_bound(maxSV, tl) + 16) {
+                    hdr = (unsigned)fse::write_ncount(out + 5, w.norm, maxSV, tl);
+                    if (hdr && fse::spread(w.sym, w.norm, maxSV, tl)) {
+                        mode = 2;
+                        w.cumul[0] = 0;
+                        for (unsigned u = 1; u <= maxSV + 1; u++)
+                            w.cumul[u] = w.cumul[u - 1] + (w.norm[u - 1] == -1 ? 1u : (uint32_t)w.norm[u - 1]);
+                    }
+                }
+            }
+        }
+        s_mode = mode;
+        s_tl = tl;
+        s_hdr = hdr;
+        s_maxsv = maxSV;
     }
     __syncthreads();
-    const unsigned long long r = r_sh;
-    if (r == 0 || r >= jb.n) {  // raw
+    if (s_mode == 2) {
+        const unsigned tl = s_tl, L = 1u << tl, maxSV = s_maxsv;
+        // state table: the cells of every symbol in increasing order (match ranks within a warp)
+        if (threadIdx.x < 32) {
+            const unsigned lane = threadIdx.x;
+            for (unsigned u0 = 0; u0 < L; u0 += 32) {
+                const unsigned u = u0 + lane;
+                const unsigned sy = u < L ? w.sym[u] : 256u + lane;
+                const unsigned peers = __match_any_sync(0xffffffffu, sy);
+                const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+                if (u < L) w.state_table[w.cumul[sy] + rank] = (uint16_t)(L + u);
+                __syncwarp();
+                if (u < L && rank == (unsigned)__popc(peers) - 1u) w.cumul[sy] += rank + 1;
+                __syncwarp();
+            }
+        }
+        for (unsigned sy = threadIdx.x; sy <= maxSV; sy += blockDim.x) {
+            const int nn = w.norm[sy];
+            uint32_t total = 0;  // cells of the symbols before sy
+            for (unsigned s2 = 0; s2 < sy; s2++) total += w.norm[s2] == -1 ? 1u : (uint32_t)max(0, (int)w.norm[s2]);
+            if (nn == 0) {
+                w.sym_tt[sy].deltaNbBits = ((tl + 1) << 16) - L;
+                w.sym_tt[sy].deltaFindState = 0;
+            } else if (nn == -1 || nn == 1) {
+                w.sym_tt[sy].deltaNbBits = (tl << 16) - L;
+                w.sym_tt[sy].deltaFindState = (int32_t)total - 1;
+            } else {
+                const uint32_t maxBitsOut = tl - fse::highbit32((uint32_t)(nn - 1));
+                const uint32_t minStatePlus = (uint32_t)nn << maxBitsOut;
+                w.sym_tt[sy].deltaNbBits = (maxBitsOut << 16) - minStatePlus;
+                w.sym_tt[sy].deltaFindState = (int32_t)total - nn;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // the two chains; rec[n - 3 - i] = emitted bits of symbol i | their count << 16
+            uint32_t st[2];
+            for (int k = 0; k < 2; k++) {
+                const unsigned i = ((n - 1) % 2 == (unsigned)k) ? n - 1 : n - 2;
+                const fse::SymTT t = w.sym_tt[src[i]];
+                const uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
+                const uint32_t v = (nb << 16) - t.deltaNbBits;
+                st[k] = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
+            }
+            const uint32_t smask = L - 1;
+            const int ka = (int)((n - 3) & 1);
+            uint32_t sA = st[ka], sB = st[ka ^ 1];
+            s_i0 = st[0] & smask;  // the states before symbols n-3 and n-4 (for checkpoints next to them)
+            s_i1 = st[1] & smask;
+            // pairs (ii, ii - 1), A codes the first.  rec is indexed in emission order
+            // (e = n - 3 - i): emitted bits (bits 0-15), their count (16-20) and the decoder's state
+            // after the symbol (21-31, table log <= 11), from which the pack step takes the
+            // checkpoint states.  (A plain loop: unrolled, prefetching or branching forms measured
+            // slower.)
+            long long ii = (long long)n - 3;
+            for (; ii >= 1; ii -= 2) {
+                const fse::SymTT ta = w.sym_tt[src[ii]], tb = w.sym_tt[src[ii - 1]];
+                const uint32_t nba = (sA + ta.deltaNbBits) >> 16;
+                const uint32_t nbb = (sB + tb.deltaNbBits) >> 16;
+                const uint32_t xa = w.state_table[(int32_t)(sA >> nba) + ta.deltaFindState];
+                const uint32_t xb = w.state_table[(int32_t)(sB >> nbb) + tb.deltaFindState];
+                rec[(long long)n - 3 - ii] = (sA & ((1u << nba) - 1u)) | (nba << 16) | ((xa & smask) << 21);
+                rec[(long long)n - 2 - ii] = (sB & ((1u << nbb) - 1u)) | (nbb << 16) | ((xb & smask) << 21);
+                sA = xa;
+                sB = xb;
+            }
+            if (ii == 0) {  // n - 3 even: symbol 0 belongs to state A
+                const fse::SymTT t = w.sym_tt[src[0]];
+                const uint32_t nb = (sA + t.deltaNbBits) >> 16;
+                const uint32_t xa = w.state_table[(int32_t)(sA >> nb) + t.deltaFindState];
+                rec[n - 3] = (sA & ((1u << nb) - 1u)) | (nb << 16) | ((xa & smask) << 21);
+                sA = xa;
+            }
+            st[ka] = sA;
+            st[ka ^ 1] = sB;
+            s_s0 = st[0];
+            s_s1 = st[1];
+        }
+    }
+    __syncthreads();
+    int mode = s_mode;
+    size_t body = 0;
+    if (mode == 2) {
+        const unsigned tl = s_tl;
+        // symbols n-3 .. 0 in emission order; thread t owns emission positions [t*per, (t+1)*per)
+        const unsigned ns = n - 2, per = (ns + blockDim.x - 1) / blockDim.x;
+        const unsigned e0 = min(ns, threadIdx.x * per), e1 = min(ns, e0 + per);
+        uint32_t cnt = 0;
+        for (unsigned e = e0; e < e1; e++) cnt += (rec[e] >> 16) & 31u;
+        s_scan[threadIdx.x] = cnt;
+        __syncthreads();
+        uint32_t off = 0;
+        for (unsigned j = 0; j < threadIdx.x; j++) off += s_scan[j];
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_scan[0] = off + cnt;  // bits of all symbols
+        __syncthreads();
+        const uint32_t sym_bits = s_scan[0];
+        const uint32_t total = sym_bits + 2 * tl + 1;
+        body = (total + 7) / 8;
+        if (body + 8 > kBlockSlot - 5 - s_hdr || s_hdr + body >= n - 1) mode = 0;  // not worth coding: raw
+        if (mode == 2) {
+            if (e1 > e0) bw[off >> 5] = 0u;
+            if (threadIdx.x == 0) bw[sym_bits >> 5] = 0u;
+        }
+        __syncthreads();
+        if (mode == 2) {
+            const unsigned lastw = (off + cnt) >> 5;
+            uint32_t wi = off >> 5, accn = off & 31u;
+            uint64_t acc = 0;
+            bool first = true;
+            auto flush_word = [&](uint32_t v) {
+                if (first || wi == lastw) atomicOr(bw + wi, v);
+                else bw[wi] = v;
+                first = false;
+            };
+            uint32_t pos = off;
+            for (unsigned e = e0; e < e1; e++) {
+                const unsigned i = n - 3 - e;
+                const uint32_t r = rec[e], nb = (r >> 16) & 31u;
+                acc |= (uint64_t)(r & 0xFFFFu) << accn;
+                accn += nb;
+                pos += nb;
+                if (ck && i > 0 && (i & (part - 1)) == 0) {
+                    // decoder states before symbol i: after symbol i (even chain), after i + 1 (odd)
+                    const uint32_t odd = i + 1 <= n - 3 ? rec[e - 1] >> 21 : ((n - 2) & 1 ? s_i1 : s_i0);
+                    ck[i / part - 1] = FseCkpt{pos, (uint16_t)(r >> 21), (uint16_t)odd};
+                }
+                if (accn >= 32) {
+                    flush_word((uint32_t)acc);
+                    wi++;
+                    acc >>= 32;
+                    accn -= 32;
+                }
+            }
+            if (e1 > e0 && accn > 0) atomicOr(bw + wi, (uint32_t)acc);
+            __syncthreads();
+            if (threadIdx.x == 0) {  // final states (odd, then even) and the end mark
+                uint32_t p2 = sym_bits;
+                auto put = [&](uint32_t v, uint32_t nb) {
+                    for (uint32_t b = 0; b < nb; b++, p2++)
+                        if ((v >> b) & 1u) atomicOr(bw + (p2 >> 5), 1u << (p2 & 31u));
+                };
+                if ((sym_bits & 31u) == 0) bw[sym_bits >> 5] = 0u;
+                for (uint32_t z = (sym_bits >> 5) + 1; z <= (total - 1) >> 5; z++) bw[z] = 0u;
+                put(s_s1 & ((1u << tl) - 1), tl);
+                put(s_s0 & ((1u << tl) - 1), tl);
+                put(1u, 1u);
+            }
+        }
+        __syncthreads();
+    }
+    if (mode == 0) {  // raw
         if (threadIdx.x == 0) out[0] = 0;
-        for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) out[1 + i] = src[i];
-        if (threadIdx.x == 0) sizes[blockIdx.x] = 1 + jb.n;
-    } else if (r == 1) {  // a single repeated symbol
+        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) out[1 + i] = src[i];
+        if (threadIdx.x == 0) sizes[blockIdx.x] = 1 + n;  // flag 0
+    } else if (mode == 1) {  // a single repeated symbol
         if (threadIdx.x == 0) {
             out[0] = 2;
             out[1] = src[0];
-            sizes[blockIdx.x] = 2;
+            sizes[blockIdx.x] = 2 | (2ULL << 56);
         }
     } else {
-        uint8_t *d = out + 5 + hdr_sh;
-        for (unsigned long long i = threadIdx.x; i < body_sh; i += blockDim.x) d[i] = bits[i];
+        const size_t r = s_hdr + body;
+        uint8_t *d = out + 5 + s_hdr;
+        const uint8_t *bb = reinterpret_cast<const uint8_t *>(bw);
+        for (size_t i = threadIdx.x; i < body; i += blockDim.x) d[i] = bb[i];
         if (threadIdx.x == 0) {
             out[0] = 1;
             const uint32_t rr = (uint32_t)r;
@@ -168,18 +333,24 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             out[2] = (uint8_t)(rr >> 8);
             out[3] = (uint8_t)(rr >> 16);
             out[4] = (uint8_t)(rr >> 24);
-            sizes[blockIdx.x] = 5 + r;
+            sizes[blockIdx.x] = (5 + r) | (1ULL << 56);
         }
     }
 }
 
-// One warp per 64 Ki block: the decode table lives in shared memory and lane 0 runs the two
-// interleaved state chains (zfse/fse_decompress.c FSE_decompress_usingDTable_generic).
+// One warp per 64 Ki block: lane 0 reads the table header and builds the decode table in shared
+// memory (zfse/fse_decompress.c FSE_buildDTable), then the block decodes either as one sequence
+// (lane 0, two interleaved states, FSE_decompress_usingDTable_generic) or, when the stream carries
+// checkpoints for it, as independent parts of `part` symbols, one per lane, each starting from its
+// checkpoint and verified against the next one (a mismatch sets err[1] and the caller decodes again
+// without checkpoints).
 __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restrict__ in,
                                                          const BlockJob *__restrict__ jobs,
-                                                         uint8_t *__restrict__ cls, int *__restrict__ err) {
+                                                         uint8_t *__restrict__ cls, int *__restrict__ err,
+                                                         uint32_t part, const FseCkpt *__restrict__ cks) {
     __shared__ fse::DEntry dt[1 << fse::kMaxTableLog];
     __shared__ uint8_t sym[1 << fse::kMaxTableLog];
+    __shared__ unsigned tl_sh, hdr_sh;
     const BlockJob jb = jobs[blockIdx.x];
     uint8_t *dst = cls + jb.src;
     const uint8_t *p = in + jb.in;
@@ -192,32 +363,61 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
         for (unsigned i = threadIdx.x; i < jb.n; i += blockDim.x) dst[i] = v;
         return;
     }
-    if (threadIdx.x != 0) return;
-    int16_t norm[256];
-    unsigned maxSV = 255, tl = 0;
     const size_t size = (size_t)jb.inlen;
-    const size_t hdr = fse::read_ncount(norm, &maxSV, &tl, p, size);
-    if (hdr == 0 || hdr >= size || tl > (unsigned)fse::kMaxTableLog || !fse::build_dtable(dt, norm, maxSV, tl, sym)) {
-        atomicExch(err, 1);
-        return;
+    if (threadIdx.x == 0) {
+        int16_t norm[256];
+        unsigned maxSV = 255, tl = 0;
+        const size_t hdr = fse::read_ncount(norm, &maxSV, &tl, p, size);
+        const bool ok = hdr != 0 && hdr < size && tl <= (unsigned)fse::kMaxTableLog &&
+                        fse::build_dtable(dt, norm, maxSV, tl, sym);
+        tl_sh = ok ? tl : 0xFFFFFFFFu;
+        hdr_sh = (unsigned)hdr;
+        if (!ok) atomicExch(err, 1);
     }
-    fse::Reader32 br;
-    if (!br.init(p + hdr, (uint32_t)(size - hdr))) {
-        atomicExch(err, 1);
-        return;
-    }
-    uint32_t s0 = br.read(tl), s1 = br.read(tl);
+    __syncwarp();
+    const unsigned tl = tl_sh;
+    if (tl == 0xFFFFFFFFu) return;
+    const uint8_t *sp = p + hdr_sh;
+    const uint32_t ssz = (uint32_t)(size - hdr_sh);
     const unsigned n = jb.n;
-    unsigned i = 0;
-    for (; i + 1 < n; i += 2) {
-        const fse::DEntry e0 = dt[s0];
-        const fse::DEntry e1 = dt[s1];
-        dst[i] = e0.symbol;
-        dst[i + 1] = e1.symbol;
-        s0 = e0.newState + br.read(e0.nbBits);
-        s1 = e1.newState + br.read(e1.nbBits);
+    const unsigned nparts = jb.ck == 0xFFFFFFFFu ? 1u : 1u + fse_ckpt_count(n, part);
+    for (unsigned q = threadIdx.x; q < nparts; q += blockDim.x) {
+        fse::ReaderPF br;
+        uint32_t s0, s1;
+        const unsigned start = q * (nparts > 1 ? part : 0u);
+        const unsigned end = q + 1 < nparts ? start + part : n;
+        if (q == 0) {
+            if (!br.init(sp, ssz)) {
+                atomicExch(err, 1);
+                continue;
+            }
+            s0 = br.read(tl);
+            s1 = br.read(tl);
+        } else {
+            const FseCkpt c = cks[jb.ck + q - 1];
+            if (c.bitpos >= ssz * 8u || (c.s0 >> tl) || (c.s1 >> tl)) {
+                atomicExch(err + 1, 1);
+                continue;
+            }
+            br.init_at(sp, (int32_t)c.bitpos);
+            s0 = c.s0;
+            s1 = c.s1;
+        }
+        unsigned i = start;
+        for (; i + 1 < end; i += 2) {
+            const fse::DEntry e0 = dt[s0];
+            const fse::DEntry e1 = dt[s1];
+            dst[i] = e0.symbol;
+            dst[i + 1] = e1.symbol;
+            s0 = e0.newState + br.read(e0.nbBits);
+            s1 = e1.newState + br.read(e1.nbBits);
+        }
+        if (i < end) dst[i] = dt[s0].symbol;
+        if (q + 1 < nparts) {
+            const FseCkpt c = cks[jb.ck + q];
+            if (c.s0 != s0 || c.s1 != s1 || br.pos != br.start_bit(sp) + (int32_t)c.bitpos) atomicExch(err + 1, 1);
+        }
     }
-    if (i < n) dst[i] = dt[s0].symbol;
 }
 
 // Walks an fse_enc record sequence (host bytes) for n symbols starting at `off`; appends jobs.
@@ -261,6 +461,8 @@ size_t parse_blocks(const ByteView &h, size_t off, unsigned long long n, unsigne
 struct GammaOut {
     std::vector<std::vector<std::pair<const uint8_t *, size_t>>> cls_pieces;  // per group
     std::vector<std::vector<unsigned>> cls_n;                                  // symbols per block
+    std::vector<std::vector<uint8_t>> cls_flag;                                // record flag per block
+    std::vector<std::vector<const FseCkpt *>> cls_ck;                          // checkpoints per block
     std::vector<size_t> cls_bytes;                                             // per group
     std::vector<const uint8_t *> man_ptr;                                      // per group
     std::vector<size_t> man_bytes;                                             // per group
@@ -309,12 +511,14 @@ __global__ void k_pick_u64(const unsigned long long *__restrict__ src, const uns
 }
 
 GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
-                      cudaStream_t st) {
+                      cudaStream_t st, uint32_t ckpt_part) {
     const int G = (int)gstart.size() - 1;
     const long long T = (long long)gstart.back();
     GammaOut out;
     out.cls_pieces.resize(G);
     out.cls_n.resize(G);
+    out.cls_flag.resize(G);
+    out.cls_ck.resize(G);
     out.cls_bytes.assign(G, 0);
     out.man_ptr.assign(G, nullptr);
     out.man_bytes.assign(G, 0);
@@ -358,27 +562,64 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     uint8_t *slots = pool.get<uint8_t>(jobs.size() * kBlockSlot);
     uint8_t *bits = pool.get<uint8_t>(jobs.size() * kBlockSlot);
     unsigned long long *sizes = pool.get<unsigned long long>(jobs.size());
-    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, 0, st>>>(cls, d_jobs, slots, sizes, bits);
+    const size_t ck_per_block = ckpt_part ? FBLK / ckpt_part : 0;
+    FseCkpt *cks = ckpt_part ? pool.get<FseCkpt>(jobs.size() * ck_per_block) : nullptr;
+    uint32_t *recs = pool.get<uint32_t>(jobs.size() * FBLK);
+    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, 0, st>>>(cls, d_jobs, slots, sizes, bits,
+                                                              ckpt_part ? ckpt_part : 4096u, cks, recs);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
     for (size_t j = 0; j < jobs.size(); j++) {
         const int g = job_group[j];
-        out.cls_pieces[g].push_back({slots + j * kBlockSlot, (size_t)hs[j]});
+        const size_t sz = (size_t)(hs[j] & ((1ULL << 56) - 1));
+        out.cls_pieces[g].push_back({slots + j * kBlockSlot, sz});
         out.cls_n[g].push_back(jobs[j].n);
-        out.cls_bytes[g] += (size_t)hs[j];
+        out.cls_flag[g].push_back((uint8_t)(hs[j] >> 56));
+        out.cls_ck[g].push_back(cks ? cks + j * ck_per_block : nullptr);
+        out.cls_bytes[g] += sz;
     }
     return out;
 }
 
 // Adds the fse_enc records of group g, recording each record's header bytes for the index.
-void add_class_pieces(Assembler &as, const GammaOut &go, int g) {
+// Gathers the decode checkpoints of the streams in stream order and writes the FB2C frame.
+struct CkptCollector {
+    uint32_t o1_part = 0, fse_part = 0;
+    const O1Ckpt *o1 = nullptr;
+    unsigned long long n_o1 = 0;
+    std::vector<std::pair<const FseCkpt *, uint32_t>> fse;
+    unsigned long long n_fse = 0;
+    void add_block(const FseCkpt *p, uint32_t count) {
+        if (p && count) {
+            fse.push_back({p, count});
+            n_fse += count;
+        }
+    }
+    void emit(Assembler &as) const {
+        if (n_o1 + n_fse == 0 || !as.with_index) return;
+        const unsigned long long content = kCkptHeader + n_o1 * sizeof(O1Ckpt) + n_fse * sizeof(FseCkpt);
+        if (content >= 0xFFFFFFFFULL) return;
+        uint8_t h[8 + kCkptHeader];
+        static_assert(kCkptHeader == 32, "content header: tag, version, o1_part, fse_part, n_o1, n_fse");
+        const uint32_t w[6] = {kSkippableMagic, (uint32_t)content, kCkptTag, kCkptVersion, o1_part, fse_part};
+        memcpy(h, w, sizeof(w));
+        memcpy(h + 24, &n_o1, 8);
+        memcpy(h + 32, &n_fse, 8);
+        as.tail_bytes(h, sizeof(h));
+        as.tail_dev(o1, n_o1 * sizeof(O1Ckpt));
+        for (auto &f : fse) as.tail_dev(f.first, (size_t)f.second * sizeof(FseCkpt));
+    }
+};
+static_assert(sizeof(O1Ckpt) == 12 && sizeof(FseCkpt) == 8, "checkpoint record sizes are part of the frame format");
+
+void add_class_pieces(Assembler &as, const GammaOut &go, int g, CkptCollector *cc = nullptr) {
     for (size_t b = 0; b < go.cls_pieces[g].size(); b++) {
         const auto &p = go.cls_pieces[g][b];
-        const unsigned n = go.cls_n[g][b];
+        if (cc && go.cls_flag[g][b] == 1) cc->add_block(go.cls_ck[g][b], fse_ckpt_count(go.cls_n[g][b], cc->fse_part));
         uint8_t h[5];
         size_t hl;
-        if (p.second == 1 + (size_t)n) { h[0] = 0; hl = 1; }
-        else if (p.second == 2) { h[0] = 2; hl = 1; }
+        const uint8_t flag = go.cls_flag[g][b];
+        if (flag != 1) { h[0] = flag; hl = 1; }
         else {
             h[0] = 1;
             const uint32_t r = (uint32_t)(p.second - 5);
@@ -759,7 +1000,15 @@ struct DecChain {
     unsigned long long lo, n;   // output range
     unsigned long long ovf;     // first escape value of this chunk
     int table;                  // segment index (tables at table * 15)
-    int pad;
+    uint32_t nesc;              // escapes of this chunk
+    uint32_t ck;                // first decode checkpoint of this chunk
+    uint32_t pad;
+};
+
+// One part of a chain decoded from a checkpoint (part 0 starts at the chain's stream end).
+struct DecPart {
+    uint32_t chain;
+    uint32_t part;
 };
 
 // ---- shared-memory resident context tables
@@ -791,7 +1040,10 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_encode_smem(const int16_t 
                                                       const uint16_t *__restrict__ stab,
                                                       const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
                                                       const unsigned long long *__restrict__ slot_off,
-                                                      unsigned long long *__restrict__ blen) {
+                                                      unsigned long long *__restrict__ blen,
+                                                      const uint32_t *__restrict__ nvk, uint32_t part,
+                                                      O1Ckpt *__restrict__ cks,
+                                                      const unsigned long long *__restrict__ ck_off) {
     extern __shared__ uint4 smem_raw[];
     uint16_t *sst = reinterpret_cast<uint16_t *>(smem_raw);
     const ChainCta w = ctas[blockIdx.x];
@@ -838,6 +1090,17 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_encode_smem(const int16_t 
     uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
     uint32_t v = (nb << 16) - t.deltaNbBits;
     uint32_t state = stlookup(c, (int32_t)(v >> nb) + t.deltaFindState);
+    // decode checkpoints: after coding index lo + q * part (q >= 1), the decoder's state, bit
+    // position, context and escape count before it decodes that index
+    O1Ckpt *ck = cks ? cks + ck_off[chain] : nullptr;
+    const uint32_t esc_total = nvk ? nvk[chain] : 0;
+    uint32_t esc_seen = (uint32_t)(Q0 + 127) > 254u;
+    uint32_t rem = (uint32_t)((idx - L0) % part);
+    auto record = [&](long long i, int prev) {
+        ck[(i - L0) / part - 1] = O1Ckpt{bw.nw * 32 + bw.nb, esc_total - esc_seen, (uint16_t)(state & (O1_M - 1)),
+                                         (uint16_t)o1_ctx(prev)};
+    };
+    if (ck && rem == 0 && idx > L0) record(idx, Q1);
     // advance to idx - 1
     Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
     idx--;
@@ -853,6 +1116,9 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_encode_smem(const int16_t 
         nb = (state + t.deltaNbBits) >> 16;
         bw.add(state, nb);
         state = stlookup(c, (int32_t)(state >> nb) + t.deltaFindState);
+        esc_seen += (uint32_t)(Q0 + 127) > 254u;
+        rem = rem == 0 ? part - 1 : rem - 1;
+        if (ck && rem == 0 && idx > L0) record(idx, Q1);
         Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
         idx--;
     }
@@ -921,6 +1187,371 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t 
 // Context frequencies of one table set: the stationary distribution of the context chain implied
 // by the normalized tables (the next context is a function of the decoded code; escapes split
 // between the two large-magnitude contexts).  Returns (map, rev) for `slots` resident tables.
+// ---- parallel chain encoder
+// Every chain is cut into parts of `part` codes, one part per thread, all parts of a chain in one
+// CTA.  A tANS encoder walks its chain backwards and only its state carries from one code to the
+// next, so:
+//   1. every part runs from a guessed entering state (the top part from the exact initial state),
+//      keeping the state at every 64th index (`sparse`) and its exit state;
+//   2. repair rounds: each part reruns from the exit state of the part above until its state
+//      equals a kept one (from there on the two runs are identical); a part that never meets its
+//      kept states has a new exit state, so the part below repairs again in the next round.
+//      Encoder states from different starting points meet after a few hundred codes, so one round
+//      nearly always suffices, and the loop ends after at most one round per part;
+//   3. emission: every part reruns from its exact entering state and writes its bits to its own
+//      staging area, counting them;
+//   4. the bit counts give every part its offset in the chain's stream; every part shifts its
+//      staged words into place (words shared with a neighbour are merged with atomicOr);
+//   5. every part start is a decode checkpoint: state, bit position, context and escape count.
+// The stream is bit-identical to a sequential encoder's (the tANS states are fully determined).
+constexpr int kSpecThreads = 256;
+constexpr int kSpecSlots = 11;  // 11 x 16 KiB state tables + 30 KiB symbol transforms in shared memory
+constexpr size_t kSpecSmem = (size_t)O1_NCTX * O1_NSYM * sizeof(fse::SymTT) + (size_t)kSpecSlots * O1_M * 2;
+constexpr int kSparseShift = 6;  // kept speculative states: every 64th index
+struct SpecCta {
+    int table;
+    int first;  // first chain
+    int count;  // chains
+    int ppc;    // threads per chain (>= parts of every chain of the CTA)
+    unsigned long long map, rev;
+};
+
+// Staging words of one part: 13 bits per code at most, plus the final state and end mark.
+__host__ __device__ __forceinline__ size_t spec_stage_words(uint32_t part) { return ((size_t)part * 13 + 64) / 32 + 4; }
+
+// keys[i] = context of code i-1 (8 bits) | symbol of code i (8 bits)
+__global__ void k_o1_keys(const int16_t *__restrict__ q, long long n, uint16_t *__restrict__ keys) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int prev = i > 0 ? (int)q[i - 1] : 0;
+        keys[i] = (uint16_t)((o1_ctx(prev) << 8) | o1_sym((int)q[i]));
+    }
+}
+
+// Calls f(i, keys[i]) for i = top down to bottom, reading the keys through aligned 16-byte vectors
+// (8 keys) fetched two vectors ahead.
+template <class F>
+__device__ __forceinline__ void walk_keys(const uint16_t *__restrict__ keys, long long top, long long bottom, F &&f) {
+    long long i = top;
+    for (; i >= bottom && (i & 7) != 7; i--) f(i, (uint32_t)__ldg(keys + i));
+    if (i - 7 >= bottom) {
+        const uint4 *kv = reinterpret_cast<const uint4 *>(keys);
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        uint4 v0 = __ldg(kv + ((i - 7) >> 3));
+        uint4 v1 = i - 15 >= 0 ? __ldg(kv + ((i - 15) >> 3)) : z;
+        while (i - 7 >= bottom) {
+            const uint4 v2 = i - 23 >= 0 ? __ldg(kv + ((i - 23) >> 3)) : z;
+            f(i, v0.w >> 16);
+            f(i - 1, v0.w & 0xFFFFu);
+            f(i - 2, v0.z >> 16);
+            f(i - 3, v0.z & 0xFFFFu);
+            f(i - 4, v0.y >> 16);
+            f(i - 5, v0.y & 0xFFFFu);
+            f(i - 6, v0.x >> 16);
+            f(i - 7, v0.x & 0xFFFFu);
+            i -= 8;
+            v0 = v1;
+            v1 = v2;
+        }
+    }
+    for (; i >= bottom; i--) f(i, (uint32_t)__ldg(keys + i));
+}
+
+// Per key (context << 8 | symbol) the encoder's symbol transform, with the table position folded
+// in: deltaFindState + 8192 * slot for a context resident in shared memory, or kFarTable +
+// 8192 * context for one read from global memory.
+struct EncRec {
+    uint32_t dfs;
+    uint32_t dnb;
+};
+constexpr uint32_t kFarTable = 1u << 30;
+
+__global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
+    const uint16_t *__restrict__ keys, const SegInfo *__restrict__ segs, const SpecCta *__restrict__ ctas,
+    const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, uint16_t *__restrict__ sparse,
+    uint32_t *__restrict__ stage, uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
+    unsigned long long *__restrict__ blen, uint32_t part, O1Ckpt *__restrict__ cks,
+    const unsigned long long *__restrict__ ck_off, int *__restrict__ err) {
+    extern __shared__ uint4 smem_raw[];
+    EncRec *rec = reinterpret_cast<EncRec *>(smem_raw);
+    uint16_t *sst = reinterpret_cast<uint16_t *>(rec + O1_NCTX * O1_NSYM);
+    __shared__ uint32_t s_bits[kSpecThreads], s_esc[kSpecThreads], s_exit[kSpecThreads + 1];
+    __shared__ int s_chg[kSpecThreads + 1];
+    const SpecCta w = ctas[blockIdx.x];
+    const size_t tb = (size_t)w.table * O1_NCTX;
+    const uint16_t *__restrict__ S = stab + tb * O1_M;
+    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) {
+        const fse::SymTT t0 = stt[tb * O1_NSYM + i];
+        const int c = i >> 8;
+        const uint32_t sl = (uint32_t)(w.map >> (4 * c)) & 15u;
+        const uint32_t base = sl < (uint32_t)kSpecSlots ? sl * O1_M : kFarTable + (uint32_t)c * O1_M;
+        rec[i] = EncRec{(uint32_t)t0.deltaFindState + base, t0.deltaNbBits};
+    }
+    for (int j = 0; j < kSpecSlots; j++) {
+        const int c = (int)((w.rev >> (4 * j)) & 15);
+        if (c >= O1_NCTX) continue;
+        const uint4 *s2 = reinterpret_cast<const uint4 *>(S + (size_t)c * O1_M);
+        uint4 *d2 = reinterpret_cast<uint4 *>(sst + (size_t)j * O1_M);
+        for (int i = threadIdx.x; i < O1_M * 2 / 16; i += blockDim.x) d2[i] = __ldg(s2 + i);
+    }
+    const int t = threadIdx.x;
+    const int ci = t / w.ppc, p = t % w.ppc;
+    const int chain = w.first + ci;
+    long long lo = 0, hi = 0;
+    if (ci < w.count) {
+        const int g = chain / kMaxK, k = chain % kMaxK;
+        const SegInfo sg = segs[g];
+        if (k < sg.K) {
+            lo = (long long)(sg.lo + (unsigned long long)k * sg.cs);
+            hi = min(lo + (long long)sg.cs, (long long)(sg.lo + sg.n));
+        }
+        if (p == 0 && hi <= lo) blen[chain] = 0;
+    }
+    const int nparts = hi > lo ? (int)((hi - lo + part - 1) / part) : 0;
+    const bool active = ci < w.count && p < nparts;
+    const bool is_top = active && p == nparts - 1;
+    const long long a = lo + (long long)p * part;
+    const long long top = active ? min(a + (long long)part, hi) - 1 : 0;
+    s_chg[t] = 0;
+    s_exit[t] = 0;
+    if (t == 0) {
+        s_chg[kSpecThreads] = 0;
+        s_exit[kSpecThreads] = 0;
+    }
+    __syncthreads();
+    auto next_state = [&](uint32_t x, const EncRec r, uint32_t nb) -> uint32_t {
+        const uint32_t y = (x >> nb) + r.dfs;
+        return y < kFarTable ? (uint32_t)sst[y] : (uint32_t)__ldg(S + (y - kFarTable));
+    };
+    auto init_state = [&](uint32_t k) -> uint32_t {
+        const EncRec r = rec[k];
+        const uint32_t nb = (r.dnb + (1u << 15)) >> 16;
+        return next_state((nb << 16) - r.dnb, r, nb);
+    };
+    // the first code of a chain has context 0, so index lo is coded apart from the walks
+    const long long istart = is_top ? hi - 2 : top;
+    const long long bottom = p == 0 ? a + 1 : a;
+    const uint32_t k_lo = p == 0 && active ? ((uint32_t)__ldg(keys + lo) & 0xFFu) : 0u;
+    // 1. speculative pass
+    uint32_t esc = 0;
+    if (active) {
+        uint32_t x;
+        if (is_top) {
+            const uint32_t k0 = hi - 1 == lo ? k_lo : (uint32_t)__ldg(keys + hi - 1);
+            x = init_state(k0);
+            esc += (k0 & 0xFFu) == 0xFFu;
+            if (((hi - 1) & 63) == 0) sparse[(hi - 1) >> 6] = (uint16_t)x;
+        } else {
+            x = init_state((uint32_t)__ldg(keys + top + 1));
+        }
+        auto step = [&](long long i, uint32_t k) {
+            const EncRec r = rec[k];
+            const uint32_t nb = (x + r.dnb) >> 16;
+            x = next_state(x, r, nb);
+            esc += (k & 0xFFu) == 0xFFu;
+            if (((uint32_t)i & 63u) == 0) sparse[i >> 6] = (uint16_t)x;
+        };
+        walk_keys(keys, istart, bottom, step);
+        if (p == 0 && istart >= lo) step(lo, k_lo);
+        s_exit[t] = x;
+    }
+    // 2. repair rounds (err[2] counts the re-run codes, err[3] the rounds, for diagnostics)
+    bool need = active && !is_top;
+    uint32_t repaired = 0;
+    for (int round = 0;; round++) {
+        if (round > nparts + 2 && need) atomicExch(err, 5);
+        if (t == 0) atomicMax(err + 3, round);
+        const uint32_t E = need ? s_exit[t + 1] : 0u;
+        __syncthreads();
+        bool changed = false;
+        if (need && round <= nparts + 2) {
+            uint32_t x = E;
+            bool met = false;
+            for (long long i = top; i >= a; i--) {
+                const uint32_t k = i == lo ? k_lo : (uint32_t)__ldg(keys + i);
+                const EncRec r = rec[k];
+                const uint32_t nb = (x + r.dnb) >> 16;
+                x = next_state(x, r, nb);
+                repaired++;
+                if (((uint32_t)i & 63u) == 0) {
+                    if (sparse[i >> 6] == (uint16_t)x) {
+                        met = true;
+                        break;
+                    }
+                    sparse[i >> 6] = (uint16_t)x;
+                }
+            }
+            if (!met) {
+                changed = x != s_exit[t];
+                s_exit[t] = x;
+            }
+        }
+        s_chg[t] = changed;
+        __syncthreads();
+        need = active && !is_top && s_chg[t + 1] != 0;
+        if (!__syncthreads_or(need)) break;
+    }
+    if (repaired) atomicAdd(err + 2, (int)repaired);
+    // 3. emission into the part's staging area
+    uint32_t bits = 0;
+    uint32_t *sw = stage + ((size_t)blockIdx.x * kSpecThreads + t) * spec_stage_words(part);
+    if (active) {
+        uint32_t x = is_top ? init_state(hi - 1 == lo ? k_lo : (uint32_t)__ldg(keys + hi - 1)) : s_exit[t + 1];
+        uint64_t acc = 0;
+        uint32_t accn = 0, nw = 0;
+        auto put = [&](uint32_t v, uint32_t nb) {
+            acc |= (uint64_t)(v & ((1u << nb) - 1u)) << accn;
+            accn += nb;
+            if (accn >= 32) {
+                sw[nw++] = (uint32_t)acc;
+                acc >>= 32;
+                accn -= 32;
+            }
+        };
+        auto step = [&](long long, uint32_t k) {
+            const EncRec r = rec[k];
+            const uint32_t nb = (x + r.dnb) >> 16;
+            put(x, nb);
+            bits += nb;
+            x = next_state(x, r, nb);
+        };
+        walk_keys(keys, istart, bottom, step);
+        if (p == 0 && istart >= lo) step(lo, k_lo);
+        if (x != s_exit[t]) atomicExch(err, 5);
+        if (p == 0) {
+            put(x & (O1_M - 1), O1_PB);  // the final state, then the end mark
+            put(1u, 1u);
+            bits += O1_PB + 1;
+        }
+        if (accn > 0) sw[nw] = (uint32_t)acc;
+    }
+    // 4. offsets (the top part's bits come first), escapes below each part, placement
+    s_bits[t] = active ? bits : 0u;
+    s_esc[t] = active ? esc : 0u;
+    __syncthreads();
+    uint32_t off = 0, esc_below = 0;
+    if (active) {
+        for (int q = p + 1; q < nparts; q++) off += s_bits[t - p + q];
+        for (int q = 0; q < p; q++) esc_below += s_esc[t - p + q];
+    }
+    uint32_t *ow = active ? reinterpret_cast<uint32_t *>(slots + slot_off[chain]) : nullptr;
+    if (active) ow[off >> 5] = 0u;  // the first word may be shared with the part above: zeroed, then OR-ed
+    __syncthreads();
+    if (active) {
+        // Output words [w0, wend).  Word w0 was zeroed by this part; the last word, when the part
+        // ends inside it and a part follows, is the next part's first word (zeroed by it).  Both are
+        // merged with atomicOr, every other word is this part's alone.
+        const uint32_t sh = off & 31u, nwords = (bits + 31) / 32;
+        const uint32_t w0 = off >> 5, wend = (off + bits + 31) >> 5;
+        const uint32_t shared_last = (p > 0 && ((off + bits) & 31u)) ? wend - 1 : 0xFFFFFFFFu;
+        auto store = [&](uint32_t wi, uint32_t v) {
+            if (wi == w0 || wi == shared_last) atomicOr(ow + wi, v);
+            else ow[wi] = v;
+        };
+        uint32_t prev = 0;
+        for (uint32_t j = 0; j < nwords; j++) {
+            const uint32_t cur = sw[j];
+            store(w0 + j, sh ? (cur << sh) | (j ? prev >> (32 - sh) : 0u) : cur);
+            prev = cur;
+        }
+        if (sh && w0 + nwords < wend) store(w0 + nwords, prev >> (32 - sh));
+        if (p == 0) blen[chain] = ((unsigned long long)off + bits + 7) / 8;
+        // 5. decode checkpoint at the part start: the state the decoder holds before index a
+        if (p > 0 && cks)
+            cks[ck_off[chain] + p - 1] = O1Ckpt{off + bits, esc_below, (uint16_t)(s_exit[t] & (O1_M - 1)),
+                                                (uint16_t)(__ldg(keys + a) >> 8)};
+    }
+}
+
+// Decodes the parts of tANS chains, one part per thread (the chains' checkpoints give every part's
+// starting bit position, state, context and escape offset).  The CTA's parts share one table set,
+// staged in shared memory as for k_o1_decode_smem.  Each part that ends at a checkpoint checks that
+// it arrived there (state, context, bit position, escapes); a mismatch sets err[1].
+__global__ void __launch_bounds__(kChainThreads) k_o1_decode_parts(const uint8_t *__restrict__ in,
+                                                                 const DecChain *__restrict__ chains,
+                                                                 const DecPart *__restrict__ parts,
+                                                                 const ChainCta *__restrict__ ctas,
+                                                                 const uint32_t *__restrict__ dt,
+                                                                 const int16_t *__restrict__ ovf,
+                                                                 unsigned long long n_ovf,
+                                                                 const O1Ckpt *__restrict__ cks, uint32_t part,
+                                                                 int16_t *__restrict__ out, int *__restrict__ err) {
+    extern __shared__ uint4 smem_raw[];
+    uint32_t *sdt = reinterpret_cast<uint32_t *>(smem_raw);
+    const ChainCta w = ctas[blockIdx.x];
+    const uint32_t *__restrict__ tb = dt + (size_t)w.table * O1_NCTX * O1_M;
+    for (int j = 0; j < kDecSlots; j++) {
+        const int c = (int)((w.rev >> (4 * j)) & 15);
+        if (c >= O1_NCTX) continue;
+        const uint4 *src = reinterpret_cast<const uint4 *>(tb + (size_t)c * O1_M);
+        uint4 *dst = reinterpret_cast<uint4 *>(sdt + (size_t)j * O1_M);
+        for (int i = threadIdx.x; i < O1_M * 4 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    if ((int)threadIdx.x >= w.count) return;
+    const DecPart pp = parts[w.first + threadIdx.x];
+    const DecChain ch = chains[pp.chain];
+    const unsigned long long start = (unsigned long long)pp.part * part;
+    if (ch.n == 0 || start >= ch.n || ch.inlen == 0 || ch.inlen >= (1ull << 28)) {
+        atomicExch(err, 6);
+        return;
+    }
+    const uint32_t n = (uint32_t)min((unsigned long long)part, ch.n - start);
+    const bool last = start + n >= ch.n;
+    const uint8_t *sb = in + ch.in;
+    const uint32_t sbits = (uint32_t)ch.inlen * 8u;
+    fse::ReaderPF br;
+    uint32_t state, ctx, oi0;
+    if (pp.part == 0) {
+        if (!br.init(sb, (uint32_t)ch.inlen)) {
+            atomicExch(err, 6);
+            return;
+        }
+        state = br.read(O1_PB);
+        ctx = 0;
+        oi0 = 0;
+    } else {
+        const O1Ckpt c = cks[ch.ck + pp.part - 1];
+        if (c.bitpos >= sbits || c.state >= O1_M || c.ctx >= O1_NCTX || c.esc > ch.nesc) {
+            atomicExch(err + 1, 1);
+            return;
+        }
+        br.init_at(sb, (int32_t)c.bitpos);
+        state = c.state;
+        ctx = c.ctx;
+        oi0 = c.esc;
+    }
+    const unsigned long long avail = n_ovf > ch.ovf + oi0 ? n_ovf - ch.ovf - oi0 : 0;
+    const uint32_t nov = (uint32_t)min((unsigned long long)(ch.nesc - oi0), avail);
+    const int16_t *__restrict__ ov = ovf + ch.ovf + oi0;
+    int16_t *o = out + ch.lo + start;
+    const unsigned long long map = w.map;
+    uint32_t oi = 0;
+    int q0 = nov > 0 ? (int)__ldg(ov) : 0;
+    int q1 = nov > 1 ? (int)__ldg(ov + 1) : 0;
+    for (uint32_t j = 0; j < n; j++) {
+        const uint32_t sl = (uint32_t)(map >> (4 * ctx)) & 15u;
+        const uint32_t e = sl < (uint32_t)kDecSlots ? sdt[sl * O1_M + state] : __ldg(tb + ctx * O1_M + state);
+        const bool esc = (e >> 21) & 1u;
+        const int code = esc ? q0 : ((int)e >> 22);
+        ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
+        if (esc) {
+            oi++;
+            q0 = q1;
+            q1 = oi + 1 < nov ? (int)__ldg(ov + oi + 1) : 0;
+        }
+        o[j] = (int16_t)code;
+        state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
+    }
+    if (oi > nov) atomicExch(err, 7);
+    if (!last) {
+        const O1Ckpt c = cks[ch.ck + pp.part];
+        if (c.state != state || c.ctx != ctx || br.pos != br.start_bit(sb) + (int32_t)c.bitpos || c.esc != oi0 + oi)
+            atomicExch(err + 1, 1);
+    } else if (br.pos < br.start_bit(sb) - 16) {
+        atomicExch(err, 8);
+    }
+}
+
 std::pair<unsigned long long, unsigned long long> hot_contexts(const uint16_t *nf, int slots) {
     double P[O1_NCTX][O1_NCTX] = {};
     for (int c = 0; c < O1_NCTX; c++) {
@@ -962,20 +1593,42 @@ std::pair<unsigned long long, unsigned long long> hot_contexts(const uint16_t *n
 }
 
 // CTAs of up to 64 consecutive chains that share a table set.
-// Groups consecutive chains of one table into CTAs of at most `per` chains; `per` is chosen so
-// that the CTAs cover the SMs once (one chain CTA fills an SM).
+// Groups consecutive items (chains or parts) of one table into CTAs.  One CTA fills an SM (its
+// tables take the shared memory), so the CTAs should be at most one per SM: every run of one table
+// gets CTAs in proportion to its size (greedily, always to the run whose CTAs are largest), and
+// a run's items are split evenly among its CTAs.  More items than SMs x max_per take several waves.
 std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std::vector<unsigned long long> &maps,
-                                 const std::vector<unsigned long long> &revs) {
+                                 const std::vector<unsigned long long> &revs, size_t max_per = kMaxChainsPerCta) {
     std::vector<ChainCta> out;
+    const size_t n = chain_table.size();
     const size_t sms = (size_t)sm_count();
-    const size_t per = std::max<size_t>(8, std::min<size_t>(kMaxChainsPerCta, (chain_table.size() + sms - 1) / sms));
-    size_t i = 0;
-    while (i < chain_table.size()) {
-        const int t = chain_table[i];
+    std::vector<std::pair<size_t, size_t>> runs;  // (first, length)
+    for (size_t i = 0; i < n;) {
         size_t j = i;
-        while (j < chain_table.size() && chain_table[j] == t && j - i < per) j++;
-        out.push_back(ChainCta{t, (int)i, (int)(j - i), 0, maps[t], revs[t]});
+        while (j < n && chain_table[j] == chain_table[i]) j++;
+        runs.push_back({i, j - i});
         i = j;
+    }
+    std::vector<size_t> ctas(runs.size(), 1);
+    if (runs.size() <= sms && n <= sms * max_per) {
+        auto size_of = [&](size_t r) { return (runs[r].second + ctas[r] - 1) / ctas[r]; };
+        for (size_t used = runs.size(); used < sms; used++) {
+            size_t best = 0;
+            for (size_t r = 1; r < runs.size(); r++)
+                if (size_of(r) > size_of(best)) best = r;
+            if (size_of(best) <= 1) break;
+            ctas[best]++;
+        }
+    }
+    for (size_t r = 0; r < runs.size(); r++) {
+        size_t c = std::max<size_t>(ctas[r], (runs[r].second + max_per - 1) / max_per);
+        c = std::min(c, runs[r].second);
+        const int t = chain_table[runs[r].first];
+        for (size_t k = 0; k < c; k++) {
+            const size_t a = runs[r].first + runs[r].second * k / c;
+            const size_t b = runs[r].first + runs[r].second * (k + 1) / c;
+            if (b > a) out.push_back(ChainCta{t, (int)a, (int)(b - a), 0, maps[t], revs[t]});
+        }
     }
     return out;
 }
@@ -987,6 +1640,9 @@ void enable_big_smem() {
                                   kEncSlots * O1_M * 2));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kDecSlots * O1_M * 4));
+    FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_parts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kDecSlots * O1_M * 4));
+    FB2_CUDA(cudaFuncSetAttribute(k_o1_encode_spec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpecSmem));
     done = true;
 }
 
@@ -1118,15 +1774,28 @@ __global__ void k_sample_windows(const int16_t *__restrict__ q, const unsigned l
 void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
                   const std::vector<size_t> &cls_off, const std::vector<size_t> &man_off,
                   const std::vector<size_t> &man_len, const std::vector<unsigned long long> &gstart,
-                  uint32_t *d_vals, int *d_err, cudaStream_t st) {
+                  uint32_t *d_vals, int *d_err, cudaStream_t st, const FseCkpt *d_fck = nullptr,
+                  uint32_t fpart = 0, unsigned long long n_fck = 0) {
     const int G = (int)gstart.size() - 1;
     const long long T = (long long)gstart.back();
     if (T == 0) return;
     std::vector<BlockJob> jobs;
     for (int g = 0; g < G; g++) parse_blocks(h, cls_off[g], gstart[g + 1] - gstart[g], gstart[g], jobs);
+    if (d_fck && fpart) {
+        // the checkpoints belong to the FSE-coded blocks in stream order
+        unsigned long long used = 0;
+        for (auto &j : jobs)
+            if (j.flag == 1) {
+                const uint32_t c = fse_ckpt_count(j.n, fpart);
+                j.ck = c ? (uint32_t)used : 0xFFFFFFFFu;
+                used += c;
+            }
+        if (used != n_fck)
+            for (auto &j : jobs) j.ck = 0xFFFFFFFFu;
+    }
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
-    k_fse_decode_blocks<<<(unsigned)jobs.size(), 32, 0, st>>>(d, dj, cls, d_err);
+    k_fse_decode_blocks<<<(unsigned)jobs.size(), 32, 0, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
     FB2_CHECK_LAUNCH();
     unsigned long long *boff = pool.get<unsigned long long>(T + 1);
     void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
@@ -1212,6 +1881,12 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         q = dq;
     }
     const uint8_t mb = (uint8_t)(ch.method | (ch.delta ? 0x80 : 0));
+    CkptCollector cc;
+    {
+        const uint32_t part = tune.ckpt_part;
+        const bool pow2 = part >= 64 && part <= (uint32_t)FBLK && (part & (part - 1)) == 0;
+        cc.o1_part = cc.fse_part = pow2 ? part : 0;
+    }
     as.val<uint8_t>(mb);
     as.val<uint16_t>(0);  // lo_
     as.val<uint16_t>(0);  // mode_
@@ -1248,15 +1923,15 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             FB2_CUDA(cudaMemcpyAsync(buf + nv, &tr, 4, cudaMemcpyHostToDevice, st));
             FB2_CUDA(cudaStreamSynchronize(st));
         }
-        GammaOut go = gamma_encode(pool, buf, {0ULL, nr, nr + nv}, st);
+        GammaOut go = gamma_encode(pool, buf, {0ULL, nr, nr + nv}, st, cc.fse_part);
         as.val<uint64_t>(nr);
         as.val<uint64_t>(nv);
         as.val<uint64_t>(go.cls_bytes[0]);
         as.val<uint64_t>(go.cls_bytes[1]);
         as.val<uint64_t>(go.man_bytes[0]);
         as.val<uint64_t>(go.man_bytes[1]);
-        add_class_pieces(as, go, 0);
-        add_class_pieces(as, go, 1);
+        add_class_pieces(as, go, 0, &cc);
+        add_class_pieces(as, go, 1, &cc);
         as.dev(go.man_ptr[0], go.man_bytes[0]);
         as.dev(go.man_ptr[1], go.man_bytes[1]);
     } else {
@@ -1282,6 +1957,30 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
                               (unsigned long long)((ng + K - 1) / K), K, 0};
         }
         SegInfo *d_segs = h2d(pool, segs, st);
+        // encoder part size (also the decode checkpoint spacing): a chain's parts fit one CTA
+        unsigned long long max_cs = 1;
+        for (const auto &sg : segs) max_cs = std::max<unsigned long long>(max_cs, sg.cs);
+        uint32_t enc_part = cc.o1_part ? cc.o1_part : 4096u;
+        while ((max_cs + enc_part - 1) / enc_part > (unsigned long long)kSpecThreads) enc_part *= 2;
+        if (cc.o1_part) cc.o1_part = enc_part;
+        const int ppc = (int)((max_cs + enc_part - 1) / enc_part);
+        // decode checkpoints of every chain: one before each index lo + q * part, q >= 1
+        const long long nchains_all = S * kMaxK;
+        std::vector<unsigned long long> ck_off(nchains_all + 1, 0);
+        for (long long g = 0; g < S; g++)
+            for (int k = 0; k < kMaxK; k++) {
+                unsigned long long cnt = 0;
+                if (k < K && cc.o1_part) {
+                    const unsigned long long clo = segs[g].lo + (unsigned long long)k * segs[g].cs;
+                    const unsigned long long chi = std::min(clo + segs[g].cs, segs[g].lo + segs[g].n);
+                    if (chi > clo) cnt = (chi - clo - 1) / cc.o1_part;
+                }
+                ck_off[g * kMaxK + k + 1] = ck_off[g * kMaxK + k] + cnt;
+            }
+        cc.n_o1 = ck_off.back();
+        O1Ckpt *o1ck = cc.n_o1 ? pool.get<O1Ckpt>(cc.n_o1) : nullptr;
+        cc.o1 = o1ck;
+        unsigned long long *d_ck_off = o1ck ? h2d(pool, ck_off, st) : nullptr;
         uint32_t *hist = pool.get<uint32_t>((size_t)S * O1_NCTX * O1_NSYM);
         uint32_t *nvk = pool.get<uint32_t>((size_t)S * kMaxK);
         k_o1_hist<<<(unsigned)S, 1024, 0, st>>>(q, d_segs, hist, nvk);
@@ -1320,8 +2019,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint16_t *stab = pool.get<uint16_t>((size_t)ntab * O1_M);
         fse::SymTT *stt = pool.get<fse::SymTT>((size_t)ntab * O1_NSYM);
         uint8_t *spread = pool.get<uint8_t>((size_t)ntab * O1_M);
-        int *d_err = pool.get<int>(4);
-        FB2_CUDA(cudaMemsetAsync(d_err, 0, 16, st));
+        int *d_err = pool.get<int>(8);
+        FB2_CUDA(cudaMemsetAsync(d_err, 0, 32, st));
         k_o1_ctable<<<ntab, 32, 0, st>>>(nf, stab, stt, spread, d_err);
         FB2_CHECK_LAUNCH();
         // chain output slots
@@ -1340,17 +2039,24 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             tr.mark("tables normalized");
             std::vector<unsigned long long> maps(R), revs(R);
             for (int r = 0; r < R; r++) {
-                auto mr = hot_contexts(hnf.data() + (size_t)r * O1_NCTX * O1_NSYM, kEncSlots);
+                auto mr = hot_contexts(hnf.data() + (size_t)r * O1_NCTX * O1_NSYM, kSpecSlots);
                 maps[r] = mr.first;
                 revs[r] = mr.second;
             }
             std::vector<int> chain_table((size_t)nchains);
             for (long long ch = 0; ch < nchains; ch++) chain_table[ch] = seg_region[ch / kMaxK];
-            std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
-            ChainCta *d_ctas = h2d(pool, ctas, st);
+            const std::vector<ChainCta> groups = chain_ctas(chain_table, maps, revs, (size_t)(kSpecThreads / ppc));
+            std::vector<SpecCta> ctas;
+            for (const ChainCta &c : groups) ctas.push_back(SpecCta{c.table, c.first, c.count, ppc, c.map, c.rev});
+            SpecCta *d_ctas = h2d(pool, ctas, st);
+            uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
+            uint16_t *sparse = pool.get<uint16_t>(((size_t)N >> kSparseShift) + 2);
+            uint32_t *stage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
+            k_o1_keys<<<grid_for(N, 256, 148 * 16), 256, 0, st>>>(q, N, keys);
+            FB2_CHECK_LAUNCH();
             enable_big_smem();
-            k_o1_encode_smem<<<(unsigned)ctas.size(), kChainThreads, kEncSlots * O1_M * 2, st>>>(q, d_segs, d_ctas, stab, stt, slots,
-                                                                                   d_soff, blen);
+            k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
+                keys, d_segs, d_ctas, stab, stt, sparse, stage, slots, d_soff, blen, enc_part, o1ck, d_ck_off, d_err);
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
         }
@@ -1366,8 +2072,11 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         FB2_CHECK_LAUNCH();
         std::vector<uint32_t> h_nvk = d2h(nvk, (size_t)S * kMaxK, st);
         std::vector<unsigned long long> h_blen = d2h(blen, (size_t)nchains, st);
-        std::vector<int> h_err = d2h(d_err, 1, st);
-        if (h_err[0]) throw std::runtime_error("tANS table construction failed");
+        std::vector<int> h_err = d2h(d_err, 5, st);
+        if (h_err[0]) throw std::runtime_error("tANS encoding failed (table construction or chain repair)");
+        if (tr.on)
+            std::fprintf(stderr, "[falcons trace] encode chain repair: %d codes re-run, %d rounds, %d far lookups\n",
+                         h_err[2], h_err[3], h_err[4]);
         tr.mark("chains done");
         unsigned long long E = 0;
         std::vector<unsigned long long> gstart(S + 1, 0);
@@ -1383,7 +2092,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, st>>>(q, N, tcnt, evals, eraw);
             FB2_CHECK_LAUNCH();
         }
-        GammaOut go = gamma_encode(pool, evals, gstart, st);
+        GammaOut go = gamma_encode(pool, evals, gstart, st, cc.fse_part);
         tr.mark("escapes coded");
         for (auto b : h_blen)
             if (b == ~0ULL) throw std::runtime_error("tANS chain overflow");
@@ -1408,12 +2117,13 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
                     as.val<uint8_t>(1);
                     as.val<uint64_t>(go.cls_bytes[g]);
                     as.val<uint64_t>(go.man_bytes[g]);
-                    add_class_pieces(as, go, (int)g);
+                    add_class_pieces(as, go, (int)g, &cc);
                     as.dev(go.man_ptr[g], go.man_bytes[g]);
                 }
             }
         }
     }
+    cc.emit(as);
 }
 
 size_t entropy_encode(Context &ctx, const int16_t *d_codes, size_t n, const EntropyChoice &ch, uint8_t *d_out,
@@ -1427,11 +2137,49 @@ size_t entropy_encode(Context &ctx, const int16_t *d_codes, size_t n, const Entr
     return (size_t)as.pos;
 }
 
+bool parse_ckpt_header(const uint8_t *h, const uint8_t *d_content, size_t avail, DecodeCheckpoints &out) {
+    if (avail < kCkptHeader) return false;
+    uint32_t w[4];
+    uint64_t n1, n2;
+    memcpy(w, h, 16);
+    memcpy(&n1, h + 16, 8);
+    memcpy(&n2, h + 24, 8);
+    if (w[0] != kCkptTag || w[1] != kCkptVersion) return false;
+    if (n1 > avail / sizeof(O1Ckpt) || n2 > avail / sizeof(FseCkpt)) return false;
+    if (kCkptHeader + n1 * sizeof(O1Ckpt) + n2 * sizeof(FseCkpt) != avail) return false;
+    out.d_o1 = d_content + kCkptHeader;
+    out.n_o1 = n1;
+    out.o1_part = w[2];
+    out.d_fse = out.d_o1 + n1 * sizeof(O1Ckpt);
+    out.n_fse = n2;
+    out.fse_part = w[3];
+    return true;
+}
+
 size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size_t n, int16_t *d_codes,
-                      cudaStream_t st) {
-    (void)ctx;
+                      cudaStream_t st, const DecodeCheckpoints *ck) {
     Trace tr("decode");
     Pool pool(st);
+    // checkpoint arrays, copied to aligned scratch (their place in the stream has any alignment)
+    auto pow2 = [](uint32_t v) { return v >= 64 && v <= (uint32_t)FBLK && (v & (v - 1)) == 0; };
+    const O1Ckpt *o1ck = nullptr;
+    const FseCkpt *fck = nullptr;
+    uint32_t o1_part = 0, f_part = 0;
+    unsigned long long n_o1ck = 0, n_fck = 0;
+    if (ck && ck->n_o1 && ck->d_o1 && pow2(ck->o1_part) && ck->n_o1 < (1ULL << 32)) {
+        O1Ckpt *d = pool.get<O1Ckpt>(ck->n_o1);
+        launch_gather(pool, {Piece{ck->d_o1, 0, ck->n_o1 * sizeof(O1Ckpt)}}, reinterpret_cast<uint8_t *>(d), st);
+        o1ck = d;
+        o1_part = ck->o1_part;
+        n_o1ck = ck->n_o1;
+    }
+    if (ck && ck->n_fse && ck->d_fse && pow2(ck->fse_part) && ck->n_fse < (1ULL << 32)) {
+        FseCkpt *d = pool.get<FseCkpt>(ck->n_fse);
+        launch_gather(pool, {Piece{ck->d_fse, 0, ck->n_fse * sizeof(FseCkpt)}}, reinterpret_cast<uint8_t *>(d), st);
+        fck = d;
+        f_part = ck->fse_part;
+        n_fck = ck->n_fse;
+    }
     const size_t len = h.len;
     size_t off = 0;
     const uint8_t mb = h.rd<uint8_t>(off);
@@ -1452,7 +2200,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
             throw std::invalid_argument("Invalid or truncated Falcons entropy payload");
         uint32_t *buf = pool.get<uint32_t>(nr + nv + 2);
         gamma_decode(pool, d_in, h, {o_rcl, o_vcl}, {o_rman, o_vman}, {(size_t)rbp, (size_t)vbp},
-                     {0ULL, nr, nr + nv}, buf, d_err, st);
+                     {0ULL, nr, nr + nv}, buf, d_err, st, fck, f_part, n_fck);
         FB2_CUDA(cudaMemsetAsync(d_codes, 0, (size_t)N * 2, st));
         if (nv > 0) {
             unsigned long long *start = pool.get<unsigned long long>(nr + 1);
@@ -1499,7 +2247,8 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 const unsigned long long clo = lo + k * cs;
                 unsigned long long chi = clo + cs;
                 if (chi > hi) chi = hi;
-                DecChain c{sp, bl[k], clo, chi > clo ? chi - clo : 0, ovf_total + tot_ov, (int)g, 0};
+                DecChain c{sp, bl[k], clo, chi > clo ? chi - clo : 0, ovf_total + tot_ov, (int)g,
+                           (uint32_t)std::min<unsigned long long>(nk[k], 0xFFFFFFFFULL), 0, 0};
                 chains.push_back(c);
                 sp += bl[k];
                 tot_ov += nk[k];
@@ -1536,7 +2285,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         int16_t *ovf = pool.get<int16_t>(ovf_total + 1);
         {
             uint32_t *gv = pool.get<uint32_t>(gstart.back() + 1);
-            gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, gv, d_err, st);
+            gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, gv, d_err, st, fck, f_part, n_fck);
             // place: raw blocks are copied, gamma groups converted
             std::vector<Piece> pcs;
             size_t gi = 0;
@@ -1590,6 +2339,16 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         k_o1_dtable<<<ntab, 128, 0, st>>>(nf, dt, spread, d_err);
         FB2_CHECK_LAUNCH();
         for (auto &c : chains) c.table = uid[c.table];
+        // checkpoint base of every chain; the checkpoints are used only if their count matches
+        bool parts_ok = false;
+        if (o1ck) {
+            unsigned long long tot = 0;
+            for (auto &c : chains) {
+                c.ck = (uint32_t)tot;
+                if (c.n) tot += (c.n - 1) / o1_part;
+            }
+            parts_ok = tot == n_o1ck;
+        }
         DecChain *dch = h2d(pool, chains, st);
         {
             std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
@@ -1600,22 +2359,44 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 maps[u] = mr.first;
                 revs[u] = mr.second;
             }
-            std::vector<int> chain_table(chains.size());
-            for (size_t i = 0; i < chains.size(); i++) chain_table[i] = chains[i].table;
-            std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
-            ChainCta *d_ctas = h2d(pool, ctas, st);
             enable_big_smem();
-            k_o1_decode_smem<<<(unsigned)ctas.size(), kChainThreads, kDecSlots * O1_M * 4, st>>>(d_in, dch, d_ctas, dt, ovf,
-                                                                                   ovf_total, d_codes, d_err);
-            FB2_CHECK_LAUNCH();
+            if (parts_ok) {
+                std::vector<DecPart> parts;
+                std::vector<int> part_table;
+                for (size_t i = 0; i < chains.size(); i++) {
+                    const unsigned long long np = chains[i].n ? 1 + (chains[i].n - 1) / o1_part : 0;
+                    for (unsigned long long q = 0; q < np; q++) {
+                        parts.push_back(DecPart{(uint32_t)i, (uint32_t)q});
+                        part_table.push_back(chains[i].table);
+                    }
+                }
+                std::vector<ChainCta> ctas = chain_ctas(part_table, maps, revs, kChainThreads);
+                ChainCta *d_ctas = h2d(pool, ctas, st);
+                DecPart *d_parts = h2d(pool, parts, st);
+                k_o1_decode_parts<<<(unsigned)ctas.size(), kChainThreads, kDecSlots * O1_M * 4, st>>>(
+                    d_in, dch, d_parts, d_ctas, dt, ovf, ovf_total, o1ck, o1_part, d_codes, d_err);
+                FB2_CHECK_LAUNCH();
+            } else {
+                std::vector<int> chain_table(chains.size());
+                for (size_t i = 0; i < chains.size(); i++) chain_table[i] = chains[i].table;
+                std::vector<ChainCta> ctas = chain_ctas(chain_table, maps, revs);
+                ChainCta *d_ctas = h2d(pool, ctas, st);
+                k_o1_decode_smem<<<(unsigned)ctas.size(), kChainThreads, kDecSlots * O1_M * 4, st>>>(
+                    d_in, dch, d_ctas, dt, ovf, ovf_total, d_codes, d_err);
+                FB2_CHECK_LAUNCH();
+            }
         }
     } else {
         throw std::invalid_argument("unsupported entropy method");
     }
     tr.mark("chains launched");
     if (delta) undelta(pool, d_codes, N, st);
-    std::vector<int> he = d2h(d_err, 1, st);
+    std::vector<int> he = d2h(d_err, 2, st);
     tr.mark("chains done");
+    if (he[1] && ck) {
+        // a checkpoint did not match the stream: decode again, sequentially
+        return entropy_decode(ctx, d_in, h, n, d_codes, st, nullptr);
+    }
     if (he[0]) throw std::invalid_argument("Invalid or corrupted Falcons entropy payload");
     return off;
 }

@@ -26,6 +26,30 @@ struct EntropyChoice {
     bool delta;        // forward difference before coding
 };
 
+// Decode checkpoints (the "FB2C" skippable frame written after the header index).  The tANS chains
+// of method 1 and the FSE class blocks are sequential bit streams; at every `part` symbols the
+// encoder records where the decoder will be (bit position, state(s), context, escape count), so
+// the decoder runs every part of every stream at once instead of one thread per stream.  Frame
+// content: u32 tag "FB2C", u32 version 1, u32 o1_part, u32 fse_part, u64 n_o1, u64 n_fse, then
+// n_o1 chain checkpoints of 12 bytes and n_fse block checkpoints of 8 bytes, in stream order.
+// Decoders that do not know the frame (the reference's included) skip it.
+constexpr uint32_t kCkptTag = 0x43324246u;  // "FB2C"
+constexpr uint32_t kCkptVersion = 1;
+constexpr size_t kCkptHeader = 32;          // content bytes before the arrays
+
+struct DecodeCheckpoints {
+    const uint8_t *d_o1 = nullptr;   // device address of the chain checkpoints (any alignment)
+    unsigned long long n_o1 = 0;
+    uint32_t o1_part = 0;
+    const uint8_t *d_fse = nullptr;  // device address of the block checkpoints
+    unsigned long long n_fse = 0;
+    uint32_t fse_part = 0;
+};
+
+// Reads an FB2C frame content header (kCkptHeader bytes); d_content is the device address of the
+// content and avail the content size.  Returns false when it is not a usable checkpoint frame.
+bool parse_ckpt_header(const uint8_t *h, const uint8_t *d_content, size_t avail, DecodeCheckpoints &out);
+
 // Encoder-side tunables (chosen by the autotuner; defaults give ~2% table overhead).
 struct EntropyTuning {
     long long o1_segment = 0;          // symbols per method-1 segment (0 = automatic)
@@ -33,6 +57,7 @@ struct EntropyTuning {
     bool per_segment_tables = false;   // one table set per segment (the reference's choice)
     std::vector<long long> regions;    // code positions where the statistics change (level starts);
                                        // segments of one region share a table set
+    uint32_t ckpt_part = 4096;         // symbols per decode part (power of two, 0 = no checkpoints)
 };
 
 EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cudaStream_t st);
@@ -50,6 +75,6 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes, size
 // h: the same bytes readable on the host (used to parse the block structure).  Returns the
 // number of bytes consumed.
 size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size_t n, int16_t *d_codes,
-                      cudaStream_t st);
+                      cudaStream_t st, const DecodeCheckpoints *ck = nullptr);
 
 }  // namespace fb2

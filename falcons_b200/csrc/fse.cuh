@@ -594,6 +594,17 @@ struct ReaderPF {
         p2 = word(top - 3);
         return true;
     }
+    // Starts reading below stream bit `bit` (0 <= bit <= 8 * size), e.g. at a decode checkpoint.
+    __device__ void init_at(const uint8_t *b, int32_t bit) {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(b);
+        w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+        pos = (int32_t)(a & 3) * 8 + bit;
+        const int32_t top = pos >> 5;
+        lo = (top - 1) * 32;
+        win = ((uint64_t)word(top) << 32) | word(top - 1);
+        p1 = word(top - 2);
+        p2 = word(top - 3);
+    }
     __device__ __forceinline__ uint32_t read(unsigned n) {
         pos -= (int32_t)n;
         if (pos < lo) {

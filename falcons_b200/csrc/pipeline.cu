@@ -208,7 +208,22 @@ struct Payload {
     const uint8_t *d_blocks = nullptr;  // device address of the first block header (raw frames)
     ByteView view;                   // host-readable view of the content (framed, flat or sparse)
     std::vector<uint8_t> flat;       // host copy of the content (non-raw frames)
+    DecodeCheckpoints ck;            // decode checkpoints frame, when the stream carries one
 };
+
+// Walks the skippable frames in host bytes [p, p + n) (device copy at d) and records an FB2C
+// decode checkpoint frame if there is one.
+void find_ckpt_frame(const uint8_t *p, const uint8_t *d, size_t n, DecodeCheckpoints &ck) {
+    size_t at = 0;
+    while (at + 8 <= n) {
+        uint32_t m, sz;
+        memcpy(&m, p + at, 4);
+        memcpy(&sz, p + at + 4, 4);
+        if ((m & 0xFFFFFFF0u) != 0x184D2A50u || at + 8 + sz > n) return;
+        if (parse_ckpt_header(p + at + 8, d + at + 8, sz, ck)) return;
+        at += 8 + (size_t)sz;
+    }
+}
 
 template <class T>
 void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_out, cudaStream_t st) {
@@ -265,7 +280,8 @@ void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_ou
     if ((long long)n_codes != plan.n_codes) throw std::invalid_argument("code count does not match the field");
     int16_t *codes = pool.get<int16_t>((size_t)n_codes + 16);
     tr.mark("headers parsed");
-    entropy_decode(ctx, d_flat + off, view.sub(off), (size_t)n_codes, codes, st);
+    entropy_decode(ctx, d_flat + off, view.sub(off), (size_t)n_codes, codes, st,
+                   pl.ck.n_o1 + pl.ck.n_fse ? &pl.ck : nullptr);
     tr.mark("entropy stage launched");
     void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
     interp_decompress<T>(plan, codes, unpred, d_out, ws, st);
@@ -287,6 +303,8 @@ void payload_from_host(const uint8_t *hp, const uint8_t *dp, size_t plen, Payloa
         pl.view.len = pl.L;
         pl.view.framed = true;
         pl.d_blocks = dp + 8 + fb;
+        const size_t end = 8 + zstd_raw_frame_size(pl.L);
+        if (end < plen) find_ckpt_frame(hp + end, dp + end, plen - end, pl.ck);
     } else {
         const unsigned long long fcs = zstd_frame_content_size(hf, flen);
         if (fcs != 0xFFFFFFFFFFFFFFFFULL && fcs != pl.L) throw std::invalid_argument("Invalid Falcons Zstd payload size");
@@ -409,9 +427,20 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
                     memcpy(&m, ih, 4);
                     memcpy(&sz, ih + 4, 4);
                     if (m == kSkippableMagic && ipos + 8 + sz <= len) {
-                        std::vector<uint8_t> content(sz);
-                        FB2_CUDA(cudaMemcpyAsync(content.data(), d_stream + ipos + 8, sz, cudaMemcpyDeviceToHost, st));
+                        // the index content, plus the header of a checkpoint frame right after it
+                        const size_t after = ipos + 8 + sz;
+                        const size_t extra = std::min<size_t>(len - after, 8 + kCkptHeader);
+                        std::vector<uint8_t> content(sz + extra);
+                        FB2_CUDA(cudaMemcpyAsync(content.data(), d_stream + ipos + 8, sz + extra,
+                                                 cudaMemcpyDeviceToHost, st));
                         FB2_CUDA(cudaStreamSynchronize(st));
+                        if (extra == 8 + kCkptHeader) {
+                            uint32_t m2, sz2;
+                            memcpy(&m2, content.data() + sz, 4);
+                            memcpy(&sz2, content.data() + sz + 4, 4);
+                            if (m2 == kSkippableMagic && after + 8 + sz2 <= len)
+                                parse_ckpt_header(content.data() + sz + 8, d_stream + after + 8, sz2, pl.ck);
+                        }
                         if (SparseIndex::parse(content.data(), sz, idx)) {
                             pl.raw = true;
                             pl.d_blocks = d_stream + hs + 8 + fb;

@@ -191,3 +191,57 @@ def test_device_resident_path_uses_header_index(cuda, reference, rel):
     before = __import__("falcons_b200")._lib.lib().falcons_kernel_launches()
     D.decompress(s, torch.float32)
     assert __import__("falcons_b200")._lib.lib().falcons_kernel_launches() > before
+
+
+def _ckpt_frame(buf):
+    """(tag offset, o1_part, fse_part, n_o1, n_fse) of the FB2C checkpoint frame at the stream's end."""
+    b = buf.tobytes()
+    pos = b.rfind(b"FB2C")
+    assert pos >= 8
+    magic, size = np.frombuffer(b[pos - 8:pos], np.uint32)
+    assert magic == 0x184D2A5B and pos + size == len(b)
+    o1_part, fse_part = np.frombuffer(b[pos + 8:pos + 16], np.uint32)
+    n_o1, n_fse = np.frombuffer(b[pos + 16:pos + 32], np.uint64)
+    assert size == 32 + 12 * int(n_o1) + 8 * int(n_fse)
+    return pos, int(o1_part), int(fse_part), int(n_o1), int(n_fse)
+
+
+def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference):
+    """Streams carry decode checkpoints (a skippable frame the reference ignores); the GPU decodes
+    every chain and FSE block as independent parts from them, and a damaged checkpoint frame only
+    makes it decode sequentially, with the same result."""
+    import torch
+    from falcons_b200 import api, device as D, synth
+    x = synth.spectral_field((128, 128, 128), seed=6)
+    conf = _conf(api, x.shape, mode="REL", rel=1e-4)
+    buf, _ = api.falcons.compress(x.copy(), conf, copy=True)
+    pos, o1_part, fse_part, n_o1, n_fse = _ckpt_frame(buf)
+    assert o1_part == 4096 and fse_part == 4096 and n_o1 > 100 and n_fse > 10
+    y_ref = reference.decompress(buf.tobytes(), np.float32, x.size).ravel()
+    y, _ = api.falcons.decompress(buf, np.float32, x.shape)
+    np.testing.assert_array_equal(np.asarray(y).ravel(), y_ref)
+    yd, _ = D.decompress(torch.from_numpy(buf.copy()).to(cuda), torch.float32)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(yd.cpu().numpy(), y_ref)
+    arr = pos + 32
+    damaged = []
+    b1 = buf.copy()                                   # a chain checkpoint's state
+    b1[arr + 12 * (n_o1 // 2) + 8] ^= 1
+    damaged.append(b1)
+    b2 = buf.copy()                                   # a chain checkpoint's bit position
+    b2[arr + 12 * 3] ^= 4
+    damaged.append(b2)
+    b3 = buf.copy()                                   # an FSE block checkpoint's bit position
+    b3[arr + 12 * n_o1 + 8 * (n_fse // 2)] ^= 2
+    damaged.append(b3)
+    b4 = buf.copy()                                   # a count that does not match the stream
+    b4[pos + 16] ^= 1
+    damaged.append(b4)
+    for bad in damaged:
+        yb, _ = api.falcons.decompress(bad, np.float32, x.shape)
+        np.testing.assert_array_equal(np.asarray(yb).ravel(), y_ref)
+        ybd, _ = D.decompress(torch.from_numpy(bad.copy()).to(cuda), torch.float32)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(ybd.cpu().numpy(), y_ref)
+    # the reference decoder skips the frame, damaged or not
+    np.testing.assert_array_equal(reference.decompress(damaged[0].tobytes(), np.float32, x.size).ravel(), y_ref)
