@@ -105,6 +105,14 @@ void Assembler::run(Pool &pool, uint8_t *d_out, cudaStream_t st) {
 }
 
 bool SparseIndex::read(void *dst, unsigned long long o, size_t n) const {
+    // reads are mostly in increasing order: try the entry of the previous read and the next one
+    for (size_t e = last; e < off.size() && e < last + 2; e++) {
+        if (off[e] <= o && o + n <= off[e] + len[e]) {
+            memcpy(dst, bytes.data() + pos[e] + (o - off[e]), n);
+            last = e;
+            return true;
+        }
+    }
     // last entry with off <= o
     size_t lo = 0, hi = off.size();
     while (lo < hi) {
@@ -116,6 +124,7 @@ bool SparseIndex::read(void *dst, unsigned long long o, size_t n) const {
     const size_t e = lo - 1;
     if (o + n > off[e] + len[e]) return false;
     memcpy(dst, bytes.data() + pos[e] + (o - off[e]), n);
+    last = e;
     return true;
 }
 
@@ -143,6 +152,13 @@ bool SparseIndex::parse(const uint8_t *c, size_t size, SparseIndex &out) {
     for (size_t i = 1; i < out.off.size(); i++)
         if (out.off[i] < out.off[i - 1]) return false;
     return true;
+}
+
+size_t Assembler::index_frame_size() const {
+    size_t n = 16;
+    for (auto &r : host_refs) n += 12 + (size_t)pieces[r.first].len;
+    for (auto &sh : shadows) n += 12 + sh.second.size();
+    return n;
 }
 
 std::vector<uint8_t> Assembler::index_frame() const {

@@ -97,6 +97,7 @@ struct SparseIndex {
     std::vector<uint32_t> len;
     std::vector<size_t> pos;               // into bytes
     std::vector<uint8_t> bytes;
+    mutable size_t last = 0;               // entry of the previous read
     // Returns false when [o, o+n) is not fully covered by one entry.
     bool read(void *dst, unsigned long long o, size_t n) const;
     static bool parse(const uint8_t *content, size_t size, SparseIndex &out);
@@ -114,6 +115,7 @@ struct Assembler {
         shadows.push_back({pos, std::vector<uint8_t>(static_cast<const uint8_t *>(b), static_cast<const uint8_t *>(b) + n)});
     }
     std::vector<uint8_t> index_frame() const;
+    size_t index_frame_size() const;
     void dev(const void *src, size_t len) {
         if (!len) return;
         pieces.push_back(Piece{static_cast<const uint8_t *>(src), pos, len});
@@ -123,8 +125,13 @@ struct Assembler {
         if (!len) return;
         const size_t off = host.size();
         host.insert(host.end(), static_cast<const uint8_t *>(p), static_cast<const uint8_t *>(p) + len);
-        host_refs.push_back({pieces.size(), off});
-        pieces.push_back(Piece{nullptr, pos, len});
+        if (!host_refs.empty() && host_refs.back().first + 1 == pieces.size() &&
+            host_refs.back().second + pieces.back().len == off) {
+            pieces.back().len += len;  // extends the previous host piece (one gather piece, one index entry)
+        } else {
+            host_refs.push_back({pieces.size(), off});
+            pieces.push_back(Piece{nullptr, pos, len});
+        }
         pos += len;
     }
     template <class T>
@@ -154,7 +161,7 @@ struct Assembler {
     // Writes [u64 pos][zstd raw-block frame of the layout] to d_out; returns the bytes written.
     size_t run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st);
     size_t framed_size() const {
-        return 8 + zstd_raw_frame_size(pos) + (with_index ? index_frame().size() + tail_len : 0);
+        return 8 + zstd_raw_frame_size(pos) + (with_index ? index_frame_size() + tail_len : 0);
     }
 };
 

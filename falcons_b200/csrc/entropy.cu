@@ -906,41 +906,149 @@ __global__ void k_o1_norm(const uint32_t *__restrict__ hist, int total_tables, u
     for (int s = 0; s < O1_NSYM; s++) freq[s] = (uint16_t)f[s];
 }
 
-__global__ void __launch_bounds__(32) k_o1_ctable(const uint16_t *__restrict__ nf, uint16_t *__restrict__ stab,
-                                                 fse::SymTT *__restrict__ stt, uint8_t *__restrict__ scratch,
-                                                 int *__restrict__ err) {
-    (void)scratch;
-    __shared__ uint8_t sym[O1_M];
-    if (threadIdx.x != 0) return;
-    const size_t t = blockIdx.x;
+// ---- tANS tables for 15 contexts x 256 symbols, built by a whole CTA per table (zfse
+// fse_compress.c FSE_buildCTable_wksp / fse_decompress.c FSE_buildDTable, restated in parallel).
+constexpr int kTabThreads = 256;
+struct TabSmem {
     int16_t norm[O1_NSYM];
-    for (int s = 0; s < O1_NSYM; s++) norm[s] = (int16_t)nf[t * O1_NSYM + s];
-    if (!fse::build_ctable(stab + t * O1_M, stt + t * O1_NSYM, sym, norm, O1_NSYM - 1, O1_PB)) atomicExch(err, 4);
-}
+    uint32_t cum[O1_NSYM + 1];   // cells before every symbol (a -1 symbol holds one cell)
+    uint32_t occ[O1_NSYM + 1];   // spread occurrences before every symbol (positive counts only)
+    uint32_t cnt[O1_NSYM];       // running per-symbol counters of the rank pass
+    uint32_t part[kTabThreads];
+    uint8_t sym[O1_M];
+    int bad;
+};
 
-// Decode table of one context with everything a decode step needs in one 32-bit word:
-//   bits 0-12 next state base, 13-16 bits to read, 17-20 context of the decoded code,
-//   bit 21 escape (value from the side stream), bits 22-31 the decoded code (signed).
-__global__ void __launch_bounds__(128) k_o1_dtable(const uint16_t *__restrict__ nf, uint32_t *__restrict__ dt,
-                                                 uint8_t *__restrict__ scratch, int *__restrict__ err) {
-    (void)scratch;
-    __shared__ uint8_t sym[O1_M];
-    __shared__ fse::DEntry e[O1_M];
-    const size_t t = blockIdx.x;
+// The spread (fse::spread): symbol s takes the occurrences occ[s] .. occ[s+1]-1 of the visit order
+// j -> (j * step) & mask that skips the cells above `high` (the -1 symbols' cells).  Every thread
+// maps one run of j; a block scan of the kept visits gives each its occurrence number.
+__device__ void cta_spread(TabSmem &w, unsigned tl) {
+    const uint32_t tsize = 1u << tl, mask = tsize - 1, step = fse::table_step(tsize);
     if (threadIdx.x == 0) {
-        int16_t norm[O1_NSYM];
-        for (int s = 0; s < O1_NSYM; s++) norm[s] = (int16_t)nf[t * O1_NSYM + s];
-        if (!fse::build_dtable(e, norm, O1_NSYM - 1, O1_PB, sym)) atomicExch(err, 5);
+        uint32_t c = 0, o = 0, high = tsize - 1;
+        for (int s2 = 0; s2 < O1_NSYM; s2++) {
+            w.cum[s2] = c;
+            w.occ[s2] = o;
+            const int nn = w.norm[s2];
+            if (nn == -1) {
+                w.sym[high--] = (uint8_t)s2;
+                c += 1;
+            } else if (nn > 0) {
+                c += (uint32_t)nn;
+                o += (uint32_t)nn;
+            }
+        }
+        w.cum[O1_NSYM] = c;
+        w.occ[O1_NSYM] = o;
+        w.bad = c != tsize;
     }
     __syncthreads();
-    for (int u = threadIdx.x; u < O1_M; u += blockDim.x) {
-        const fse::DEntry d = e[u];
-        const bool esc = d.symbol == O1_NSYM - 1;
-        const int code = esc ? 0 : unzz(d.symbol);
-        const int ctx = esc ? 0 : o1_ctx(code);
-        dt[t * O1_M + u] = (uint32_t)d.newState | ((uint32_t)d.nbBits << 13) | ((uint32_t)ctx << 17) |
-                           ((uint32_t)esc << 21) | ((uint32_t)(code & 0x3FF) << 22);
+    const uint32_t high = tsize - 1 - (w.cum[O1_NSYM] - w.occ[O1_NSYM]);
+    const uint32_t per = tsize / blockDim.x;  // tsize is a multiple of the block size
+    const uint32_t j0 = threadIdx.x * per;
+    uint32_t kept = 0;
+    for (uint32_t j = j0; j < j0 + per; j++) kept += ((j * step) & mask) <= high;
+    w.part[threadIdx.x] = kept;
+    __syncthreads();
+    uint32_t k = 0;
+    for (uint32_t t2 = 0; t2 < threadIdx.x; t2++) k += w.part[t2];
+    for (uint32_t j = j0; j < j0 + per; j++) {
+        const uint32_t pos = (j * step) & mask;
+        if (pos > high) continue;
+        int lo = 0, hi = O1_NSYM;  // the symbol whose occurrences hold k: occ[lo] <= k < occ[lo+1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (w.occ[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        w.sym[pos] = (uint8_t)lo;
+        k++;
     }
+    __syncthreads();
+}
+
+// For every cell u in increasing order, f(u, s, rank) with rank = the cells of symbol s before u
+// (warp 0, 32 cells at a time with match ranks).
+template <class F>
+__device__ void cta_ranks(TabSmem &w, uint32_t tsize, F &&f) {
+    for (int s2 = threadIdx.x; s2 < O1_NSYM; s2 += blockDim.x) w.cnt[s2] = 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const unsigned lane = threadIdx.x;
+        for (uint32_t u0 = 0; u0 < tsize; u0 += 32) {
+            const uint32_t u = u0 + lane;
+            const unsigned sy = w.sym[u];
+            const unsigned peers = __match_any_sync(0xffffffffu, sy);
+            const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+            f(u, sy, w.cnt[sy] + rank);
+            __syncwarp();
+            if (rank == (unsigned)__popc(peers) - 1u) w.cnt[sy] += rank + 1;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kTabThreads) k_o1_ctable(const uint16_t *__restrict__ nf, uint16_t *__restrict__ stab,
+                                                         fse::SymTT *__restrict__ stt, uint8_t *__restrict__ scratch,
+                                                         int *__restrict__ err) {
+    (void)scratch;
+    __shared__ TabSmem w;
+    const size_t t = blockIdx.x;
+    for (int s2 = threadIdx.x; s2 < O1_NSYM; s2 += blockDim.x) w.norm[s2] = (int16_t)nf[t * O1_NSYM + s2];
+    __syncthreads();
+    cta_spread(w, O1_PB);
+    if (w.bad) {
+        if (threadIdx.x == 0) atomicExch(err, 4);
+        return;
+    }
+    uint16_t *st = stab + t * O1_M;
+    cta_ranks(w, O1_M, [&](uint32_t u, unsigned sy, uint32_t r) { st[w.cum[sy] + r] = (uint16_t)(O1_M + u); });
+    for (int s2 = threadIdx.x; s2 < O1_NSYM; s2 += blockDim.x) {
+        const int nn = w.norm[s2];
+        const uint32_t total = w.cum[s2];
+        fse::SymTT tt;
+        if (nn == 0) {
+            tt.deltaNbBits = ((O1_PB + 1) << 16) - O1_M;
+            tt.deltaFindState = 0;
+        } else if (nn == -1 || nn == 1) {
+            tt.deltaNbBits = (O1_PB << 16) - O1_M;
+            tt.deltaFindState = (int32_t)total - 1;
+        } else {
+            const uint32_t maxBitsOut = O1_PB - fse::highbit32((uint32_t)(nn - 1));
+            const uint32_t minStatePlus = (uint32_t)nn << maxBitsOut;
+            tt.deltaNbBits = (maxBitsOut << 16) - minStatePlus;
+            tt.deltaFindState = (int32_t)total - nn;
+        }
+        stt[t * O1_NSYM + s2] = tt;
+    }
+}
+
+// Decode tables, one packed u32 per cell: bits 0-12 newState, 13-16 nbBits, 17-20 the context
+// of the decoded code, 21 escape, 22-31 the code (10 bits, two's complement).
+__global__ void __launch_bounds__(kTabThreads) k_o1_dtable(const uint16_t *__restrict__ nf, uint32_t *__restrict__ dt,
+                                                         uint8_t *__restrict__ scratch, int *__restrict__ err) {
+    (void)scratch;
+    __shared__ TabSmem w;
+    const size_t t = blockIdx.x;
+    for (int s2 = threadIdx.x; s2 < O1_NSYM; s2 += blockDim.x) w.norm[s2] = (int16_t)nf[t * O1_NSYM + s2];
+    __syncthreads();
+    cta_spread(w, O1_PB);
+    if (w.bad) {
+        if (threadIdx.x == 0) atomicExch(err, 5);
+        return;
+    }
+    uint32_t *d = dt + t * O1_M;
+    cta_ranks(w, O1_M, [&](uint32_t u, unsigned sy, uint32_t r) {
+        const int nn = w.norm[sy];
+        const uint32_t ns = (nn == -1 ? 1u : (uint32_t)nn) + r;
+        const uint32_t nb = O1_PB - fse::highbit32(ns);
+        const uint32_t newState = (ns << nb) - O1_M;
+        const bool esc = sy == O1_NSYM - 1;
+        const int code = esc ? 0 : unzz(sy);
+        const int ctx = esc ? 0 : o1_ctx(code);
+        d[u] = newState | (nb << 13) | ((uint32_t)ctx << 17) | ((uint32_t)esc << 21) | ((uint32_t)(code & 0x3FF) << 22);
+    });
 }
 
 // One thread per (segment, chunk) chain: reverse tANS encode with per-symbol context tables
@@ -2021,7 +2129,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint8_t *spread = pool.get<uint8_t>((size_t)ntab * O1_M);
         int *d_err = pool.get<int>(8);
         FB2_CUDA(cudaMemsetAsync(d_err, 0, 32, st));
-        k_o1_ctable<<<ntab, 32, 0, st>>>(nf, stab, stt, spread, d_err);
+        k_o1_ctable<<<ntab, kTabThreads, 0, st>>>(nf, stab, stt, spread, d_err);
         FB2_CHECK_LAUNCH();
         // chain output slots
         const long long nchains = S * kMaxK;
@@ -2336,7 +2444,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         }
         uint32_t *dt = pool.get<uint32_t>((size_t)ntab * O1_M);
         uint8_t *spread = pool.get<uint8_t>(16);
-        k_o1_dtable<<<ntab, 128, 0, st>>>(nf, dt, spread, d_err);
+        k_o1_dtable<<<ntab, kTabThreads, 0, st>>>(nf, dt, spread, d_err);
         FB2_CHECK_LAUNCH();
         for (auto &c : chains) c.table = uid[c.table];
         // checkpoint base of every chain; the checkpoints are used only if their count matches
