@@ -1312,8 +1312,8 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t 
 //      staged words into place (words shared with a neighbour are merged with atomicOr);
 //   5. every part start is a decode checkpoint: state, bit position, context and escape count.
 // The stream is bit-identical to a sequential encoder's (the tANS states are fully determined).
-constexpr int kSpecThreads = 256;
-constexpr int kSpecSlots = 11;  // 11 x 16 KiB state tables + 30 KiB symbol transforms in shared memory
+constexpr int kSpecThreads = 1024;
+constexpr int kSpecSlots = 10;  // 10 x 16 KiB state tables + 30 KiB symbol transforms in shared memory
 constexpr size_t kSpecSmem = (size_t)O1_NCTX * O1_NSYM * sizeof(fse::SymTT) + (size_t)kSpecSlots * O1_M * 2;
 constexpr int kSparseShift = 6;  // kept speculative states: every 64th index
 struct SpecCta {
@@ -1378,7 +1378,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, uint16_t *__restrict__ sparse,
     uint32_t *__restrict__ stage, uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
     unsigned long long *__restrict__ blen, uint32_t part, O1Ckpt *__restrict__ cks,
-    const unsigned long long *__restrict__ ck_off, int *__restrict__ err) {
+    const unsigned long long *__restrict__ ck_off, uint32_t ck_every, int *__restrict__ err) {
     extern __shared__ uint4 smem_raw[];
     EncRec *rec = reinterpret_cast<EncRec *>(smem_raw);
     uint16_t *sst = reinterpret_cast<uint16_t *>(rec + O1_NCTX * O1_NSYM);
@@ -1563,9 +1563,10 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         }
         if (sh && w0 + nwords < wend) store(w0 + nwords, prev >> (32 - sh));
         if (p == 0) blen[chain] = ((unsigned long long)off + bits + 7) / 8;
-        // 5. decode checkpoint at the part start: the state the decoder holds before index a
-        if (p > 0 && cks)
-            cks[ck_off[chain] + p - 1] = O1Ckpt{off + bits, esc_below, (uint16_t)(s_exit[t] & (O1_M - 1)),
+        // 5. decode checkpoint at every ck_every-th part start: the state the decoder holds
+        // before index a
+        if (p > 0 && cks && (uint32_t)p % ck_every == 0)
+            cks[ck_off[chain] + (uint32_t)p / ck_every - 1] = O1Ckpt{off + bits, esc_below, (uint16_t)(s_exit[t] & (O1_M - 1)),
                                                 (uint16_t)(__ldg(keys + a) >> 8)};
     }
 }
@@ -1574,7 +1575,8 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
 // starting bit position, state, context and escape offset).  The CTA's parts share one table set,
 // staged in shared memory as for k_o1_decode_smem.  Each part that ends at a checkpoint checks that
 // it arrived there (state, context, bit position, escapes); a mismatch sets err[1].
-__global__ void __launch_bounds__(kChainThreads) k_o1_decode_parts(const uint8_t *__restrict__ in,
+constexpr int kPartThreads = 512;
+__global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t *__restrict__ in,
                                                                  const DecChain *__restrict__ chains,
                                                                  const DecPart *__restrict__ parts,
                                                                  const ChainCta *__restrict__ ctas,
@@ -2068,9 +2070,10 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         // encoder part size (also the decode checkpoint spacing): a chain's parts fit one CTA
         unsigned long long max_cs = 1;
         for (const auto &sg : segs) max_cs = std::max<unsigned long long>(max_cs, sg.cs);
-        uint32_t enc_part = cc.o1_part ? cc.o1_part : 4096u;
+        uint32_t enc_part = std::min<uint32_t>(cc.o1_part ? cc.o1_part : 1024u, 1024u);
         while ((max_cs + enc_part - 1) / enc_part > (unsigned long long)kSpecThreads) enc_part *= 2;
-        if (cc.o1_part) cc.o1_part = enc_part;
+        if (cc.o1_part && cc.o1_part < enc_part) cc.o1_part = enc_part;
+        const uint32_t ck_every = cc.o1_part ? cc.o1_part / enc_part : 1u;
         const int ppc = (int)((max_cs + enc_part - 1) / enc_part);
         // decode checkpoints of every chain: one before each index lo + q * part, q >= 1
         const long long nchains_all = S * kMaxK;
@@ -2164,7 +2167,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             FB2_CHECK_LAUNCH();
             enable_big_smem();
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
-                keys, d_segs, d_ctas, stab, stt, sparse, stage, slots, d_soff, blen, enc_part, o1ck, d_ck_off, d_err);
+                keys, d_segs, d_ctas, stab, stt, sparse, stage, slots, d_soff, blen, enc_part, o1ck, d_ck_off, ck_every,
+                d_err);
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
         }
@@ -2478,10 +2482,10 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                         part_table.push_back(chains[i].table);
                     }
                 }
-                std::vector<ChainCta> ctas = chain_ctas(part_table, maps, revs, kChainThreads);
+                std::vector<ChainCta> ctas = chain_ctas(part_table, maps, revs, kPartThreads);
                 ChainCta *d_ctas = h2d(pool, ctas, st);
                 DecPart *d_parts = h2d(pool, parts, st);
-                k_o1_decode_parts<<<(unsigned)ctas.size(), kChainThreads, kDecSlots * O1_M * 4, st>>>(
+                k_o1_decode_parts<<<(unsigned)ctas.size(), kPartThreads, kDecSlots * O1_M * 4, st>>>(
                     d_in, dch, d_parts, d_ctas, dt, ovf, ovf_total, o1ck, o1_part, d_codes, d_err);
                 FB2_CHECK_LAUNCH();
             } else {

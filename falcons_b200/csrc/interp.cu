@@ -557,8 +557,141 @@ __global__ void __launch_bounds__(kTileThreads) k_esc_scatter(const int16_t *__r
     }
 }
 
+// Cubic interior predictor (Interpolators.hpp cubic: (9 (b + c) - a - d) / 16) and linear.
+template <class T>
+__device__ __forceinline__ T cubic_pred(T a, T b, T c, T d) {
+    using A = Arith<T>;
+    T t = A::mul(A::add(b, c), T(9));
+    t = A::sub(t, a);
+    t = A::sub(t, d);
+    return A::mul(t, T(0.0625));
+}
+template <class T>
+__device__ __forceinline__ T linear_pred(T a, T b) {
+    return Arith<T>::mul(Arith<T>::add(a, b), T(0.5));
+}
+
+// Quantizes (compress: v is the target's value, recon goes back to *xp unless `skip`) or
+// reconstructs (decompress) one target; p is its position in the code stream.
+template <class T, bool DECOMP>
+__device__ __forceinline__ void pass_target(T *__restrict__ xp, T v, T pred, int16_t *__restrict__ cp,
+                                            T *__restrict__ ep, const QParams &qp, bool skip) {
+    if (!DECOMP) {
+        T recon;
+        const int q = quantize<T>(v, pred, qp, recon);
+        *cp = (int16_t)q;
+        if (q == -qp.radius) *ep = v;
+        else if (!skip) *xp = recon;
+    } else {
+        const int q = *cp;
+        *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : *ep;
+    }
+}
+
+// Row-buffer passes (KIND_ROW): one thread per column, kRowsPerBlock consecutive target rows per
+// block (their operand rows overlap, so most operand loads hit L1), grid (columns, row groups,
+// outer).  Interior targets take the cubic (or linear) formula without evaluating the edge rules.
+constexpr int kRowsPerBlock = 8;
+template <class T, bool DECOMP>
+__global__ void __launch_bounds__(kPassThreads) k_row_fast(const PassLaunch L, T *__restrict__ x,
+                                                          int16_t *__restrict__ codes, T *__restrict__ esc,
+                                                          const QParams qp) {
+    const long long cstride = (long long)gridDim.x * blockDim.x;
+    const long long st = L.step;
+    for (long long a = blockIdx.z; a < L.A; a += gridDim.z) {
+        for (long long bg = blockIdx.y; bg * kRowsPerBlock < L.B; bg += gridDim.y)
+        for (long long b = bg * kRowsPerBlock; b < min(L.B, (bg + 1) * kRowsPerBlock); b++) {
+            const int t = L.t0 + 2 * (int)b;
+            const bool interior = L.cubic ? (t >= 3 && t <= L.n - 5) : (t < L.n - 1);
+            const Rule r = row_rule(L.cubic, t, L.n, L.skip);
+            const long long prow = L.p_base + (a * L.rows_in_group + b + L.b_off) * L.C;
+            for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < L.C; c += cstride) {
+                T *xl = x + a * L.sa + c * L.sc;
+                T pred;
+                if (interior) {
+                    pred = L.cubic ? cubic_pred<T>(__ldg(xl + (t - 3) * st), __ldg(xl + (t - 1) * st),
+                                                   __ldg(xl + (t + 1) * st), __ldg(xl + (t + 3) * st))
+                                   : linear_pred<T>(__ldg(xl + (t - 1) * st), __ldg(xl + (t + 1) * st));
+                } else {
+                    const T o0 = __ldg(xl + (long long)r.o0 * st);
+                    const T o1 = r.f != F_EQUAL ? __ldg(xl + (long long)r.o1 * st) : o0;
+                    const T o2 = r.f >= F_QUAD1 ? __ldg(xl + (long long)r.o2 * st) : o0;
+                    const T o3 = r.f == F_CUBIC ? __ldg(xl + (long long)r.o3 * st) : o0;
+                    pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+                }
+                T *xp = xl + (long long)t * st;
+                pass_target<T, DECOMP>(xp, DECOMP ? T(0) : *xp, pred, codes + prow + c, esc + prow + c, qp, L.skip);
+            }
+        }
+    }
+}
+
+// Line passes (KIND_LINE) whose line fits kLineMax bytes: one warp per line; the warp stages the
+// line in shared memory with coalesced loads (every value read once), then predicts its targets
+// (odd positions; their operands are the even positions, which this pass never writes).
+// Interior targets take the cubic (or linear) formula without evaluating the edge rules.
+constexpr int kLineThreads = 256;
+constexpr int kLineMax = 4096;
+template <class T, bool DECOMP>
+__global__ void __launch_bounds__(kLineThreads) k_line_smem(const PassLaunch L, T *__restrict__ x,
+                                                           int16_t *__restrict__ codes, T *__restrict__ esc,
+                                                           const QParams qp) {
+    __shared__ T buf[kLineThreads / 32][kLineMax / sizeof(T)];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    T *bw = buf[wid];
+    const long long nlines = L.A * L.B;
+    const long long st = L.step;
+    const int n = L.n, C = (int)L.C, odd = n / 2;
+    // cubic interior: 3 <= t <= 2 * odd - 5; linear interior: t < 2 * odd - 1
+    const int tlo = L.cubic ? 3 : 1, thi = L.cubic ? 2 * odd - 5 : 2 * odd - 3;
+    for (long long l = (long long)blockIdx.x * (kLineThreads / 32) + wid; l < nlines;
+         l += (long long)gridDim.x * (kLineThreads / 32)) {
+        const long long a = l / L.B, b = l - a * L.B;
+        T *xl = x + a * L.sa + b * L.sb;
+        __syncwarp();
+        if (st == 1) {
+            for (int i = lane; i < n; i += 32) bw[i] = xl[i];
+        } else {
+            for (int i = lane; i < n; i += 32) bw[i] = xl[(long long)i * st];
+        }
+        __syncwarp();
+        int16_t *cl = codes + L.p_base + l * L.C;
+        T *el = esc + L.p_base + l * L.C;
+        for (int cc = lane; cc < C; cc += 32) {
+            const int t = 1 + 2 * cc;
+            T pred;
+            if (t >= tlo && t <= thi) {
+                pred = L.cubic ? cubic_pred<T>(bw[t - 3], bw[t - 1], bw[t + 1], bw[t + 3]) : linear_pred<T>(bw[t - 1], bw[t + 1]);
+            } else {
+                const Rule r = line_rule(L.cubic, t, n);
+                const T o0 = bw[r.o0];
+                const T o1 = r.f != F_EQUAL ? bw[r.o1] : o0;
+                const T o2 = r.f >= F_QUAD1 ? bw[r.o2] : o0;
+                const T o3 = r.f == F_CUBIC ? bw[r.o3] : o0;
+                pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+            }
+            pass_target<T, DECOMP>(xl + (long long)t * st, bw[t], pred, cl + cc, el + cc, qp, L.skip);
+        }
+    }
+}
+
 template <class T, bool DECOMP>
 void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
+    if (L.kind == KIND_ROW) {
+        dim3 grid((unsigned)std::max<long long>(1, std::min<long long>((L.C + kPassThreads - 1) / kPassThreads, 1 << 20)),
+                  (unsigned)std::min<long long>((L.B + kRowsPerBlock - 1) / kRowsPerBlock, 65535),
+                  (unsigned)std::min<long long>(L.A, 65535));
+        k_row_fast<T, DECOMP><<<grid, kPassThreads, 0, st>>>(L, x, codes, esc, qp);
+        FB2_CHECK_LAUNCH();
+        return;
+    }
+    if (L.kind == KIND_LINE && (long long)L.n * (long long)sizeof(T) <= kLineMax) {
+        const long long nlines = L.A * L.B;
+        const long long blocks = std::min<long long>((nlines + kLineThreads / 32 - 1) / (kLineThreads / 32), 148LL * 64);
+        k_line_smem<T, DECOMP><<<(unsigned)std::max<long long>(blocks, 1), kLineThreads, 0, st>>>(L, x, codes, esc, qp);
+        FB2_CHECK_LAUNCH();
+        return;
+    }
     dim3 block(kPassThreads);
     const long long gx = std::min<long long>((L.C + kPassThreads - 1) / kPassThreads, 1 << 20);
     dim3 grid((unsigned)std::max<long long>(gx, 1), (unsigned)std::min<long long>(L.B, 65535),

@@ -216,7 +216,9 @@ def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference):
     conf = _conf(api, x.shape, mode="REL", rel=1e-4)
     buf, _ = api.falcons.compress(x.copy(), conf, copy=True)
     pos, o1_part, fse_part, n_o1, n_fse = _ckpt_frame(buf)
-    assert o1_part == 4096 and fse_part == 4096 and n_o1 > 100 and n_fse > 10
+    for part in (o1_part, fse_part):
+        assert part >= 64 and part & (part - 1) == 0
+    assert n_o1 > 100 and n_fse > 10
     y_ref = reference.decompress(buf.tobytes(), np.float32, x.size).ravel()
     y, _ = api.falcons.decompress(buf, np.float32, x.shape)
     np.testing.assert_array_equal(np.asarray(y).ravel(), y_ref)
