@@ -1051,57 +1051,6 @@ __global__ void __launch_bounds__(kTabThreads) k_o1_dtable(const uint16_t *__res
     });
 }
 
-// One thread per (segment, chunk) chain: reverse tANS encode with per-symbol context tables
-// (RleFseEncoder.hpp:671-707).  tab[g] selects the table set of segment g.
-__global__ void __launch_bounds__(32) k_o1_encode(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
-                                                  int nseg, const int *__restrict__ tab,
-                                                  const uint16_t *__restrict__ stab,
-                                                  const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
-                                                  const unsigned long long *__restrict__ slot_off,
-                                                  unsigned long long *__restrict__ blen) {
-    const int chain = blockIdx.x * blockDim.x + threadIdx.x;
-    const int g = chain / kMaxK, k = chain % kMaxK;
-    if (g >= nseg) return;
-    const SegInfo sg = segs[g];
-    if (k >= sg.K) return;
-    const unsigned long long lo = sg.lo + (unsigned long long)k * sg.cs;
-    unsigned long long hi = lo + sg.cs;
-    if (hi > sg.lo + sg.n) hi = sg.lo + sg.n;
-    if (lo >= hi) {
-        blen[chain] = 0;
-        return;
-    }
-    const size_t tb = (size_t)tab[g] * O1_NCTX;
-    const uint16_t *__restrict__ S = stab + tb * O1_M;
-    const fse::SymTT *__restrict__ T = stt + tb * O1_NSYM;
-    fse::Writer32 bw;
-    const unsigned long long cap = slot_off[chain + 1] - slot_off[chain];
-    bw.init(slots + slot_off[chain], (size_t)cap);
-    unsigned long long idx = hi - 1;
-    int cur = q[idx];
-    int prev = idx > lo ? (int)__ldg(q + idx - 1) : 0;
-    fse::SymTT t = T[o1_ctx(prev) * O1_NSYM + o1_sym(cur)];
-    uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
-    uint32_t v = (nb << 16) - t.deltaNbBits;
-    uint32_t state = S[o1_ctx(prev) * O1_M + (int32_t)(v >> nb) + t.deltaFindState];
-    // walk down: the symbol at idx-1 becomes current, its predecessor is loaded one step ahead
-    int nxt = (idx >= lo + 2) ? (int)__ldg(q + idx - 2) : 0;
-    while (idx > lo) {
-        idx--;
-        cur = prev;
-        prev = idx > lo ? nxt : 0;
-        if (idx >= lo + 2) nxt = (int)__ldg(q + idx - 2);
-        const int c = o1_ctx(prev);
-        t = T[c * O1_NSYM + o1_sym(cur)];
-        nb = (state + t.deltaNbBits) >> 16;
-        bw.add(state, nb);
-        state = S[c * O1_M + (int32_t)(state >> nb) + t.deltaFindState];
-    }
-    bw.add(state, O1_PB);
-    const size_t len = bw.close();
-    blen[chain] = bw.overflow ? ~0ULL : len;
-}
-
 struct DecChain {
     unsigned long long in;      // stream byte offset
     unsigned long long inlen;   // stream length (0 = empty chunk)
@@ -1133,7 +1082,6 @@ __device__ __forceinline__ int chain_slot() {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     return lane < kMaxChainsPerCta / (kChainThreads / 32) ? lane * (kChainThreads / 32) + warp : -1;
 }
-constexpr int kEncSlots = 13;  // 13 x 8192 x u16 encode state tables = 208 KiB
 constexpr int kDecSlots = 7;   // 7 x 8192 x u32 decode tables = 224 KiB
 struct ChainCta {
     int table;
@@ -1142,98 +1090,6 @@ struct ChainCta {
     int pad;
     unsigned long long map, rev;
 };
-
-__global__ void __launch_bounds__(kChainThreads) k_o1_encode_smem(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
-                                                      const ChainCta *__restrict__ ctas,
-                                                      const uint16_t *__restrict__ stab,
-                                                      const fse::SymTT *__restrict__ stt, uint8_t *__restrict__ slots,
-                                                      const unsigned long long *__restrict__ slot_off,
-                                                      unsigned long long *__restrict__ blen,
-                                                      const uint32_t *__restrict__ nvk, uint32_t part,
-                                                      O1Ckpt *__restrict__ cks,
-                                                      const unsigned long long *__restrict__ ck_off) {
-    extern __shared__ uint4 smem_raw[];
-    uint16_t *sst = reinterpret_cast<uint16_t *>(smem_raw);
-    const ChainCta w = ctas[blockIdx.x];
-    const size_t tb = (size_t)w.table * O1_NCTX;
-    const uint16_t *__restrict__ S = stab + tb * O1_M;
-    const fse::SymTT *__restrict__ T = stt + tb * O1_NSYM;
-    for (int j = 0; j < kEncSlots; j++) {
-        const int c = (int)((w.rev >> (4 * j)) & 15);
-        if (c >= O1_NCTX) continue;
-        const uint4 *src = reinterpret_cast<const uint4 *>(S + (size_t)c * O1_M);
-        uint4 *dst = reinterpret_cast<uint4 *>(sst + (size_t)j * O1_M);
-        for (int i = threadIdx.x; i < O1_M * 2 / 16; i += blockDim.x) dst[i] = __ldg(src + i);
-    }
-    __syncthreads();
-    const int lc = chain_slot();
-    if (lc < 0 || lc >= w.count) return;
-    const int chain = w.first + lc;
-    const int g = chain / kMaxK, k = chain % kMaxK;
-    const SegInfo sg = segs[g];
-    if (k >= sg.K) return;
-    const unsigned long long lo = sg.lo + (unsigned long long)k * sg.cs;
-    unsigned long long hi = lo + sg.cs;
-    if (hi > sg.lo + sg.n) hi = sg.lo + sg.n;
-    if (lo >= hi) {
-        blen[chain] = 0;
-        return;
-    }
-    const unsigned long long map = w.map;
-    fse::Writer32 bw;
-    const unsigned long long cap = slot_off[chain + 1] - slot_off[chain];
-    bw.init(slots + slot_off[chain], (size_t)cap);
-    auto stlookup = [&](int c, int idx) -> uint32_t {
-        const int sl = (int)((map >> (4 * c)) & 15);
-        return sl < kEncSlots ? sst[sl * O1_M + idx] : __ldg(S + (size_t)c * O1_M + idx);
-    };
-    // codes are read through a 6-deep register queue (Q[i] = q[idx - i]) and the symbol transform
-    // of the next step is loaded during the current one, so no step waits on global memory
-    const long long L0 = (long long)lo;
-    long long idx = (long long)hi - 1;
-    auto ld = [&](long long i) -> int { return i >= L0 ? (int)__ldg(q + i) : 0; };
-    int Q0 = ld(idx), Q1 = ld(idx - 1), Q2 = ld(idx - 2), Q3 = ld(idx - 3), Q4 = ld(idx - 4), Q5 = ld(idx - 5);
-    int c = o1_ctx(idx > L0 ? Q1 : 0);
-    fse::SymTT t = T[c * O1_NSYM + o1_sym(Q0)];
-    uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
-    uint32_t v = (nb << 16) - t.deltaNbBits;
-    uint32_t state = stlookup(c, (int32_t)(v >> nb) + t.deltaFindState);
-    // decode checkpoints: after coding index lo + q * part (q >= 1), the decoder's state, bit
-    // position, context and escape count before it decodes that index
-    O1Ckpt *ck = cks ? cks + ck_off[chain] : nullptr;
-    const uint32_t esc_total = nvk ? nvk[chain] : 0;
-    uint32_t esc_seen = (uint32_t)(Q0 + 127) > 254u;
-    uint32_t rem = (uint32_t)((idx - L0) % part);
-    auto record = [&](long long i, int prev) {
-        ck[(i - L0) / part - 1] = O1Ckpt{bw.nw * 32 + bw.nb, esc_total - esc_seen, (uint16_t)(state & (O1_M - 1)),
-                                         (uint16_t)o1_ctx(prev)};
-    };
-    if (ck && rem == 0 && idx > L0) record(idx, Q1);
-    // advance to idx - 1
-    Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
-    idx--;
-    int cn = o1_ctx(idx > L0 ? Q1 : 0);
-    fse::SymTT tn = idx >= L0 ? T[cn * O1_NSYM + o1_sym(Q0)] : t;
-    while (idx >= L0) {
-        c = cn;
-        t = tn;
-        // prefetch for idx - 1
-        const int n0 = Q1, n1 = Q2;
-        cn = o1_ctx(idx - 1 > L0 ? n1 : 0);
-        if (idx - 1 >= L0) tn = T[cn * O1_NSYM + o1_sym(n0)];
-        nb = (state + t.deltaNbBits) >> 16;
-        bw.add(state, nb);
-        state = stlookup(c, (int32_t)(state >> nb) + t.deltaFindState);
-        esc_seen += (uint32_t)(Q0 + 127) > 254u;
-        rem = rem == 0 ? part - 1 : rem - 1;
-        if (ck && rem == 0 && idx > L0) record(idx, Q1);
-        Q0 = Q1; Q1 = Q2; Q2 = Q3; Q3 = Q4; Q4 = Q5; Q5 = ld(idx - 6);
-        idx--;
-    }
-    bw.add(state, O1_PB);
-    const size_t len = bw.close();
-    blen[chain] = bw.overflow ? ~0ULL : len;
-}
 
 __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t *__restrict__ in,
                                                       const DecChain *__restrict__ chains,
@@ -1746,8 +1602,6 @@ std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std:
 void enable_big_smem() {
     static bool done = false;
     if (done) return;
-    FB2_CUDA(cudaFuncSetAttribute(k_o1_encode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kEncSlots * O1_M * 2));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kDecSlots * O1_M * 4));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_parts, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1826,43 +1680,6 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_extract(const int16_t *__r
 }
 
 
-
-__global__ void __launch_bounds__(32) k_o1_decode(const uint8_t *__restrict__ in, const DecChain *__restrict__ chains,
-                                                 int nchains, const uint32_t *__restrict__ dt,
-                                                 const int16_t *__restrict__ ovf, unsigned long long n_ovf,
-                                                 int16_t *__restrict__ out, int *__restrict__ err) {
-    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= nchains) return;
-    const DecChain ch = chains[ci];
-    if (ch.n == 0) return;
-    fse::Reader32 br;
-    if (ch.inlen == 0 || ch.inlen >= (1ull << 28) || !br.init(in + ch.in, (uint32_t)ch.inlen)) {
-        atomicExch(err, 6);
-        return;
-    }
-    const uint32_t *__restrict__ tb = dt + (size_t)ch.table * O1_NCTX * O1_M;
-    uint32_t state = br.read(O1_PB);
-    uint32_t ctx = 0;
-    const int16_t *__restrict__ ov = ovf + ch.ovf;
-    const uint32_t nov = (uint32_t)min((unsigned long long)0x7fffffff, n_ovf - ch.ovf);
-    int16_t *o = out + ch.lo;
-    const uint32_t n = (uint32_t)ch.n;
-    uint32_t oi = 0;
-    int next_ov = nov ? (int)__ldg(ov) : 0;  // escape value prefetched one step ahead
-    for (uint32_t j = 0; j < n; j++) {
-        const uint32_t e = __ldg(tb + ctx * O1_M + state);
-        const bool esc = (e >> 21) & 1u;
-        const int code = esc ? next_ov : ((int)e >> 22);
-        ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
-        oi += esc;
-        if (esc) next_ov = oi < nov ? (int)__ldg(ov + oi) : 0;
-        o[j] = (int16_t)code;
-        state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
-    }
-    if (oi > nov) atomicExch(err, 7);
-    // the step after the last symbol reads at most 13 bits below the stream start
-    if (br.pos < -16) atomicExch(err, 8);
-}
 
 __global__ void k_m0_scatter(const uint32_t *__restrict__ runs, const uint32_t *__restrict__ vals,
                              const unsigned long long *__restrict__ start, long long nv, long long n,
