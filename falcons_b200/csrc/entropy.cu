@@ -635,7 +635,8 @@ __global__ void k_gamma_unpack(const uint8_t *__restrict__ cls, const unsigned l
                                long long n, const unsigned long long *__restrict__ gstart, int G,
                                const unsigned long long *__restrict__ gman, const uint8_t *__restrict__ base,
                                const unsigned long long *__restrict__ gman_len, uint32_t *__restrict__ v,
-                               int *__restrict__ err) {
+                               int *__restrict__ err, const unsigned long long *__restrict__ gdst,
+                               int16_t *__restrict__ ovf) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int k = cls[i];
         uint32_t m = 0;
@@ -657,7 +658,13 @@ __global__ void k_gamma_unpack(const uint8_t *__restrict__ cls, const unsigned l
                 m = (uint32_t)((acc >> drop) & ((1ull << k) - 1));
             }
         }
-        v[i] = (k <= 31) ? ((1u << k) | m) : 0u;
+        const uint32_t val = (k <= 31) ? ((1u << k) | m) : 0u;
+        if (ovf) {  // escape values: zigzag + 1 gamma-coded, written in place as int16
+            const int g = find_group(gstart, G, (unsigned long long)i);
+            ovf[gdst[g] + ((unsigned long long)i - gstart[g])] = (int16_t)unzz(val - 1u);
+        } else {
+            v[i] = val;
+        }
     }
 }
 
@@ -830,15 +837,23 @@ __global__ void __launch_bounds__(1024) k_o1_hist(const int16_t *__restrict__ q,
     for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) h[i] = 0;
     if (threadIdx.x < kMaxK) esc[threadIdx.x] = 0;
     __syncthreads();
-    for (unsigned long long r = threadIdx.x; r < sg.n; r += blockDim.x) {
-        const unsigned long long i = sg.lo + r;
-        const int k = (int)(r / sg.cs);
-        const bool first = (r % sg.cs) == 0;
-        const int code = q[i];
-        const int prev = first ? 0 : (int)q[i - 1];
-        const int s = o1_sym(code);
-        atomicAdd(&h[o1_ctx(prev) * O1_NSYM + s], 1u);
-        if (s == O1_NSYM - 1) atomicAdd(&esc[k], 1u);
+    for (int k = 0; k < sg.K; k++) {
+        const unsigned long long c0 = (unsigned long long)k * sg.cs;
+        const unsigned long long c1 = min(c0 + sg.cs, sg.n);
+        uint32_t ne = 0;
+        // warp-uniform loop (the escape count is reduced over the warp after it)
+        for (unsigned long long rb = c0 + (threadIdx.x & ~31u); rb < c1; rb += blockDim.x) {
+            const unsigned long long r = rb + (threadIdx.x & 31);
+            if (r < c1) {
+                const unsigned long long i = sg.lo + r;
+                const int prev = r == c0 ? 0 : (int)q[i - 1];
+                const int s = o1_sym((int)q[i]);
+                atomicAdd(&h[o1_ctx(prev) * O1_NSYM + s], 1u);
+                ne += s == O1_NSYM - 1;
+            }
+        }
+        ne = __reduce_add_sync(0xffffffffu, ne);
+        if ((threadIdx.x & 31) == 0 && ne) atomicAdd(&esc[k], ne);
     }
     __syncthreads();
     uint32_t *gh = hist + (size_t)blockIdx.x * O1_NCTX * O1_NSYM;
@@ -1702,7 +1717,8 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
                   const std::vector<size_t> &cls_off, const std::vector<size_t> &man_off,
                   const std::vector<size_t> &man_len, const std::vector<unsigned long long> &gstart,
                   uint32_t *d_vals, int *d_err, cudaStream_t st, const FseCkpt *d_fck = nullptr,
-                  uint32_t fpart = 0, unsigned long long n_fck = 0) {
+                  uint32_t fpart = 0, unsigned long long n_fck = 0, const unsigned long long *d_gdst = nullptr,
+                  int16_t *d_ovf = nullptr) {
     const int G = (int)gstart.size() - 1;
     const long long T = (long long)gstart.back();
     if (T == 0) return;
@@ -1735,16 +1751,11 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     unsigned long long *d_gstart = h2d(pool, gstart, st);
     unsigned long long *d_gman = h2d(pool, gman, st);
     unsigned long long *d_glen = h2d(pool, glen, st);
-    k_gamma_unpack<<<grid_for(T, 256), 256, 0, st>>>(cls, boff, T, d_gstart, G, d_gman, d, d_glen, d_vals, d_err);
+    k_gamma_unpack<<<grid_for(T, 256), 256, 0, st>>>(cls, boff, T, d_gstart, G, d_gman, d, d_glen, d_vals, d_err,
+                                                    d_gdst, d_ovf);
     FB2_CHECK_LAUNCH();
 }
 
-__global__ void k_ovf_convert(const uint32_t *gv, const unsigned long long *src, const unsigned long long *dst,
-                              const unsigned long long *cnt, int ng, int16_t *out) {
-    for (int g = blockIdx.x; g < ng; g += gridDim.x)
-        for (unsigned long long i = threadIdx.x; i < cnt[g]; i += blockDim.x)
-            out[dst[g] + i] = (int16_t)unzz(gv[src[g] + i] - 1u);
-}
 
 
 }  // namespace
@@ -2213,30 +2224,19 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         // escape values
         int16_t *ovf = pool.get<int16_t>(ovf_total + 1);
         {
-            uint32_t *gv = pool.get<uint32_t>(gstart.back() + 1);
-            gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, gv, d_err, st, fck, f_part, n_fck);
-            // place: raw blocks are copied, gamma groups converted
+            // raw blocks are copied; gamma groups are unpacked straight into their place
             std::vector<Piece> pcs;
-            size_t gi = 0;
-            std::vector<unsigned long long> conv_src, conv_dst, conv_n;
+            std::vector<unsigned long long> conv_dst;
             for (auto &r : raws) {
-                if (r.off != ~size_t(0)) {
-                    pcs.push_back(Piece{d_in + r.off, r.dst * 2, r.n * 2});
-                } else {
-                    conv_src.push_back(gstart[gi]);
-                    conv_dst.push_back(r.dst);
-                    conv_n.push_back(r.n);
-                    gi++;
-                }
+                if (r.off != ~size_t(0)) pcs.push_back(Piece{d_in + r.off, r.dst * 2, r.n * 2});
+                else conv_dst.push_back(r.dst);
+            }
+            if (!conv_dst.empty()) {
+                unsigned long long *d_cd = h2d(pool, conv_dst, st);
+                gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, nullptr, d_err, st, fck, f_part, n_fck,
+                             d_cd, ovf);
             }
             launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(ovf), st);
-            if (!conv_src.empty()) {
-                unsigned long long *d_cs = h2d(pool, conv_src, st), *d_cd = h2d(pool, conv_dst, st),
-                                   *d_cn = h2d(pool, conv_n, st);
-                const int ng = (int)conv_src.size();
-                k_ovf_convert<<<std::min(ng, 65535), 256, 0, st>>>(gv, d_cs, d_cd, d_cn, ng, ovf);
-                FB2_CHECK_LAUNCH();
-            }
         }
         tr.mark("escapes launched");
         // decode tables: consecutive segments with identical tables share one decode table set
