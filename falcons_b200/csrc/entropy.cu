@@ -1442,6 +1442,12 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     }
 }
 
+// A decode table entry of a context not resident in shared memory (kept out of line so that the
+// global load is only issued when taken).
+__device__ __noinline__ uint32_t far_entry(const uint32_t *__restrict__ tb, uint32_t ctx, uint32_t state) {
+    return __ldg(tb + ctx * O1_M + state);
+}
+
 // Decodes the parts of tANS chains, one part per thread (the chains' checkpoints give every part's
 // starting bit position, state, context and escape offset).  The CTA's parts share one table set,
 // staged in shared memory as for k_o1_decode_smem.  Each part that ends at a checkpoint checks that
@@ -1509,9 +1515,11 @@ __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t 
     uint32_t oi = 0;
     int q0 = nov > 0 ? (int)__ldg(ov) : 0;
     int q1 = nov > 1 ? (int)__ldg(ov + 1) : 0;
-    for (uint32_t j = 0; j < n; j++) {
+    auto step = [&]() -> int {
         const uint32_t sl = (uint32_t)(map >> (4 * ctx)) & 15u;
-        const uint32_t e = sl < (uint32_t)kDecSlots ? sdt[sl * O1_M + state] : __ldg(tb + ctx * O1_M + state);
+        uint32_t e;
+        if (sl < (uint32_t)kDecSlots) e = sdt[sl * O1_M + state];
+        else e = far_entry(tb, ctx, state);  // a real branch: the global load is never speculated
         const bool esc = (e >> 21) & 1u;
         const int code = esc ? q0 : ((int)e >> 22);
         ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
@@ -1520,9 +1528,24 @@ __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t 
             q0 = q1;
             q1 = oi + 1 < nov ? (int)__ldg(ov + oi + 1) : 0;
         }
-        o[j] = (int16_t)code;
         state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
+        return code;
+    };
+    // codes leave in aligned groups of eight (one 16-byte store) between a scalar head and tail
+    const unsigned long long base = ch.lo + start;
+    uint32_t j = 0;
+    for (; j < n && ((base + j) & 7); j++) o[j] = (int16_t)step();
+    for (; j + 8 <= n; j += 8) {
+        uint32_t wv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int a = step();
+            const int b = step();
+            wv[k] = (uint32_t)(uint16_t)a | ((uint32_t)(uint16_t)b << 16);
+        }
+        *reinterpret_cast<uint4 *>(o + j) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
     }
+    for (; j < n; j++) o[j] = (int16_t)step();
     if (oi > nov) atomicExch(err, 7);
     if (!last) {
         const O1Ckpt c = cks[ch.ck + pp.part];
