@@ -163,7 +163,7 @@ def main():
         run_reference(args, rank, world)
         return
     import torch
-    from falcons_b200 import _lib, api
+    from falcons_b200 import _lib, api, replicas
     from falcons_b200 import device as D
     from falcons_b200 import synth
     torch.cuda.set_device(local)
@@ -228,11 +228,8 @@ def main():
     tc = [a.elapsed_time(b) for a, b, c, n in times]
     td = [b.elapsed_time(c) for a, b, c, n in times]
     stream_len = times[-1][3]
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = 2 * nbytes * args.steps * world / (total_ms / 1e3) / 1e9
+    # whole job: bytes of all ranks over the slowest rank's device time
+    value, total_ms, _ = replicas.job_throughput(2 * nbytes * args.steps, total_ms, device=dev)
 
     # ---- live roofline of the prediction + quantization stage (interpolation kernels)
     eb_abs = args.rel * float(x0.max() - x0.min())
@@ -297,12 +294,9 @@ def main():
             m = e2e_step()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / args.e2e_steps
-        e2e = {"value": round(2 * nbytes / dt / 1e9, 3), "unit": UNIT, "h2d_bytes_per_step": int(nbytes + m),
-               "d2h_bytes_per_step": int(m + nbytes), "ms_per_step": round(dt * 1e3, 3)}
-        if dist:
-            t = torch.tensor([e2e["value"]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.SUM)
-            e2e["value"] = round(float(t.item()), 3)
+        e2e_gbs, e2e_ms, _ = replicas.job_throughput(2 * nbytes, dt * 1e3, device=dev)
+        e2e = {"value": round(e2e_gbs, 3), "unit": UNIT, "h2d_bytes_per_step": int(nbytes + m),
+               "d2h_bytes_per_step": int(m + nbytes), "ms_per_step": round(e2e_ms, 3)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
