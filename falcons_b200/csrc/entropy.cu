@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <vector>
 
@@ -88,18 +89,22 @@ __host__ __device__ __forceinline__ uint32_t fse_ckpt_count(uint32_t n, uint32_t
 }
 
 // FSE class block encoder (zfse/fse_compress.c FSE_compress), one CTA per 64 Ki-symbol block.
-// The histogram is parallel; thread 0 normalizes and writes the table header; the CTA builds the
-// coding tables in shared memory (the state table with warp match ranks, the symbol transforms
-// per symbol); thread 0 then runs the two interleaved state chains (symbols
-// n-3 .. 0, each coded by the state of its index parity), recording for every symbol its emitted
-// bits and their count instead of packing them; the CTA then packs in parallel: a block scan of
-// the bit counts gives every symbol its bit position, each thread writes the bits of one run of
-// symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends the two final
-// states and the end mark.  (The chains of these skewed class streams converge too slowly for a
-// speculative split.)  Writes the complete fse_enc record ([1][u32 len][data] | [0][raw] |
-// [2][sym]) to the block's slot; the record flag goes into bits 56-63 of `sizes`.  `recs` is
-// scratch of FBLK words per block.
+// The CTA stages the block in shared memory and counts it; thread 0 normalizes and writes the
+// table header; the CTA builds the coding tables in shared memory (the state table with warp match
+// ranks, the symbol transforms per symbol); two warps then run the two state chains (symbols
+// n-3 .. 0, each coded by the state of its index parity) side by side, recording for every symbol
+// its emitted bits and their count instead of packing them; the CTA then packs in parallel: a
+// block scan of the bit counts gives every symbol its bit position, each thread writes the bits of
+// one run of symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends
+// the two final states and the end mark.  (The chains of these skewed class streams converge too
+// slowly for a speculative split.)  Writes the complete fse_enc record ([1][u32 len][data] |
+// [0][raw] | [2][sym]) to the block's slot; the record flag goes into bits 56-63 of `sizes`.
+// `recs` is scratch of FBLK words per block.
 constexpr unsigned kFseMaxLog = 11;               // the block coder's table log never exceeds 11
+// The block's symbols are staged in dynamic shared memory from the 16-byte word below the block's
+// start: (FBLK + 15) / 16 + 1 words at most.
+constexpr unsigned kFseSrcWords = FBLK / 16 + 1;
+constexpr size_t kFseSrcSmem = (size_t)kFseSrcWords * 16;
 struct FseSmem {
     uint32_t count[256];
     uint32_t cumul[257];
@@ -117,6 +122,7 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                                                           uint8_t *__restrict__ scratch, uint32_t part,
                                                           FseCkpt *__restrict__ cks, uint32_t *__restrict__ recs) {
     __shared__ FseSmem w;
+    extern __shared__ uint4 s_src4[];  // the block's symbols, from byte `lead` on
     __shared__ int s_mode;  // 0 raw, 1 RLE, 2 FSE
     __shared__ unsigned s_tl, s_hdr, s_s0, s_s1, s_maxsv, s_i0, s_i1;
     uint32_t *s_scan = w.scan;
@@ -129,7 +135,38 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
     const unsigned n = jb.n;
     for (int s = threadIdx.x; s < 256; s += blockDim.x) w.count[s] = 0;
     __syncthreads();
-    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&w.count[src[i]], 1u);
+    // Stage the symbols (aligned 16-byte words; the pool's allocations are 16-byte aligned with
+    // slack behind them) and count them: every thread takes a contiguous run of words, visited
+    // from a rotated start so that a quarter warp's stores fall in distinct banks, and adds runs
+    // of equal symbols with one atomic (the class streams are dominated by a few symbols).
+    const unsigned lead = (unsigned)(jb.src & 15u);
+    const uint8_t *s_src = reinterpret_cast<const uint8_t *>(s_src4) + lead;
+    {
+        const uint4 *g4 = reinterpret_cast<const uint4 *>(src - lead);
+        const unsigned nw = (lead + n + 15) / 16, per = (nw + blockDim.x - 1) / blockDim.x;
+        const unsigned w0 = min(nw, threadIdx.x * per), cnt = min(nw, w0 + per) - w0;
+        unsigned cur = 256, run = 0;
+        for (unsigned j = 0; j < cnt; j++) {
+            const unsigned wi = w0 + (j + threadIdx.x) % cnt;
+            const uint4 v = g4[wi];
+            s_src4[wi] = v;
+            const uint32_t q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int h = 0; h < 16; h++) {
+                const unsigned b = wi * 16 + h;
+                if (b < lead || b >= lead + n) continue;
+                const unsigned sy = (q[h >> 2] >> ((h & 3) * 8)) & 0xFFu;
+                if (sy == cur) {
+                    run++;
+                } else {
+                    if (run) atomicAdd(&w.count[cur], run);
+                    cur = sy;
+                    run = 1;
+                }
+            }
+        }
+        if (run) atomicAdd(&w.count[cur], run);
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         int mode = 0;
@@ -194,49 +231,42 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            // the two chains; rec[n - 3 - i] = emitted bits of symbol i | their count << 16
-            uint32_t st[2];
-            for (int k = 0; k < 2; k++) {
-                const unsigned i = ((n - 1) % 2 == (unsigned)k) ? n - 1 : n - 2;
-                const fse::SymTT t = w.sym_tt[src[i]];
+        if ((threadIdx.x & 31u) == 0 && threadIdx.x < 64) {
+            // The two chains run on two warps: chain k codes the symbols i <= n - 3 of parity k,
+            // from the top down, starting from the state that symbol n-1 or n-2 (of parity k)
+            // initialised.  rec is indexed in emission order (e = n - 3 - i): emitted bits
+            // (bits 0-15), their count (16-20) and the decoder's state after the symbol (21-31,
+            // table log <= 11), from which the pack step takes the checkpoint states.  The symbol
+            // transform of the next symbol and the symbol after it are loaded ahead, so that only
+            // the state table lookup stays on the chain.
+            const unsigned k = threadIdx.x >> 5;
+            const uint32_t smask = L - 1;
+            uint32_t sA;
+            {
+                const unsigned i0 = ((n - 1) % 2 == k) ? n - 1 : n - 2;
+                const fse::SymTT t = w.sym_tt[s_src[i0]];
                 const uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
                 const uint32_t v = (nb << 16) - t.deltaNbBits;
-                st[k] = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
+                sA = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
             }
-            const uint32_t smask = L - 1;
-            const int ka = (int)((n - 3) & 1);
-            uint32_t sA = st[ka], sB = st[ka ^ 1];
-            s_i0 = st[0] & smask;  // the states before symbols n-3 and n-4 (for checkpoints next to them)
-            s_i1 = st[1] & smask;
-            // pairs (ii, ii - 1), A codes the first.  rec is indexed in emission order
-            // (e = n - 3 - i): emitted bits (bits 0-15), their count (16-20) and the decoder's state
-            // after the symbol (21-31, table log <= 11), from which the pack step takes the
-            // checkpoint states.  (A plain loop: unrolled, prefetching or branching forms measured
-            // slower.)
-            long long ii = (long long)n - 3;
-            for (; ii >= 1; ii -= 2) {
-                const fse::SymTT ta = w.sym_tt[src[ii]], tb = w.sym_tt[src[ii - 1]];
+            // the decoder's states before symbols n-3 and n-4 (for checkpoints next to them)
+            if (k == 0) s_i0 = sA & smask;
+            else s_i1 = sA & smask;
+            int i = (int)n - 3 - (int)(((n - 3) & 1u) != k);
+            fse::SymTT ta = w.sym_tt[s_src[max(i, 0)]];
+            unsigned ya = s_src[max(i - 2, 0)];
+            uint32_t *rk = rec + (n - 3);
+            for (; i >= 0; i -= 2) {
+                const fse::SymTT na = w.sym_tt[ya];
+                ya = s_src[max(i - 4, 0)];
                 const uint32_t nba = (sA + ta.deltaNbBits) >> 16;
-                const uint32_t nbb = (sB + tb.deltaNbBits) >> 16;
                 const uint32_t xa = w.state_table[(int32_t)(sA >> nba) + ta.deltaFindState];
-                const uint32_t xb = w.state_table[(int32_t)(sB >> nbb) + tb.deltaFindState];
-                rec[(long long)n - 3 - ii] = (sA & ((1u << nba) - 1u)) | (nba << 16) | ((xa & smask) << 21);
-                rec[(long long)n - 2 - ii] = (sB & ((1u << nbb) - 1u)) | (nbb << 16) | ((xb & smask) << 21);
+                rk[-i] = (sA & ((1u << nba) - 1u)) | (nba << 16) | ((xa & smask) << 21);
                 sA = xa;
-                sB = xb;
+                ta = na;
             }
-            if (ii == 0) {  // n - 3 even: symbol 0 belongs to state A
-                const fse::SymTT t = w.sym_tt[src[0]];
-                const uint32_t nb = (sA + t.deltaNbBits) >> 16;
-                const uint32_t xa = w.state_table[(int32_t)(sA >> nb) + t.deltaFindState];
-                rec[n - 3] = (sA & ((1u << nb) - 1u)) | (nb << 16) | ((xa & smask) << 21);
-                sA = xa;
-            }
-            st[ka] = sA;
-            st[ka ^ 1] = sB;
-            s_s0 = st[0];
-            s_s1 = st[1];
+            if (k == 0) s_s0 = sA;
+            else s_s1 = sA;
         }
     }
     __syncthreads();
@@ -565,7 +595,14 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     const size_t ck_per_block = ckpt_part ? FBLK / ckpt_part : 0;
     FseCkpt *cks = ckpt_part ? pool.get<FseCkpt>(jobs.size() * ck_per_block) : nullptr;
     uint32_t *recs = pool.get<uint32_t>(jobs.size() * FBLK);
-    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, 0, st>>>(cls, d_jobs, slots, sizes, bits,
+    static std::once_flag smem_attr[64];
+    int dev = 0;
+    FB2_CUDA(cudaGetDevice(&dev));
+    std::call_once(smem_attr[dev & 63], [] {
+        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kFseSrcSmem));
+    });
+    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, kFseSrcSmem, st>>>(cls, d_jobs, slots, sizes, bits,
                                                               ckpt_part ? ckpt_part : 4096u, cks, recs);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
