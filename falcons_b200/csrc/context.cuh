@@ -59,6 +59,10 @@ struct Context {
     DevBuf field, codes, unpred, work, work2, out, small;
     PinnedBuf host_small;
     cudaEvent_t ev[8] = {};
+    // a second stream for work that overlaps the calling stream, with its fork/join events
+    // (created on first use by side_stream())
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_ev[2] = {};
     ~Context() {
         field.release();
         codes.release();
@@ -70,7 +74,42 @@ struct Context {
         host_small.release();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto &e : side_ev)
+            if (e) cudaEventDestroy(e);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// The context's second stream (non-blocking), created on first use on the current device.
+inline cudaStream_t side_stream(Context &ctx) {
+    if (!ctx.side) FB2_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
+    for (auto &e : ctx.side_ev)
+        if (!e) FB2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return ctx.side;
+}
+
+// Work issued on `side` after construction is ordered after the work already issued on `st`;
+// work issued on `st` after join() (or after destruction) is ordered after all of it.
+struct SideFork {
+    cudaStream_t st, side;
+    cudaEvent_t fork_ev, join_ev;
+    bool joined = false;
+    SideFork(Context &ctx, cudaStream_t s) : st(s), side(side_stream(ctx)), fork_ev(ctx.side_ev[0]),
+                                             join_ev(ctx.side_ev[1]) {
+        FB2_CUDA(cudaEventRecord(fork_ev, st));
+        FB2_CUDA(cudaStreamWaitEvent(side, fork_ev, 0));
+    }
+    void join() {
+        FB2_CUDA(cudaEventRecord(join_ev, side));
+        FB2_CUDA(cudaStreamWaitEvent(st, join_ev, 0));
+        joined = true;
+    }
+    ~SideFork() {
+        if (!joined) {  // error paths: the calling stream must not free what `side` still uses
+            cudaEventRecord(join_ev, side);
+            cudaStreamWaitEvent(st, join_ev, 0);
+        }
     }
 };
 

@@ -588,6 +588,9 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
             job_group.push_back(g);
         }
     }
+    if (std::getenv("FALCONS_TRACE"))
+        std::fprintf(stderr, "[falcons trace] escapes: %lld values in %d groups, %zu class blocks\n", T, G,
+                     jobs.size());
     BlockJob *d_jobs = h2d(pool, jobs, st);
     uint8_t *slots = pool.get<uint8_t>(jobs.size() * kBlockSlot);
     uint8_t *bits = pool.get<uint8_t>(jobs.size() * kBlockSlot);
@@ -1492,7 +1495,8 @@ __device__ __noinline__ uint32_t far_entry(const uint32_t *__restrict__ tb, uint
 constexpr int kPartThreads = 512;
 __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t *__restrict__ in,
                                                                  const DecChain *__restrict__ chains,
-                                                                 const DecPart *__restrict__ parts,
+                                                                 const uint32_t *__restrict__ pstart,
+                                                                 uint32_t nchains,
                                                                  const ChainCta *__restrict__ ctas,
                                                                  const uint32_t *__restrict__ dt,
                                                                  const int16_t *__restrict__ ovf,
@@ -1512,7 +1516,19 @@ __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t 
     }
     __syncthreads();
     if ((int)threadIdx.x >= w.count) return;
-    const DecPart pp = parts[w.first + threadIdx.x];
+    // this thread's part: the last chain (from the CTA's first one on) whose first part is at or
+    // before the item
+    DecPart pp;
+    {
+        const uint32_t item = (uint32_t)(w.first + (int)threadIdx.x);
+        uint32_t lo = (uint32_t)w.pad, hi = nchains;  // pstart[lo] <= item < pstart[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(pstart + mid) <= item) lo = mid;
+            else hi = mid;
+        }
+        pp = DecPart{lo, item - __ldg(pstart + lo)};
+    }
     const DecChain ch = chains[pp.chain];
     const unsigned long long start = (unsigned long long)pp.part * part;
     if (ch.n == 0 || start >= ch.n || ch.inlen == 0 || ch.inlen >= (1ull << 28)) {
@@ -1638,21 +1654,31 @@ std::pair<unsigned long long, unsigned long long> hot_contexts(const uint16_t *n
 // tables take the shared memory), so the CTAs should be at most one per SM: every run of one table
 // gets CTAs in proportion to its size (greedily, always to the run whose CTAs are largest), and
 // a run's items are split evenly among its CTAs.  More items than SMs x max_per take several waves.
-std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std::vector<unsigned long long> &maps,
-                                 const std::vector<unsigned long long> &revs, size_t max_per = kMaxChainsPerCta) {
-    std::vector<ChainCta> out;
+struct ItemRun {
+    size_t first, len;
+    int table;
+};
+
+// Runs of consecutive items with one table.
+std::vector<ItemRun> table_runs(const std::vector<int> &chain_table) {
+    std::vector<ItemRun> runs;
     const size_t n = chain_table.size();
-    const size_t sms = (size_t)sm_count();
-    std::vector<std::pair<size_t, size_t>> runs;  // (first, length)
     for (size_t i = 0; i < n;) {
         size_t j = i;
         while (j < n && chain_table[j] == chain_table[i]) j++;
-        runs.push_back({i, j - i});
+        runs.push_back({i, j - i, chain_table[i]});
         i = j;
     }
+    return runs;
+}
+
+std::vector<ChainCta> run_ctas(const std::vector<ItemRun> &runs, size_t n, const std::vector<unsigned long long> &maps,
+                               const std::vector<unsigned long long> &revs, size_t max_per) {
+    std::vector<ChainCta> out;
+    const size_t sms = (size_t)sm_count();
     std::vector<size_t> ctas(runs.size(), 1);
     if (runs.size() <= sms && n <= sms * max_per) {
-        auto size_of = [&](size_t r) { return (runs[r].second + ctas[r] - 1) / ctas[r]; };
+        auto size_of = [&](size_t r) { return (runs[r].len + ctas[r] - 1) / ctas[r]; };
         for (size_t used = runs.size(); used < sms; used++) {
             size_t best = 0;
             for (size_t r = 1; r < runs.size(); r++)
@@ -1662,16 +1688,21 @@ std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std:
         }
     }
     for (size_t r = 0; r < runs.size(); r++) {
-        size_t c = std::max<size_t>(ctas[r], (runs[r].second + max_per - 1) / max_per);
-        c = std::min(c, runs[r].second);
-        const int t = chain_table[runs[r].first];
+        size_t c = std::max<size_t>(ctas[r], (runs[r].len + max_per - 1) / max_per);
+        c = std::min(c, runs[r].len);
+        const int t = runs[r].table;
         for (size_t k = 0; k < c; k++) {
-            const size_t a = runs[r].first + runs[r].second * k / c;
-            const size_t b = runs[r].first + runs[r].second * (k + 1) / c;
+            const size_t a = runs[r].first + runs[r].len * k / c;
+            const size_t b = runs[r].first + runs[r].len * (k + 1) / c;
             if (b > a) out.push_back(ChainCta{t, (int)a, (int)(b - a), 0, maps[t], revs[t]});
         }
     }
     return out;
+}
+
+std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std::vector<unsigned long long> &maps,
+                                 const std::vector<unsigned long long> &revs, size_t max_per = kMaxChainsPerCta) {
+    return run_ctas(table_runs(chain_table), chain_table.size(), maps, revs, max_per);
 }
 
 void enable_big_smem() {
@@ -2075,8 +2106,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         std::vector<int> h_err = d2h(d_err, 5, st);
         if (h_err[0]) throw std::runtime_error("tANS encoding failed (table construction or chain repair)");
         if (tr.on)
-            std::fprintf(stderr, "[falcons trace] encode chain repair: %d codes re-run, %d rounds, %d far lookups\n",
-                         h_err[2], h_err[3], h_err[4]);
+            std::fprintf(stderr, "[falcons trace] encode chain repair: %d codes re-run, %d rounds, %d far lookups; "
+                         "%lld segments, %d chains each\n", h_err[2], h_err[3], h_err[4], S, K);
         tr.mark("chains done");
         unsigned long long E = 0;
         std::vector<unsigned long long> gstart(S + 1, 0);
@@ -2281,10 +2312,12 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         for (unsigned long long g = 0; g < S; g++)
             if (nf_off[g] + O1_NCTX * O1_NSYM * 2 > len) throw std::invalid_argument("truncated tANS tables");
         tr.mark("segments parsed");
-        // escape values
+        // escape values, decoded on the side stream while this stream builds the decode tables
+        // (raw blocks are copied; gamma groups are unpacked straight into their place)
         int16_t *ovf = pool.get<int16_t>(ovf_total + 1);
+        SideFork fork(ctx, st);
+        Pool spool(fork.side);
         {
-            // raw blocks are copied; gamma groups are unpacked straight into their place
             std::vector<Piece> pcs;
             std::vector<unsigned long long> conv_dst;
             for (auto &r : raws) {
@@ -2292,11 +2325,11 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 else conv_dst.push_back(r.dst);
             }
             if (!conv_dst.empty()) {
-                unsigned long long *d_cd = h2d(pool, conv_dst, st);
-                gamma_decode(pool, d_in, h, cls_off, man_off, man_len, gstart, nullptr, d_err, st, fck, f_part, n_fck,
-                             d_cd, ovf);
+                unsigned long long *d_cd = h2d(spool, conv_dst, fork.side);
+                gamma_decode(spool, d_in, h, cls_off, man_off, man_len, gstart, nullptr, d_err, fork.side, fck, f_part,
+                             n_fck, d_cd, ovf);
             }
-            launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(ovf), st);
+            launch_gather(spool, pcs, reinterpret_cast<uint8_t *>(ovf), fork.side);
         }
         tr.mark("escapes launched");
         // decode tables: consecutive segments with identical tables share one decode table set
@@ -2348,22 +2381,33 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 maps[u] = mr.first;
                 revs[u] = mr.second;
             }
+            tr.mark("hot contexts ranked");
             enable_big_smem();
+            fork.join();  // the chains consume the escape values
             if (parts_ok) {
-                std::vector<DecPart> parts;
-                std::vector<int> part_table;
+                // parts of every chain (their first indices in pstart), CTAs over runs of one table
+                std::vector<uint32_t> pstart(chains.size() + 1, 0);
+                std::vector<int> chain_table(chains.size());
                 for (size_t i = 0; i < chains.size(); i++) {
                     const unsigned long long np = chains[i].n ? 1 + (chains[i].n - 1) / o1_part : 0;
-                    for (unsigned long long q = 0; q < np; q++) {
-                        parts.push_back(DecPart{(uint32_t)i, (uint32_t)q});
-                        part_table.push_back(chains[i].table);
-                    }
+                    pstart[i + 1] = pstart[i] + (uint32_t)np;
+                    chain_table[i] = chains[i].table;
                 }
-                std::vector<ChainCta> ctas = chain_ctas(part_table, maps, revs, kPartThreads);
+                std::vector<ItemRun> runs = table_runs(chain_table);
+                for (auto &r : runs) {
+                    const size_t a = pstart[r.first], b = pstart[r.first + r.len];
+                    r.first = a;
+                    r.len = b - a;
+                }
+                std::vector<ChainCta> ctas = run_ctas(runs, pstart.back(), maps, revs, kPartThreads);
+                for (auto &c : ctas)  // the chain of the CTA's first part
+                    c.pad = (int)(std::upper_bound(pstart.begin(), pstart.end(), (uint32_t)c.first) - pstart.begin()) - 1;
+                tr.mark("parts listed");
                 ChainCta *d_ctas = h2d(pool, ctas, st);
-                DecPart *d_parts = h2d(pool, parts, st);
+                uint32_t *d_pstart = h2d(pool, pstart, st);
                 k_o1_decode_parts<<<(unsigned)ctas.size(), kPartThreads, kDecSlots * O1_M * 4, st>>>(
-                    d_in, dch, d_parts, d_ctas, dt, ovf, ovf_total, o1ck, o1_part, d_codes, d_err);
+                    d_in, dch, d_pstart, (uint32_t)chains.size(), d_ctas, dt, ovf, ovf_total, o1ck, o1_part, d_codes,
+                    d_err);
                 FB2_CHECK_LAUNCH();
             } else {
                 std::vector<int> chain_table(chains.size());
