@@ -12,7 +12,6 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
-#include <mutex>
 #include <stdexcept>
 #include <vector>
 
@@ -88,23 +87,28 @@ __host__ __device__ __forceinline__ uint32_t fse_ckpt_count(uint32_t n, uint32_t
     return n >= 3 ? (n - 3) / part : 0;
 }
 
-// FSE class block encoder (zfse/fse_compress.c FSE_compress), one CTA per 64 Ki-symbol block.
-// The CTA stages the block in shared memory and counts it; thread 0 normalizes and writes the
-// table header; the CTA builds the coding tables in shared memory (the state table with warp match
-// ranks, the symbol transforms per symbol); two warps then run the two state chains (symbols
-// n-3 .. 0, each coded by the state of its index parity) side by side, recording for every symbol
-// its emitted bits and their count instead of packing them; the CTA then packs in parallel: a
-// block scan of the bit counts gives every symbol its bit position, each thread writes the bits of
-// one run of symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends
-// the two final states and the end mark.  (The chains of these skewed class streams converge too
-// slowly for a speculative split.)  Writes the complete fse_enc record ([1][u32 len][data] |
-// [0][raw] | [2][sym]) to the block's slot; the record flag goes into bits 56-63 of `sizes`.
-// `recs` is scratch of FBLK words per block.
+// FSE class block encoder (zfse/fse_compress.c FSE_compress), one CTA per 64 Ki-symbol block,
+// the largest blocks first.  The CTA counts the block; thread 0 normalizes and writes the table
+// header; the CTA builds the coding tables in shared memory (the state table with warp match
+// ranks, the symbol transforms per symbol, and, where it fits, the next-state table); two warps
+// then code the two state chains (symbols n-3 .. 0, each coded by the state of its index parity)
+// side by side, recording for every symbol its emitted bits and their count instead of packing
+// them; the CTA then packs in parallel: a block scan of the bit counts gives every symbol its bit
+// position, each thread writes the bits of one run of symbols (words shared with a neighbour
+// merged with atomicOr), and thread 0 appends the two final states and the end mark.  (The
+// chains of these skewed class streams converge too slowly for a speculative split.)  Writes the
+// complete fse_enc record ([1][u32 len][data] | [0][raw] | [2][sym]) to the block's slot; the
+// record flag goes into bits 56-63 of `sizes`.  `recs` is scratch of kFseRecWords words per block.
 constexpr unsigned kFseMaxLog = 11;               // the block coder's table log never exceeds 11
-// The block's symbols are staged in dynamic shared memory from the 16-byte word below the block's
-// start: (FBLK + 15) / 16 + 1 words at most.
-constexpr unsigned kFseSrcWords = FBLK / 16 + 1;
-constexpr size_t kFseSrcSmem = (size_t)kFseSrcWords * 16;
+// Next-state table of the chains (dynamic shared memory): for every symbol s from the smallest
+// to the largest present one and every state x, the coded state minus L (bits 0-10) and the
+// number of emitted bits (bits 11-14), so that a chain step is one table load.  Blocks whose
+// table would not fit (symbol span x L x 2 bytes) take the state-table path.
+constexpr size_t kFseNxtBytes = 40 * 1024;
+// Per-chain record scratch (words): a chain's records are indexed by step plus the chain's lead
+// (the steps that its first 16-byte symbol word holds above the chain's start).
+constexpr unsigned kFseChainRec = FBLK / 2 + 32;
+constexpr unsigned kFseRecWords = 2 * kFseChainRec;
 struct FseSmem {
     uint32_t count[256];
     uint32_t cumul[257];
@@ -120,42 +124,42 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                                                           uint8_t *__restrict__ slots,
                                                           unsigned long long *__restrict__ sizes,
                                                           uint8_t *__restrict__ scratch, uint32_t part,
-                                                          FseCkpt *__restrict__ cks, uint32_t *__restrict__ recs) {
+                                                          FseCkpt *__restrict__ cks, uint32_t *__restrict__ recs,
+                                                          const uint32_t *__restrict__ order) {
     __shared__ FseSmem w;
-    extern __shared__ uint4 s_src4[];  // the block's symbols, from byte `lead` on
+    extern __shared__ uint4 s_nxt4[];  // next-state table (kFseNxtBytes)
     __shared__ int s_mode;  // 0 raw, 1 RLE, 2 FSE
-    __shared__ unsigned s_tl, s_hdr, s_s0, s_s1, s_maxsv, s_i0, s_i1;
-    uint32_t *s_scan = w.scan;
-    const BlockJob jb = jobs[blockIdx.x];
+    __shared__ unsigned s_tl, s_hdr, s_s0, s_s1, s_maxsv, s_i0, s_i1, s_minsv, s_fast;
+    __shared__ unsigned s_lead[2], s_high;
+    __shared__ uint32_t s_sh[32];
+    const unsigned b = order[blockIdx.x];  // the largest blocks first
+    const BlockJob jb = jobs[b];
     const uint8_t *src = cls + jb.src;
-    uint8_t *out = slots + (size_t)blockIdx.x * kBlockSlot;
-    uint32_t *bw = reinterpret_cast<uint32_t *>(scratch + (size_t)blockIdx.x * kBlockSlot);
-    uint32_t *rec = recs + (size_t)blockIdx.x * FBLK;
-    FseCkpt *ck = cks ? cks + (size_t)blockIdx.x * (FBLK / part) : nullptr;
+    uint8_t *out = slots + (size_t)b * kBlockSlot;
+    uint32_t *bw = reinterpret_cast<uint32_t *>(scratch + (size_t)b * kBlockSlot);
+    uint32_t *rec = recs + (size_t)b * kFseRecWords;
+    FseCkpt *ck = cks ? cks + (size_t)b * (FBLK / part) : nullptr;
     const unsigned n = jb.n;
     for (int s = threadIdx.x; s < 256; s += blockDim.x) w.count[s] = 0;
     __syncthreads();
-    // Stage the symbols (aligned 16-byte words; the pool's allocations are 16-byte aligned with
-    // slack behind them) and count them: every thread takes a contiguous run of words, visited
-    // from a rotated start so that a quarter warp's stores fall in distinct banks, and adds runs
-    // of equal symbols with one atomic (the class streams are dominated by a few symbols).
-    const unsigned lead = (unsigned)(jb.src & 15u);
-    const uint8_t *s_src = reinterpret_cast<const uint8_t *>(s_src4) + lead;
+    // Count the symbols: every thread reads a contiguous run of aligned 16-byte words (the pool's
+    // allocations are 16-byte aligned with slack behind them) and adds runs of equal symbols with
+    // one atomic (the class streams are dominated by a few symbols).
     {
+        const unsigned lead = (unsigned)(jb.src & 15u);
         const uint4 *g4 = reinterpret_cast<const uint4 *>(src - lead);
         const unsigned nw = (lead + n + 15) / 16, per = (nw + blockDim.x - 1) / blockDim.x;
         const unsigned w0 = min(nw, threadIdx.x * per), cnt = min(nw, w0 + per) - w0;
         unsigned cur = 256, run = 0;
         for (unsigned j = 0; j < cnt; j++) {
-            const unsigned wi = w0 + (j + threadIdx.x) % cnt;
+            const unsigned wi = w0 + j;
             const uint4 v = g4[wi];
-            s_src4[wi] = v;
-            const uint32_t q[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (int h = 0; h < 16; h++) {
-                const unsigned b = wi * 16 + h;
-                if (b < lead || b >= lead + n) continue;
-                const unsigned sy = (q[h >> 2] >> ((h & 3) * 8)) & 0xFFu;
+                const unsigned bi = wi * 16 + h;
+                if (bi < lead || bi >= lead + n) continue;
+                const uint32_t qw = h < 4 ? v.x : h < 8 ? v.y : h < 12 ? v.z : v.w;
+                const unsigned sy = (qw >> ((h & 3) * 8)) & 0xFFu;
                 if (sy == cur) {
                     run++;
                 } else {
@@ -182,7 +186,20 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                 if (tl <= kFseMaxLog && fse::normalize_count(w.norm, tl, w.count, n, maxSV) == tl &&
                     kBlockSlot - 5 >= fse::ncount_bound(maxSV, tl) + 16) {
                     hdr = (unsigned)fse::write_ncount(out + 5, w.norm, maxSV, tl);
-                    if (hdr && fse::spread(w.sym, w.norm, maxSV, tl)) {
+                    // the spread (zfse FSE_buildCTable): the low-probability (-1) symbols take the
+                    // top cells; the cells of the others, in symbol order, go to the kept positions
+                    // (j * step) & mask <= high in order of j (spread in parallel below; the
+                    // sequential walk ends at position 0 exactly when the cells fill the kept
+                    // positions)
+                    uint32_t c = 0, high = (1u << tl) - 1;
+                    for (unsigned s2 = 0; s2 <= maxSV; s2++) {
+                        w.scan[s2] = c;
+                        if (w.norm[s2] > 0) c += (uint32_t)w.norm[s2];
+                        else if (w.norm[s2] == -1) w.sym[high--] = (uint8_t)s2;
+                    }
+                    w.scan[maxSV + 1] = c;
+                    s_high = high;
+                    if (hdr && c == high + 1) {
                         mode = 2;
                         w.cumul[0] = 0;
                         for (unsigned u = 1; u <= maxSV + 1; u++)
@@ -199,6 +216,31 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
     __syncthreads();
     if (s_mode == 2) {
         const unsigned tl = s_tl, L = 1u << tl, maxSV = s_maxsv;
+        {
+            // parallel spread: thread t ranks the kept positions of j in [t * per, (t + 1) * per)
+            const uint32_t step = fse::table_step(L), mask = L - 1, high = s_high;
+            const unsigned per = (L + blockDim.x - 1) / blockDim.x;
+            const unsigned j0 = min(L, threadIdx.x * per), j1 = min(L, j0 + per);
+            uint32_t cnt = 0;
+            for (unsigned j = j0; j < j1; j++) cnt += ((j * step) & mask) <= high;
+            uint32_t tot;
+            uint32_t kc = block_excl_scan<uint32_t>(cnt, s_sh, tot);
+            unsigned sy = 0;  // the symbol of cell kc: the last one whose first cell is <= kc
+            for (unsigned lo = 0, hi = maxSV + 1; hi - lo > 1;) {
+                const unsigned mid = (lo + hi) >> 1;
+                if (w.scan[mid] <= kc) lo = mid;
+                else hi = mid;
+                sy = lo;
+            }
+            for (unsigned j = j0; j < j1; j++) {
+                const uint32_t pos = (j * step) & mask;
+                if (pos > high) continue;
+                while (w.scan[sy + 1] <= kc) sy++;
+                w.sym[pos] = (uint8_t)sy;
+                kc++;
+            }
+            __syncthreads();
+        }
         // state table: the cells of every symbol in increasing order (match ranks within a warp)
         if (threadIdx.x < 32) {
             const unsigned lane = threadIdx.x;
@@ -231,42 +273,146 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned lo = 0;
+            while (lo < maxSV && w.count[lo] == 0) lo++;
+            s_minsv = lo;
+            s_fast = (size_t)(maxSV - lo + 1) * L * 2 <= kFseNxtBytes;
+        }
+        __syncthreads();
+        uint16_t *nxt = reinterpret_cast<uint16_t *>(s_nxt4);
+        const unsigned minSV = s_minsv;
+        const bool fast = s_fast != 0;
+        if (fast) {
+            for (unsigned e = threadIdx.x; e < (maxSV - minSV + 1) * L; e += blockDim.x) {
+                const unsigned sy = minSV + (e >> tl), x = L + (e & (L - 1));
+                if (!w.count[sy]) continue;
+                const fse::SymTT t = w.sym_tt[sy];
+                const uint32_t nb = (x + t.deltaNbBits) >> 16;
+                nxt[e] = (uint16_t)((w.state_table[(int32_t)(x >> nb) + t.deltaFindState] - L) | (nb << 11));
+            }
+            __syncthreads();
+        }
         if ((threadIdx.x & 31u) == 0 && threadIdx.x < 64) {
-            // The two chains run on two warps: chain k codes the symbols i <= n - 3 of parity k,
-            // from the top down, starting from the state that symbol n-1 or n-2 (of parity k)
-            // initialised.  rec is indexed in emission order (e = n - 3 - i): emitted bits
-            // (bits 0-15), their count (16-20) and the decoder's state after the symbol (21-31,
-            // table log <= 11), from which the pack step takes the checkpoint states.  The symbol
-            // transform of the next symbol and the symbol after it are loaded ahead, so that only
-            // the state table lookup stays on the chain.
+            // The two state chains, one per warp: chain k codes the symbols i <= n - 3 of parity k
+            // from the top down (step j codes symbol top - 2 j), starting from the state that
+            // symbol n-1 or n-2 (of parity k) initialised.  Each step records the state before
+            // it minus L (bits 0-10, table log <= 11; its low bits are the emitted ones), the state
+            // after it minus L (bits 11-21, the decoder's state there, from which the pack step
+            // takes the checkpoint states) and the number of emitted bits (22-25).
             const unsigned k = threadIdx.x >> 5;
             const uint32_t smask = L - 1;
-            uint32_t sA;
+            uint32_t v;  // the state minus L
             {
                 const unsigned i0 = ((n - 1) % 2 == k) ? n - 1 : n - 2;
-                const fse::SymTT t = w.sym_tt[s_src[i0]];
+                const fse::SymTT t = w.sym_tt[src[i0]];
                 const uint32_t nb = (t.deltaNbBits + (1u << 15)) >> 16;
-                const uint32_t v = (nb << 16) - t.deltaNbBits;
-                sA = w.state_table[(int32_t)(v >> nb) + t.deltaFindState];
+                const uint32_t u = (nb << 16) - t.deltaNbBits;
+                v = w.state_table[(int32_t)(u >> nb) + t.deltaFindState] - L;
             }
             // the decoder's states before symbols n-3 and n-4 (for checkpoints next to them)
-            if (k == 0) s_i0 = sA & smask;
-            else s_i1 = sA & smask;
-            int i = (int)n - 3 - (int)(((n - 3) & 1u) != k);
-            fse::SymTT ta = w.sym_tt[s_src[max(i, 0)]];
-            unsigned ya = s_src[max(i - 2, 0)];
-            uint32_t *rk = rec + (n - 3);
-            for (; i >= 0; i -= 2) {
-                const fse::SymTT na = w.sym_tt[ya];
-                ya = s_src[max(i - 4, 0)];
-                const uint32_t nba = (sA + ta.deltaNbBits) >> 16;
-                const uint32_t xa = w.state_table[(int32_t)(sA >> nba) + ta.deltaFindState];
-                rk[-i] = (sA & ((1u << nba) - 1u)) | (nba << 16) | ((xa & smask) << 21);
-                sA = xa;
-                ta = na;
+            if (k == 0) s_i0 = v;
+            else s_i1 = v;
+            const int top = (int)n - 3 - (int)(((n - 3) & 1u) != k);
+            const unsigned m = top >= 0 ? (unsigned)top / 2 + 1 : 0;  // steps
+            uint32_t *rk = rec + k * kFseChainRec;
+            unsigned lead = 0;
+            if (fast && m > 0) {
+                // The chain's symbols are every other byte of the aligned 16-byte words from the one
+                // holding symbol `top` down: eight steps per word (whole words loaded three words
+                // ahead), the first word holding `lead` steps above the chain's start.  A step is
+                // one load from the next-state table; the records of whole words leave as two
+                // 16-byte stores.
+                const uintptr_t a0 = reinterpret_cast<uintptr_t>(src + top);
+                const unsigned par = (unsigned)(a0 & 1u), sh = 8u * par;
+                lead = (14u + par - (unsigned)(a0 & 15u)) >> 1;
+                const unsigned nv = lead + m;
+                const uint4 *wp = reinterpret_cast<const uint4 *>(a0 & ~(uintptr_t)15);  // word g at wp - g
+                const uint16_t *tb = nxt;  // shared memory: row of symbol s at (s - minSV) << tl
+                // the chain's bytes of a word at even offsets 14, 12, .., 0 (descending steps), as the
+                // row offsets of their symbols in the next-state table
+                auto offsets = [&](const uint4 &q, uint32_t *o) {
+                    const uint32_t h0 = __funnelshift_r(q.x, q.y, sh), h1 = __funnelshift_r(q.y, q.z, sh);
+                    const uint32_t h2 = __funnelshift_r(q.z, q.w, sh), h3 = q.w >> sh;
+                    o[0] = (((h3 >> 16) & 0xFFu) - minSV) << tl;
+                    o[1] = ((h3 & 0xFFu) - minSV) << tl;
+                    o[2] = (((h2 >> 16) & 0xFFu) - minSV) << tl;
+                    o[3] = ((h2 & 0xFFu) - minSV) << tl;
+                    o[4] = (((h1 >> 16) & 0xFFu) - minSV) << tl;
+                    o[5] = ((h1 & 0xFFu) - minSV) << tl;
+                    o[6] = (((h0 >> 16) & 0xFFu) - minSV) << tl;
+                    o[7] = ((h0 & 0xFFu) - minSV) << tl;
+                };
+                // the record of a step from the state before it and its table entry
+                auto record = [](uint32_t v0, uint32_t e) -> uint32_t { return v0 | (e << 11); };
+                // steps [t0, t1) of word g one at a time (the partial first and last words)
+                auto partial = [&](unsigned g, unsigned t0, unsigned t1) {
+                    uint32_t o[8];
+                    offsets(wp[-(int)g], o);
+#pragma unroll
+                    for (unsigned t = 0; t < 8; t++) {
+                        if (t < t0 || t >= t1) continue;
+                        const uint32_t e = tb[o[t] + v];
+                        rk[8 * g + t] = record(v, e);
+                        v = e & 0x7FFu;
+                    }
+                };
+                const unsigned gs = lead ? 1u : 0u, ge = nv >> 3;  // the whole words [gs, ge)
+                if (lead) partial(0, lead, min(8u, nv));
+                if (gs < ge) {
+                    // Whole words, software-pipelined: the lookup of the next step is issued before
+                    // the record of the current one is formed, so that only the lookups and the
+                    // masking of their states stay on the chain.
+                    uint4 q1 = gs + 1 < ge ? wp[-(int)(gs + 1)] : make_uint4(0, 0, 0, 0);
+                    uint4 q2 = gs + 2 < ge ? wp[-(int)(gs + 2)] : make_uint4(0, 0, 0, 0);
+                    uint32_t o[8];
+                    offsets(wp[-(int)gs], o);
+                    uint32_t e = tb[o[0] + v];
+                    for (unsigned g = gs; g < ge; g++) {
+                        const uint4 qn = q1;
+                        q1 = q2;
+                        if (g + 3 < ge) q2 = wp[-(int)(g + 3)];
+                        uint32_t on[8];
+                        offsets(qn, on);
+                        uint32_t r[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) {
+                            const uint32_t vn = e & 0x7FFu;
+                            uint32_t en = 0;
+                            if (t < 7) en = tb[o[t + 1] + vn];
+                            else if (g + 1 < ge) en = tb[on[0] + vn];
+                            r[t] = record(v, e);
+                            v = vn;
+                            e = en;
+                        }
+                        reinterpret_cast<uint4 *>(rk + 8 * g)[0] = make_uint4(r[0], r[1], r[2], r[3]);
+                        reinterpret_cast<uint4 *>(rk + 8 * g)[1] = make_uint4(r[4], r[5], r[6], r[7]);
+#pragma unroll
+                        for (int t = 0; t < 8; t++) o[t] = on[t];
+                    }
+                }
+                if (ge >= gs && 8 * ge < nv && (ge > 0 || !lead)) partial(ge, 0, nv - 8 * ge);
+            } else if (m > 0) {
+                // the state-table path: the symbol transform of the next symbol and the symbol
+                // after it are loaded ahead, so that only the state table lookup stays on the chain
+                uint32_t sA = v + L;
+                int i = top;
+                fse::SymTT ta = w.sym_tt[src[i]];
+                unsigned ya = src[max(i - 2, 0)];
+                for (unsigned j = 0; j < m; j++, i -= 2) {
+                    const fse::SymTT na = w.sym_tt[ya];
+                    ya = __ldg(src + max(i - 4, 0));
+                    const uint32_t nba = (sA + ta.deltaNbBits) >> 16;
+                    const uint32_t xa = w.state_table[(int32_t)(sA >> nba) + ta.deltaFindState];
+                    rk[j] = (sA - L) | ((xa & smask) << 11) | (nba << 22);
+                    sA = xa;
+                    ta = na;
+                }
+                v = sA - L;
             }
-            if (k == 0) s_s0 = sA;
-            else s_s1 = sA;
+            s_lead[k] = lead;
+            if (k == 0) s_s0 = v + L;
+            else s_s1 = v + L;
         }
     }
     __syncthreads();
@@ -277,16 +423,14 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
         // symbols n-3 .. 0 in emission order; thread t owns emission positions [t*per, (t+1)*per)
         const unsigned ns = n - 2, per = (ns + blockDim.x - 1) / blockDim.x;
         const unsigned e0 = min(ns, threadIdx.x * per), e1 = min(ns, e0 + per);
+        // the record of emission position e: even positions belong to the chain of n-3's parity
+        const unsigned ka = (n - 3) & 1u;
+        const unsigned offA = ka * kFseChainRec + s_lead[ka], offB = (ka ^ 1u) * kFseChainRec + s_lead[ka ^ 1u];
+        auto R = [&](unsigned e) -> uint32_t { return rec[((e & 1u) ? offB : offA) + (e >> 1)]; };
         uint32_t cnt = 0;
-        for (unsigned e = e0; e < e1; e++) cnt += (rec[e] >> 16) & 31u;
-        s_scan[threadIdx.x] = cnt;
-        __syncthreads();
-        uint32_t off = 0;
-        for (unsigned j = 0; j < threadIdx.x; j++) off += s_scan[j];
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) s_scan[0] = off + cnt;  // bits of all symbols
-        __syncthreads();
-        const uint32_t sym_bits = s_scan[0];
+        for (unsigned e = e0; e < e1; e++) cnt += R(e) >> 22;
+        uint32_t sym_bits;  // bits of all symbols
+        const uint32_t off = block_excl_scan<uint32_t>(cnt, s_sh, sym_bits);
         const uint32_t total = sym_bits + 2 * tl + 1;
         body = (total + 7) / 8;
         if (body + 8 > kBlockSlot - 5 - s_hdr || s_hdr + body >= n - 1) mode = 0;  // not worth coding: raw
@@ -308,14 +452,14 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             uint32_t pos = off;
             for (unsigned e = e0; e < e1; e++) {
                 const unsigned i = n - 3 - e;
-                const uint32_t r = rec[e], nb = (r >> 16) & 31u;
-                acc |= (uint64_t)(r & 0xFFFFu) << accn;
+                const uint32_t r = R(e), nb = r >> 22;
+                acc |= (uint64_t)(r & ((1u << nb) - 1u)) << accn;
                 accn += nb;
                 pos += nb;
                 if (ck && i > 0 && (i & (part - 1)) == 0) {
                     // decoder states before symbol i: after symbol i (even chain), after i + 1 (odd)
-                    const uint32_t odd = i + 1 <= n - 3 ? rec[e - 1] >> 21 : ((n - 2) & 1 ? s_i1 : s_i0);
-                    ck[i / part - 1] = FseCkpt{pos, (uint16_t)(r >> 21), (uint16_t)odd};
+                    const uint32_t odd = i + 1 <= n - 3 ? (R(e - 1) >> 11) & 0x7FFu : ((n - 2) & 1 ? s_i1 : s_i0);
+                    ck[i / part - 1] = FseCkpt{pos, (uint16_t)((r >> 11) & 0x7FFu), (uint16_t)odd};
                 }
                 if (accn >= 32) {
                     flush_word((uint32_t)acc);
@@ -344,12 +488,12 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
     if (mode == 0) {  // raw
         if (threadIdx.x == 0) out[0] = 0;
         for (unsigned i = threadIdx.x; i < n; i += blockDim.x) out[1 + i] = src[i];
-        if (threadIdx.x == 0) sizes[blockIdx.x] = 1 + n;  // flag 0
+        if (threadIdx.x == 0) sizes[b] = 1 + n;  // flag 0
     } else if (mode == 1) {  // a single repeated symbol
         if (threadIdx.x == 0) {
             out[0] = 2;
             out[1] = src[0];
-            sizes[blockIdx.x] = 2 | (2ULL << 56);
+            sizes[b] = 2 | (2ULL << 56);
         }
     } else {
         const size_t r = s_hdr + body;
@@ -363,7 +507,7 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             out[2] = (uint8_t)(rr >> 8);
             out[3] = (uint8_t)(rr >> 16);
             out[4] = (uint8_t)(rr >> 24);
-            sizes[blockIdx.x] = (5 + r) | (1ULL << 56);
+            sizes[b] = (5 + r) | (1ULL << 56);
         }
     }
 }
@@ -597,16 +741,15 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     unsigned long long *sizes = pool.get<unsigned long long>(jobs.size());
     const size_t ck_per_block = ckpt_part ? FBLK / ckpt_part : 0;
     FseCkpt *cks = ckpt_part ? pool.get<FseCkpt>(jobs.size() * ck_per_block) : nullptr;
-    uint32_t *recs = pool.get<uint32_t>(jobs.size() * FBLK);
-    static std::once_flag smem_attr[64];
-    int dev = 0;
-    FB2_CUDA(cudaGetDevice(&dev));
-    std::call_once(smem_attr[dev & 63], [] {
-        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kFseSrcSmem));
-    });
-    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, kFseSrcSmem, st>>>(cls, d_jobs, slots, sizes, bits,
-                                                              ckpt_part ? ckpt_part : 4096u, cks, recs);
+    uint32_t *recs = pool.get<uint32_t>(jobs.size() * kFseRecWords);
+    std::vector<uint32_t> order(jobs.size());
+    for (size_t j = 0; j < jobs.size(); j++) order[j] = (uint32_t)j;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return jobs[a].n > jobs[b].n; });
+    uint32_t *d_order = h2d(pool, order, st);
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFseNxtBytes));
+    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, kFseNxtBytes, st>>>(cls, d_jobs, slots, sizes, bits,
+                                                                         ckpt_part ? ckpt_part : 4096u, cks, recs,
+                                                                         d_order);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
     for (size_t j = 0; j < jobs.size(); j++) {
