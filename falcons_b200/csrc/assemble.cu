@@ -26,48 +26,59 @@ __global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__re
         const Piece pc = pieces[p];
         const uint8_t *s = pc.src;
         uint8_t *d = out + pc.dst;
-        if ((((uintptr_t)s ^ (uintptr_t)d) & 15) == 0) {
-            unsigned long long head = (16 - ((uintptr_t)s & 15)) & 15;
-            if (head > pc.len) head = pc.len;
-            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
-            const unsigned long long nv = (pc.len - head) / 16;
-            const int4 *sv = reinterpret_cast<const int4 *>(s + head);
-            int4 *dv = reinterpret_cast<int4 *>(d + head);
+        // bytes up to the first 16-byte destination boundary, whole 16-byte destination words, and
+        // the remaining bytes
+        unsigned long long head = (16 - ((uintptr_t)d & 15)) & 15;
+        if (head > pc.len) head = pc.len;
+        for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
+        const uint8_t *s2 = s + head;
+        uint4 *dv = reinterpret_cast<uint4 *>(d + head);
+        const unsigned long long nv = (pc.len - head) / 16;
+        const unsigned o = (unsigned)((uintptr_t)s2 & 15);
+        if (o == 0) {
+            const uint4 *sv = reinterpret_cast<const uint4 *>(s2);
             for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
-            for (unsigned long long i = head + nv * 16 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
-        } else if ((((uintptr_t)s ^ (uintptr_t)d) & 3) == 0) {
-            unsigned long long head = (4 - ((uintptr_t)s & 3)) & 3;
-            if (head > pc.len) head = pc.len;
-            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
-            const unsigned long long nv = (pc.len - head) / 4;
-            const uint32_t *sv = reinterpret_cast<const uint32_t *>(s + head);
-            uint32_t *dv = reinterpret_cast<uint32_t *>(d + head);
-            for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
-            for (unsigned long long i = head + nv * 4 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
         } else {
-            // misaligned: aligned 4-byte destination words assembled from a funnel of source words
-            unsigned long long head = (4 - ((uintptr_t)d & 3)) & 3;
-            if (head > pc.len) head = pc.len;
-            for (unsigned long long i = threadIdx.x; i < head; i += blockDim.x) d[i] = s[i];
-            const uint8_t *s2 = s + head;
-            uint32_t *dw = reinterpret_cast<uint32_t *>(d + head);
-            const unsigned long long nw = (pc.len - head) / 4;
-            const int sh = (int)((uintptr_t)s2 & 3);
-            const uint32_t *sw = reinterpret_cast<const uint32_t *>(s2 - sh);
-            for (unsigned long long i = threadIdx.x; i < nw; i += blockDim.x) {
-                const uint32_t lo = sw[i], hi = sw[i + 1];
-                dw[i] = __funnelshift_r(lo, hi, 8 * sh);
+            // a destination word from the two aligned source words that hold its 16 bytes (both
+            // hold bytes of the piece, so they are readable)
+            const uint4 *sa = reinterpret_cast<const uint4 *>(s2 - o);
+            const unsigned q = o >> 2, r = 8 * (o & 3);
+            for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) {
+                const uint4 A = sa[i], B = sa[i + 1];
+                uint32_t w0, w1, w2, w3, w4;
+                if (q == 0) { w0 = A.x; w1 = A.y; w2 = A.z; w3 = A.w; w4 = B.x; }
+                else if (q == 1) { w0 = A.y; w1 = A.z; w2 = A.w; w3 = B.x; w4 = B.y; }
+                else if (q == 2) { w0 = A.z; w1 = A.w; w2 = B.x; w3 = B.y; w4 = B.z; }
+                else { w0 = A.w; w1 = B.x; w2 = B.y; w3 = B.z; w4 = B.w; }
+                dv[i] = make_uint4(__funnelshift_r(w0, w1, r), __funnelshift_r(w1, w2, r), __funnelshift_r(w2, w3, r),
+                                   __funnelshift_r(w3, w4, r));
             }
-            for (unsigned long long i = head + nw * 4 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
         }
+        for (unsigned long long i = head + nv * 16 + threadIdx.x; i < pc.len; i += blockDim.x) d[i] = s[i];
     }
 }
 }  // namespace
 
 void launch_gather(Pool &pool, const std::vector<Piece> &pieces, uint8_t *d_out, cudaStream_t st) {
     if (pieces.empty()) return;
-    Piece *dp = h2d(pool, pieces, st);
-    k_gather<<<(unsigned)std::min<size_t>(pieces.size(), 65535), 256, 0, st>>>(dp, (int)pieces.size(), d_out);
+    // pieces longer than kGatherChunk are split (at multiples of 16 bytes, which keeps the
+    // alignment of source and destination) so that large copies spread over many CTAs
+    constexpr unsigned long long kGatherChunk = 32 * 1024;
+    std::vector<Piece> split;
+    const std::vector<Piece> *use = &pieces;
+    bool big = false;
+    for (const Piece &pc : pieces) big |= pc.len > kGatherChunk;
+    if (big) {
+        split.reserve(pieces.size() + 64);
+        for (const Piece &pc : pieces)
+            for (unsigned long long o = 0; o < pc.len || (o == 0 && pc.len == 0); o += kGatherChunk) {
+                split.push_back(Piece{pc.src + o, pc.dst + o, std::min(kGatherChunk, pc.len - o)});
+                if (pc.len == 0) break;
+            }
+        use = &split;
+    }
+    Piece *dp = h2d(pool, *use, st);
+    k_gather<<<(unsigned)std::min<size_t>(use->size(), 65535), 256, 0, st>>>(dp, (int)use->size(), d_out);
     FB2_CHECK_LAUNCH();
 }
 
