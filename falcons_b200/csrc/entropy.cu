@@ -524,7 +524,9 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
                                                          uint32_t part, const FseCkpt *__restrict__ cks) {
     __shared__ fse::DEntry dt[1 << fse::kMaxTableLog];
     __shared__ uint8_t sym[1 << fse::kMaxTableLog];
-    __shared__ unsigned tl_sh, hdr_sh;
+    __shared__ int16_t s_norm[256];
+    __shared__ uint32_t s_scan[257], s_next[256];
+    __shared__ unsigned tl_sh, hdr_sh, maxsv_sh, high_sh;
     const BlockJob jb = jobs[blockIdx.x];
     uint8_t *dst = cls + jb.src;
     const uint8_t *p = in + jb.in;
@@ -538,19 +540,80 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
         return;
     }
     const size_t size = (size_t)jb.inlen;
+    // The decode table (zfse FSE_buildDTable), built by the warp: lane 0 reads the header and lays
+    // the low-probability (-1) symbols on the top cells; the lanes spread the other cells (cell k
+    // in symbol order goes to the k-th position (j * step) & mask <= high in order of j) and then
+    // number every symbol's cells in cell order (warp match ranks, 32 cells at a time).
     if (threadIdx.x == 0) {
-        int16_t norm[256];
         unsigned maxSV = 255, tl = 0;
-        const size_t hdr = fse::read_ncount(norm, &maxSV, &tl, p, size);
-        const bool ok = hdr != 0 && hdr < size && tl <= (unsigned)fse::kMaxTableLog &&
-                        fse::build_dtable(dt, norm, maxSV, tl, sym);
+        const size_t hdr = fse::read_ncount(s_norm, &maxSV, &tl, p, size);
+        bool ok = hdr != 0 && hdr < size && tl <= (unsigned)fse::kMaxTableLog;
+        if (ok) {
+            uint32_t c = 0, high = (1u << tl) - 1;
+            for (unsigned s2 = 0; s2 <= maxSV; s2++) {
+                s_scan[s2] = c;
+                const int nn = s_norm[s2];
+                if (nn > 0) c += (uint32_t)nn;
+                else if (nn == -1) sym[high--] = (uint8_t)s2;
+                s_next[s2] = nn == -1 ? 1u : (uint32_t)max(nn, 0);
+            }
+            s_scan[maxSV + 1] = c;
+            ok = c == high + 1;  // the sequential spread ends at position 0 exactly then
+            high_sh = high;
+        }
         tl_sh = ok ? tl : 0xFFFFFFFFu;
         hdr_sh = (unsigned)hdr;
+        maxsv_sh = maxSV;
         if (!ok) atomicExch(err, 1);
     }
     __syncwarp();
     const unsigned tl = tl_sh;
     if (tl == 0xFFFFFFFFu) return;
+    {
+        const unsigned lane = threadIdx.x, L = 1u << tl, maxSV = maxsv_sh;
+        const uint32_t step = fse::table_step(L), mask = L - 1, high = high_sh;
+        const unsigned per = (L + 31) / 32, j0 = min(L, lane * per), j1 = min(L, j0 + per);
+        uint32_t cnt = 0;
+        for (unsigned j = j0; j < j1; j++) cnt += ((j * step) & mask) <= high;
+        uint32_t kc = cnt;  // exclusive warp scan
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, kc, o);
+            if (lane >= (unsigned)o) kc += t;
+        }
+        kc -= cnt;
+        unsigned sy = 0;  // the symbol of cell kc: the last one whose first cell is <= kc
+        for (unsigned lo = 0, hi = maxSV + 1; hi - lo > 1;) {
+            const unsigned mid = (lo + hi) >> 1;
+            if (s_scan[mid] <= kc) lo = mid;
+            else hi = mid;
+            sy = lo;
+        }
+        for (unsigned j = j0; j < j1; j++) {
+            const uint32_t pos = (j * step) & mask;
+            if (pos > high) continue;
+            while (s_scan[sy + 1] <= kc) sy++;
+            sym[pos] = (uint8_t)sy;
+            kc++;
+        }
+        __syncwarp();
+        for (unsigned u0 = 0; u0 < L; u0 += 32) {
+            const unsigned u = u0 + lane;
+            const unsigned sv = u < L ? sym[u] : 256u + lane;
+            const unsigned peers = __match_any_sync(0xffffffffu, sv);
+            const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+            if (u < L) {
+                const uint32_t ns = s_next[sv] + rank;
+                const uint32_t nb = tl - fse::highbit32(ns);
+                dt[u].symbol = (uint8_t)sv;
+                dt[u].nbBits = (uint8_t)nb;
+                dt[u].newState = (uint16_t)((ns << nb) - L);
+            }
+            __syncwarp();
+            if (u < L && rank == (unsigned)__popc(peers) - 1u) s_next[sv] += rank + 1;
+            __syncwarp();
+        }
+    }
     const uint8_t *sp = p + hdr_sh;
     const uint32_t ssz = (uint32_t)(size - hdr_sh);
     const unsigned n = jb.n;
