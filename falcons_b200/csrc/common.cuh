@@ -6,6 +6,8 @@
 //   interpolation formulas   include/Falcons/utils/Interpolators.hpp:49-117
 //   linear quantizer         include/Falcons/quantizer/LinearQuantizer.hpp:49-133
 #pragma once
+#include <cmath>
+#include <limits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -161,10 +163,27 @@ __device__ __forceinline__ T apply_formula(int f, T a, T b, T c, T d) {
 struct QParams {
     double eb, ebx2, ebx2_r;
     int radius;
+    float ebf;  // the largest float <= eb: for a float e, |e| <= eb exactly when |e| <= ebf
 };
+
+// The largest float not above v (v >= 0).
+inline float float_at_most(double v) {
+    float f = (float)v;
+    if ((double)f > v) f = std::nextafter(f, -std::numeric_limits<float>::infinity());
+    return f;
+}
 
 // LinearQuantizer::quantize_and_overwrite / quantize_without_overwrite.  Returns the code;
 // `recon` receives the reconstructed value (the input itself for an unpredictable value).
+template <class T>
+__device__ __forceinline__ bool within_eb(T err, const QParams &qp) {
+    return (double)err >= -qp.eb && (double)err <= qp.eb;
+}
+template <>
+__device__ __forceinline__ bool within_eb<float>(float err, const QParams &qp) {
+    return fabsf(err) <= qp.ebf;  // the same test in float (NaN fails both)
+}
+
 template <class T>
 __device__ __forceinline__ int quantize(T x, T pred, const QParams &qp, T &recon) {
     using A = Arith<T>;
@@ -172,8 +191,7 @@ __device__ __forceinline__ int quantize(T x, T pred, const QParams &qp, T &recon
     const int q = __double2int_rn(__dmul_rn((double)diff, qp.ebx2_r));
     if (q > -qp.radius && q < qp.radius) {
         const T dq = A::from_double(__fma_rn((double)q, qp.ebx2, (double)pred));
-        const double err = (double)A::sub(dq, x);
-        if (err >= -qp.eb && err <= qp.eb) {
+        if (within_eb<T>(A::sub(dq, x), qp)) {
             recon = dq;
             return q;
         }

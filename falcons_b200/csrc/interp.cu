@@ -271,7 +271,7 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
         if (maxl <= level_count) level_count = maxl;
     }
     // index 0: the constructor's reciprocal 0.5/eb (used only by the anchor-free first point)
-    P.levels.push_back(QParams{p.eb, 2 * p.eb, 0.5 / p.eb, p.radius});
+    P.levels.push_back(QParams{p.eb, 2 * p.eb, 0.5 / p.eb, p.radius, float_at_most(p.eb)});
     Builder b(P, p);
     P.first_point = 0;
     P.n_anchor = 0;
@@ -293,7 +293,7 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
             cur = p.eb / ratio;
         }
         const int li = (int)P.levels.size();
-        P.levels.push_back(QParams{cur, 2 * cur, 1.0 / (2 * cur), p.radius});
+        P.levels.push_back(QParams{cur, 2 * cur, 1.0 / (2 * cur), p.radius, float_at_most(cur)});
         P.level_starts.push_back(b.pos);
         const long long s = 1LL << (level - 1);
         if (p.tuning || N == 4) b.tuning_level(li, s);
@@ -476,22 +476,30 @@ __global__ void __launch_bounds__(kTileThreads) k_esc_count(const int16_t *__res
     }
 }
 
-// Exclusive scan of tile counts (single block, chunked); writes offsets[0..ntiles] and the total.
+// Exclusive scan of tile counts (single block; every thread scans kScanRun consecutive counts per
+// round); writes offsets[0..ntiles] and the total.
+constexpr int kScanRun = 16;
 __global__ void __launch_bounds__(1024) k_scan_u32(const unsigned *__restrict__ in, unsigned long long *__restrict__ out,
                                                    long long n, unsigned long long *total) {
     __shared__ unsigned long long warp_sums[32];
     __shared__ unsigned long long carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (long long base = 0; base < n; base += 1024) {
-        const long long i = base + threadIdx.x;
-        unsigned long long v = i < n ? in[i] : 0;
-        // inclusive warp scan
-        unsigned long long s = v;
+    for (long long base = 0; base < n; base += 1024LL * kScanRun) {
+        const long long i0 = base + (long long)threadIdx.x * kScanRun;
+        unsigned v[kScanRun];
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int j = 0; j < kScanRun; j++) {
+            v[j] = i0 + j < n ? __ldg(in + i0 + j) : 0u;
+            sum += v[j];
+        }
+        // inclusive warp scan of the run sums, then across warps
+        unsigned long long s = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
-            if ((threadIdx.x & 31) >= o) s += y;
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+            if ((threadIdx.x & 31) >= (unsigned)o) s += y;
         }
         if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = s;
         __syncthreads();
@@ -499,14 +507,19 @@ __global__ void __launch_bounds__(1024) k_scan_u32(const unsigned *__restrict__ 
             unsigned long long w = warp_sums[threadIdx.x];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
-                if (threadIdx.x >= o) w += y;
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (threadIdx.x >= (unsigned)o) w += y;
             }
             warp_sums[threadIdx.x] = w;  // inclusive over warps
         }
         __syncthreads();
         const unsigned long long wprev = (threadIdx.x >> 5) ? warp_sums[(threadIdx.x >> 5) - 1] : 0;
-        if (i < n) out[i] = carry + wprev + s - v;
+        unsigned long long e = carry + wprev + s - sum;
+#pragma unroll
+        for (int j = 0; j < kScanRun; j++) {
+            if (i0 + j < n) out[i0 + j] = e;
+            e += v[j];
+        }
         __syncthreads();
         if (threadIdx.x == 1023) carry += wprev + s;
         __syncthreads();
@@ -705,6 +718,206 @@ void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParam
     FB2_CHECK_LAUNCH();
 }
 
+// The y pass and the x pass of one level of a field with unit x step (direction 0), fused: one
+// CTA per (z plane, tile of kFuseR rows x kFuseW columns) stages its tile plus a halo of kFuseHalo
+// rows and columns (every rule operand lies within 3 grid units of its target) in shared memory,
+// runs the y pass (ROW: odd rows, even columns; the halo columns' targets are recomputed so that
+// the x pass can read them) and then the x pass (LINE: odd columns) on the staged tile, and
+// writes the tile back once.  Codes and escape slots go to the positions the two passes have in
+// the code stream (InterpolationDecomposition.hpp:2294-2527 visiting order).
+struct FusedYX {
+    PassLaunch y;     // ROW pass along y: rows t = 1 + 2 b (b < y.B), columns at even x
+    PassLaunch late;  // its last-row pass (t = n - 1), when has_late
+    PassLaunch x;     // LINE pass along x: lines (z, y)
+    int has_late;
+};
+constexpr int kFuseW = 64, kFuseR = 64, kFuseHalo = 4;
+constexpr int kFusePW = kFuseW + 2 * kFuseHalo, kFusePR = kFuseR + 2 * kFuseHalo;
+constexpr int kFuseThreads = 256;
+
+template <class T, bool DECOMP>
+__global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *__restrict__ xf,
+                                                           int16_t *__restrict__ codes, T *__restrict__ esc,
+                                                           const QParams qp) {
+    __shared__ __align__(16) T tile[kFusePR * kFusePW];
+    constexpr int P = kFusePW, H = kFuseHalo;
+    const int ny = F.y.n, nx = F.x.n;
+    const long long a = blockIdx.z;
+    const int x0 = (int)blockIdx.x * kFuseW, x1 = min(nx, x0 + kFuseW);
+    const int y0 = (int)blockIdx.y * kFuseR, y1 = min(ny, y0 + kFuseR);
+    const int xl = max(0, x0 - H), xr = min(nx, x1 + H), TW = xr - xl;
+    const int yl = max(0, y0 - H), yr = min(ny, y1 + H), TR = yr - yl;
+    T *plane = xf + a * F.x.sa;
+    const long long sy = F.x.sb;
+    // stage rows [yl, yr) x columns [xl, xr) (tile row r, column c: y = yl + r, x = xl + c)
+    constexpr int V = 16 / sizeof(T);
+    const bool vec = ((reinterpret_cast<uintptr_t>(plane + xl) & 15) == 0) && (sy % V == 0) && (TW % V == 0);
+    if (vec) {
+        const int nq = TW / V;
+        for (int i = threadIdx.x; i < TR * nq; i += blockDim.x) {
+            const int rr = i / nq, qq = i - rr * nq;
+            const unsigned sa = (unsigned)__cvta_generic_to_shared(tile + rr * P + qq * V);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
+                         "l"(plane + (yl + rr) * sy + xl + qq * V)
+                         : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+    } else {
+        for (int i = threadIdx.x; i < TR * TW; i += blockDim.x) {
+            const int rr = i / TW, cc = i - rr * TW;
+            tile[rr * P + cc] = plane[(yl + rr) * sy + xl + cc];
+        }
+    }
+    __syncthreads();
+    // y pass: odd rows of [y0, y1) x even columns of [xl, xr); thread (column tc, row group g)
+    {
+        constexpr int NC = kFusePW / 2, NG = kFuseThreads / NC;
+        const int ce0 = (xl + 1) & ~1;
+        const int tc = threadIdx.x % NC, g = threadIdx.x / NC;
+        const int xg = ce0 + 2 * tc;
+        for (int tr = g; tr < kFuseR / 2 && g < NG && xg < xr; tr += NG) {
+            const int t = y0 + 1 + 2 * tr;
+            if (t >= y1) break;
+            const bool late = F.has_late && t == ny - 1;
+            const T *col = tile + (xg - xl) - yl * P;  // col[y * P] is (y, xg)
+            T pred;
+            if (t >= 3 && t <= ny - 5) {
+                pred = cubic_pred<T>(col[(t - 3) * P], col[(t - 1) * P], col[(t + 1) * P], col[(t + 3) * P]);
+            } else {
+                const Rule r = row_rule(true, t, ny, F.y.skip);
+                const T o0 = col[r.o0 * P];
+                const T o1 = r.f != F_EQUAL ? col[r.o1 * P] : o0;
+                const T o2 = r.f >= F_QUAD1 ? col[r.o2 * P] : o0;
+                const T o3 = r.f == F_CUBIC ? col[r.o3 * P] : o0;
+                pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+            }
+            const long long c = xg >> 1;
+            const long long p = late ? F.late.p_base + a * F.late.C + c
+                                     : F.y.p_base + (a * F.y.rows_in_group + ((t - 1) >> 1) + F.y.b_off) * F.y.C + c;
+            T *xp = tile + (t - yl) * P + (xg - xl);
+            if (!DECOMP) {
+                const bool own = xg >= x0 && xg < x1;
+                T recon;
+                const T v = *xp;
+                const int q = quantize<T>(v, pred, qp, recon);
+                if (own) codes[p] = (int16_t)q;
+                if (q == -qp.radius) {
+                    if (own) esc[p] = v;
+                } else if (!F.y.skip) {
+                    *xp = recon;
+                }
+            } else {
+                const int q = codes[p];
+                *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
+            }
+        }
+    }
+    __syncthreads();
+    // x pass: rows [y0, y1) x odd columns of [x0, x1); thread (column k, row group g)
+    {
+        constexpr int NO = kFuseW / 2, NG = kFuseThreads / NO;
+        static_assert(kFuseThreads % NO == 0, "whole row groups");
+        const int odd = nx / 2, tlo = 3, thi = 2 * odd - 5;
+        const int k = threadIdx.x % NO, g = threadIdx.x / NO;
+        const int t = x0 + 1 + 2 * k;
+        for (int yy = y0 + g; yy < y1 && t < x1; yy += NG) {
+            const T *row = tile + (yy - yl) * P - xl;  // row[x]
+            T pred;
+            if (t >= tlo && t <= thi) {
+                pred = cubic_pred<T>(row[t - 3], row[t - 1], row[t + 1], row[t + 3]);
+            } else {
+                const Rule r = line_rule(true, t, nx);
+                const T o0 = row[r.o0];
+                const T o1 = r.f != F_EQUAL ? row[r.o1] : o0;
+                const T o2 = r.f >= F_QUAD1 ? row[r.o2] : o0;
+                const T o3 = r.f == F_CUBIC ? row[r.o3] : o0;
+                pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+            }
+            const long long p = F.x.p_base + (a * F.x.B + yy) * F.x.C + ((t - 1) >> 1);
+            T *xp = tile + (yy - yl) * P + (t - xl);
+            if (!DECOMP) {
+                T recon;
+                const T v = *xp;
+                const int q = quantize<T>(v, pred, qp, recon);
+                codes[p] = (int16_t)q;
+                if (q == -qp.radius) esc[p] = v;
+                else if (!F.x.skip) *xp = recon;
+            } else {
+                const int q = codes[p];
+                *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
+            }
+        }
+    }
+    __syncthreads();
+    // write the tile back: every row, or (compress with a final x pass) the y pass's target rows
+    {
+        const bool odd_rows = !DECOMP && F.x.skip;
+        constexpr int NG = kFuseThreads / kFuseW;
+        static_assert(kFuseThreads % kFuseW == 0, "whole row groups");
+        const int cc = threadIdx.x % kFuseW, g = threadIdx.x / kFuseW;
+        const int ys = odd_rows ? 2 : 1;
+        if (x0 + cc < x1)
+            for (int yy = y0 + (odd_rows ? 1 : 0) + ys * g; yy < y1; yy += ys * NG)
+                plane[yy * sy + x0 + cc] = tile[(yy - yl) * P + (x0 - xl) + cc];
+    }
+}
+
+// Whether passes i (and i + 1, i + 2) form a fusable y + x pair; fills F.
+bool fusable_yx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedYX &F, size_t &used) {
+    if (i + 1 >= ps.size()) return false;
+    const PassLaunch &y = ps[i];
+    if (y.kind != KIND_ROW || !y.cubic || y.skip || y.t0 != 1 || y.b_off != 0 || y.B != y.rows_in_group) return false;
+    size_t j = i + 1;
+    F.has_late = 0;
+    if (ps[j].kind == KIND_ROW) {
+        const PassLaunch &e = ps[j];
+        if (e.t0 != y.n - 1 || e.B != 1 || e.rows_in_group != 1 || e.b_off != 0 || e.A != y.A || e.C != y.C ||
+            e.sa != y.sa || e.sc != y.sc || e.step != y.step || e.level != y.level || e.n != y.n || e.skip != y.skip ||
+            e.p_base != y.p_base + y.A * y.B * y.C)
+            return false;
+        F.late = e;
+        F.has_late = 1;
+        j++;
+        if (j >= ps.size()) return false;
+    }
+    if (y.B != y.n / 2 - (F.has_late ? 1 : 0)) return false;  // the passes cover every odd row
+    const PassLaunch &x = ps[j];
+    if (x.kind != KIND_LINE || !x.cubic || x.level != y.level || x.step != 1 || x.A != y.A || x.sa != y.sa ||
+        x.sb != y.step || x.B != y.n || x.C != x.n / 2 || y.sc != 2 || y.C != (x.n - 1) / 2 + 1 || y.A > 65535 ||
+        x.n < 2 || y.n < 2)
+        return false;
+    (void)elem;
+    if (y.A > 65535 || (y.n + kFuseR - 1) / kFuseR > 65535) return false;
+    F.y = y;
+    F.x = x;
+    used = j - i + 1;
+    return true;
+}
+
+template <class T, bool DECOMP>
+void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
+    dim3 grid((unsigned)((F.x.n + kFuseW - 1) / kFuseW), (unsigned)((F.y.n + kFuseR - 1) / kFuseR), (unsigned)F.y.A);
+    k_yx_fused<T, DECOMP><<<grid, kFuseThreads, 0, st>>>(F, x, codes, esc, qp);
+    FB2_CHECK_LAUNCH();
+}
+
+// Runs the plan's passes in order, the fusable y + x pairs as one kernel.
+template <class T, bool DECOMP>
+void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, cudaStream_t st) {
+    const std::vector<PassLaunch> &ps = plan.passes;
+    for (size_t i = 0; i < ps.size();) {
+        FusedYX F;
+        size_t used = 0;
+        if (fusable_yx(ps, i, sizeof(T), F, used)) {
+            launch_fused_yx<T, DECOMP>(F, x, codes, esc, plan.levels[F.y.level], st);
+            i += used;
+        } else {
+            launch_pass<T, DECOMP>(ps[i], x, codes, esc, plan.levels[ps[i].level], st);
+            i++;
+        }
+    }
+}
+
 struct WsLayout {
     size_t esc_off, tiles_off, scan_off, total_off, bytes;
     long long ntiles;
@@ -755,7 +968,7 @@ void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpr
         k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0]);
         FB2_CHECK_LAUNCH();
     }
-    for (const PassLaunch &L : plan.passes) launch_pass<T, false>(L, d_x, d_codes, esc, plan.levels[L.level], st);
+    run_passes<T, false>(plan, d_x, d_codes, esc, st);
     const int escc = -plan.levels[0].radius;
     if (w.ntiles > 0) {
         k_esc_count<<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, tiles);
@@ -801,7 +1014,7 @@ void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *
         k_first_point<T, true><<<1, 1, 0, st>>>(d_x, codes, esc, plan.levels[0]);
         FB2_CHECK_LAUNCH();
     }
-    for (const PassLaunch &L : plan.passes) launch_pass<T, true>(L, d_x, codes, esc, plan.levels[L.level], st);
+    run_passes<T, true>(plan, d_x, codes, esc, st);
 }
 
 // ------------------------------------------------------------------------------------------ range
@@ -882,6 +1095,9 @@ cudaError_t preload_decompress_kernels() {
         reinterpret_cast<const void *>(&k_pass<T, KIND_LINE, true>),
         reinterpret_cast<const void *>(&k_pass<T, KIND_GENERIC, true>),
         reinterpret_cast<const void *>(&k_pass<T, KIND_LEGACY, true>),
+        reinterpret_cast<const void *>(&k_row_fast<T, true>),
+        reinterpret_cast<const void *>(&k_line_smem<T, true>),
+        reinterpret_cast<const void *>(&k_yx_fused<T, true>),
     };
     for (const void *f : fns) {
         cudaFuncAttributes a;

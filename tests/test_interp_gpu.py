@@ -56,6 +56,17 @@ def test_exhaustive_small_3d(cuda, restatement):
                 _run(cuda, restatement, _field(shape, np.float32, sum(shape)), algo, direction)
 
 
+@pytest.mark.parametrize("shape,dtype", [((4, 700, 90), np.float32), ((5, 330, 75), np.float64),
+                                         ((3, 64, 200), np.float32), ((650, 101), np.float32),
+                                         ((6, 9, 133), np.float64)])
+def test_fused_level_passes(cuda, restatement, shape, dtype):
+    # the y and x passes of a level run as one kernel over x chunks (with halos); long rows, long
+    # columns (narrower chunks) and ragged last chunks
+    for algo in (0, 1):
+        for direction in ((0, 1) if len(shape) == 2 else (0, 5)):
+            _run(cuda, restatement, _field(shape, dtype, 11), algo, direction)
+
+
 @pytest.mark.parametrize("shape", [(33, 40, 17), (20, 21, 22), (5, 6, 7, 8), (17, 3, 9, 4)])
 def test_generic_and_tuning_sweeps(cuda, restatement, shape):
     for algo in (0, 1):
