@@ -1417,21 +1417,24 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t 
 // CTA.  A tANS encoder walks its chain backwards and only its state carries from one code to the
 // next, so:
 //   1. every part runs from a guessed entering state (the top part from the exact initial state),
-//      keeping the state at every 64th index (`sparse`) and its exit state;
-//   2. repair rounds: each part reruns from the exit state of the part above until its state
-//      equals a kept one (from there on the two runs are identical); a part that never meets its
-//      kept states has a new exit state, so the part below repairs again in the next round.
-//      Encoder states from different starting points meet after a few hundred codes, so one round
-//      nearly always suffices, and the loop ends after at most one round per part;
-//   3. emission: every part reruns from its exact entering state and writes its bits to its own
-//      staging area, counting them;
+//      writing its bits to its own staging area and keeping the state and the bit count at every
+//      64th index (`sparse`, `sparse_bits`) and its exit state;
+//   2. repair rounds: each part reruns from the exit state of the part above, writing the bits
+//      again into a second staging area, until its state equals a kept one (from there on the two
+//      runs, and their bits, are identical); a part that never meets its kept states has a new
+//      exit state, so the part below repairs again in the next round.  Encoder states from
+//      different starting points meet after a few hundred codes, so one round nearly always
+//      suffices, and the loop ends after at most one round per part;
+//   3. (the bits of a part: the repaired bits above the meeting index, then the speculative ones)
 //   4. the bit counts give every part its offset in the chain's stream; every part shifts its
-//      staged words into place (words shared with a neighbour are merged with atomicOr);
+//      staged bits into place (words shared with a neighbour are merged with atomicOr);
 //   5. every part start is a decode checkpoint: state, bit position, context and escape count.
 // The stream is bit-identical to a sequential encoder's (the tANS states are fully determined).
+// All 15 context state tables stay in shared memory, as 13-bit entries (state - 8192) packed into
+// words, next to the symbol transforms (deltaNbBits as a word, deltaFindState + 8192 as 16 bits).
 constexpr int kSpecThreads = 1024;
-constexpr int kSpecSlots = 10;  // 10 x 16 KiB state tables + 30 KiB symbol transforms in shared memory
-constexpr size_t kSpecSmem = (size_t)O1_NCTX * O1_NSYM * sizeof(fse::SymTT) + (size_t)kSpecSlots * O1_M * 2;
+constexpr unsigned kSpecPackWords = O1_NCTX * O1_M * O1_PB / 32 + 1;  // + 1: a read of word w + 1
+constexpr size_t kSpecSmem = (size_t)kSpecPackWords * 4 + (size_t)O1_NCTX * O1_NSYM * (4 + 2);
 constexpr int kSparseShift = 6;  // kept speculative states: every 64th index
 struct SpecCta {
     int table;
@@ -1481,42 +1484,47 @@ __device__ __forceinline__ void walk_keys(const uint16_t *__restrict__ keys, lon
     for (; i >= bottom; i--) f(i, (uint32_t)__ldg(keys + i));
 }
 
-// Per key (context << 8 | symbol) the encoder's symbol transform, with the table position folded
-// in: deltaFindState + 8192 * slot for a context resident in shared memory, or kFarTable +
-// 8192 * context for one read from global memory.
+// Per key (context << 8 | symbol) the encoder's symbol transform: the bit position of the
+// symbol's state-table block in the packed tables (13 x (8192 x context + deltaFindState)) and
+// deltaNbBits.
 struct EncRec {
-    uint32_t dfs;
+    int32_t b13;
     uint32_t dnb;
 };
-constexpr uint32_t kFarTable = 1u << 30;
 
 __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     const uint16_t *__restrict__ keys, const SegInfo *__restrict__ segs, const SpecCta *__restrict__ ctas,
     const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, uint16_t *__restrict__ sparse,
-    uint32_t *__restrict__ stage, uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
+    uint16_t *__restrict__ sparse_bits, uint32_t *__restrict__ stage, uint32_t *__restrict__ rstage,
+    uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
     unsigned long long *__restrict__ blen, uint32_t part, O1Ckpt *__restrict__ cks,
     const unsigned long long *__restrict__ ck_off, uint32_t ck_every, int *__restrict__ err) {
     extern __shared__ uint4 smem_raw[];
-    EncRec *rec = reinterpret_cast<EncRec *>(smem_raw);
-    uint16_t *sst = reinterpret_cast<uint16_t *>(rec + O1_NCTX * O1_NSYM);
-    __shared__ uint32_t s_bits[kSpecThreads], s_esc[kSpecThreads], s_exit[kSpecThreads + 1];
-    __shared__ int s_chg[kSpecThreads + 1];
+    uint32_t *pk = reinterpret_cast<uint32_t *>(smem_raw);  // packed state tables
+    uint32_t *r_dnb = pk + kSpecPackWords;                   // deltaNbBits per key
+    uint16_t *r_dfs = reinterpret_cast<uint16_t *>(r_dnb + O1_NCTX * O1_NSYM);  // deltaFindState + 8192
+    // after the walks, the transforms' space holds the parts' bit and escape counts
+    uint16_t *s_bits = reinterpret_cast<uint16_t *>(r_dnb), *s_esc = s_bits + kSpecThreads;
+    __shared__ uint16_t s_exit[kSpecThreads + 1];
+    __shared__ uint8_t s_chg[kSpecThreads + 1];
     const SpecCta w = ctas[blockIdx.x];
     const size_t tb = (size_t)w.table * O1_NCTX;
     const uint16_t *__restrict__ S = stab + tb * O1_M;
     for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) {
         const fse::SymTT t0 = stt[tb * O1_NSYM + i];
-        const int c = i >> 8;
-        const uint32_t sl = (uint32_t)(w.map >> (4 * c)) & 15u;
-        const uint32_t base = sl < (uint32_t)kSpecSlots ? sl * O1_M : kFarTable + (uint32_t)c * O1_M;
-        rec[i] = EncRec{(uint32_t)t0.deltaFindState + base, t0.deltaNbBits};
+        r_dnb[i] = t0.deltaNbBits;
+        r_dfs[i] = (uint16_t)(t0.deltaFindState + O1_M);
     }
-    for (int j = 0; j < kSpecSlots; j++) {
-        const int c = (int)((w.rev >> (4 * j)) & 15);
-        if (c >= O1_NCTX) continue;
-        const uint4 *s2 = reinterpret_cast<const uint4 *>(S + (size_t)c * O1_M);
-        uint4 *d2 = reinterpret_cast<uint4 *>(sst + (size_t)j * O1_M);
-        for (int i = threadIdx.x; i < O1_M * 2 / 16; i += blockDim.x) d2[i] = __ldg(s2 + i);
+    // word wd holds the bits [32 wd, 32 wd + 32) of the entries (entry j at bit 13 j)
+    for (unsigned wd = threadIdx.x; wd < kSpecPackWords; wd += blockDim.x) {
+        uint32_t v = 0;
+        const unsigned j0 = wd * 32 / O1_PB, j1 = min((wd * 32 + 31) / O1_PB, (unsigned)(O1_NCTX * O1_M - 1));
+        for (unsigned j = j0; j <= j1 && j < (unsigned)(O1_NCTX * O1_M); j++) {
+            const uint32_t e = (uint32_t)__ldg(S + j) - O1_M;  // 13 bits
+            const int sh = (int)(j * O1_PB) - (int)(wd * 32);
+            v |= sh >= 0 ? e << sh : e >> -sh;
+        }
+        pk[wd] = v;
     }
     const int t = threadIdx.x;
     const int ci = t / w.ppc, p = t % w.ppc;
@@ -1543,12 +1551,16 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         s_exit[kSpecThreads] = 0;
     }
     __syncthreads();
+    auto rec_of = [&](uint32_t k) -> EncRec {
+        return EncRec{((int32_t)((k >> 8) << O1_PB) + (int32_t)r_dfs[k] - O1_M) * O1_PB, r_dnb[k]};
+    };
     auto next_state = [&](uint32_t x, const EncRec r, uint32_t nb) -> uint32_t {
-        const uint32_t y = (x >> nb) + r.dfs;
-        return y < kFarTable ? (uint32_t)sst[y] : (uint32_t)__ldg(S + (y - kFarTable));
+        const uint32_t bit = (uint32_t)(r.b13 + (int32_t)(x >> nb) * O1_PB);
+        const uint32_t wd = bit >> 5;
+        return O1_M + (__funnelshift_r(pk[wd], pk[wd + 1], bit & 31u) & (O1_M - 1));
     };
     auto init_state = [&](uint32_t k) -> uint32_t {
-        const EncRec r = rec[k];
+        const EncRec r = rec_of(k);
         const uint32_t nb = (r.dnb + (1u << 15)) >> 16;
         return next_state((nb << 16) - r.dnb, r, nb);
     };
@@ -1556,32 +1568,76 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     const long long istart = is_top ? hi - 2 : top;
     const long long bottom = p == 0 ? a + 1 : a;
     const uint32_t k_lo = p == 0 && active ? ((uint32_t)__ldg(keys + lo) & 0xFFu) : 0u;
-    // 1. speculative pass
-    uint32_t esc = 0;
+    // Bit writer into a part's staging words (LSB first, as the stream).
+    struct Stager {
+        uint32_t *w;
+        uint64_t acc = 0;
+        uint32_t accn = 0, nw = 0, bits = 0;
+        __device__ void put(uint32_t v, uint32_t nb) {
+            acc |= (uint64_t)(v & ((1u << nb) - 1u)) << accn;
+            accn += nb;
+            bits += nb;
+            if (accn >= 32) {
+                w[nw++] = (uint32_t)acc;
+                acc >>= 32;
+                accn -= 32;
+            }
+        }
+        __device__ void flush() {
+            if (accn > 0) w[nw] = (uint32_t)acc;
+        }
+    };
+    const size_t stw = spec_stage_words(part);
+    uint32_t *sw = stage + ((size_t)blockIdx.x * kSpecThreads + t) * stw;   // speculative bits
+    uint32_t *rw = rstage + ((size_t)blockIdx.x * kSpecThreads + t) * stw;  // repaired bits
+    // 1. speculative pass: walk and emit from the guessed state, keeping the state and the bit
+    //    count after every 64th index
+    uint32_t esc = 0, spec_bits = 0, spec_exit = 0;
     if (active) {
+        Stager sg{sw};
         uint32_t x;
         if (is_top) {
             const uint32_t k0 = hi - 1 == lo ? k_lo : (uint32_t)__ldg(keys + hi - 1);
             x = init_state(k0);
             esc += (k0 & 0xFFu) == 0xFFu;
-            if (((hi - 1) & 63) == 0) sparse[(hi - 1) >> 6] = (uint16_t)x;
+            if (((hi - 1) & 63) == 0) {
+                sparse[(hi - 1) >> 6] = (uint16_t)x;
+                sparse_bits[(hi - 1) >> 6] = 0;
+            }
         } else {
             x = init_state((uint32_t)__ldg(keys + top + 1));
         }
         auto step = [&](long long i, uint32_t k) {
-            const EncRec r = rec[k];
+            const EncRec r = rec_of(k);
             const uint32_t nb = (x + r.dnb) >> 16;
+            sg.put(x, nb);
             x = next_state(x, r, nb);
             esc += (k & 0xFFu) == 0xFFu;
-            if (((uint32_t)i & 63u) == 0) sparse[i >> 6] = (uint16_t)x;
+            if (((uint32_t)i & 63u) == 0) {
+                sparse[i >> 6] = (uint16_t)x;
+                sparse_bits[i >> 6] = (uint16_t)sg.bits;
+            }
         };
         walk_keys(keys, istart, bottom, step);
         if (p == 0 && istart >= lo) step(lo, k_lo);
-        s_exit[t] = x;
+        if (p == 0) {
+            sg.put(x & (O1_M - 1), O1_PB);  // the final state, then the end mark
+            sg.put(1u, 1u);
+        }
+        sg.flush();
+        spec_bits = sg.bits;
+        spec_exit = x;
+        s_exit[t] = (uint16_t)x;
     }
-    // 2. repair rounds (err[2] counts the re-run codes, err[3] the rounds, for diagnostics)
+    // 2. repair rounds (err[2] counts the re-run codes, err[3] the rounds, for diagnostics): a part
+    //    whose entering state changed walks again from it, emitting into its repair staging, until
+    //    its state meets a kept one at index m; its bits are then the repaired bits of the codes
+    //    above m followed by the speculative bits from m on.  A part that never meets has all its
+    //    bits in the repair staging and a new exit state, so the part below repairs again.
     bool need = active && !is_top;
     uint32_t repaired = 0;
+    int mode = 0;                    // 0 speculative bits, 1 met, 2 repaired whole
+    uint32_t rep_bits = 0, cut = 0;  // repaired bits; speculative bit where the suffix starts
     for (int round = 0;; round++) {
         if (round > nparts + 2 && need) atomicExch(err, 5);
         if (t == 0) atomicMax(err + 3, round);
@@ -1589,26 +1645,33 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         __syncthreads();
         bool changed = false;
         if (need && round <= nparts + 2) {
+            Stager rg{rw};
             uint32_t x = E;
             bool met = false;
             for (long long i = top; i >= a; i--) {
                 const uint32_t k = i == lo ? k_lo : (uint32_t)__ldg(keys + i);
-                const EncRec r = rec[k];
+                const EncRec r = rec_of(k);
                 const uint32_t nb = (x + r.dnb) >> 16;
+                rg.put(x, nb);
                 x = next_state(x, r, nb);
                 repaired++;
-                if (((uint32_t)i & 63u) == 0) {
-                    if (sparse[i >> 6] == (uint16_t)x) {
-                        met = true;
-                        break;
-                    }
-                    sparse[i >> 6] = (uint16_t)x;
+                if (((uint32_t)i & 63u) == 0 && sparse[i >> 6] == (uint16_t)x) {
+                    met = true;
+                    cut = sparse_bits[i >> 6];
+                    break;
                 }
             }
-            if (!met) {
-                changed = x != s_exit[t];
-                s_exit[t] = x;
+            if (!met && p == 0) {
+                rg.put(x & (O1_M - 1), O1_PB);
+                rg.put(1u, 1u);
             }
+            rg.flush();
+            rep_bits = rg.bits;
+            // the exit state: the speculative run's once met, else this run's
+            const uint32_t ex = met ? spec_exit : x;
+            mode = met ? 1 : 2;
+            changed = ex != s_exit[t];
+            s_exit[t] = (uint16_t)ex;
         }
         s_chg[t] = changed;
         __syncthreads();
@@ -1616,42 +1679,12 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         if (!__syncthreads_or(need)) break;
     }
     if (repaired) atomicAdd(err + 2, (int)repaired);
-    // 3. emission into the part's staging area
-    uint32_t bits = 0;
-    uint32_t *sw = stage + ((size_t)blockIdx.x * kSpecThreads + t) * spec_stage_words(part);
-    if (active) {
-        uint32_t x = is_top ? init_state(hi - 1 == lo ? k_lo : (uint32_t)__ldg(keys + hi - 1)) : s_exit[t + 1];
-        uint64_t acc = 0;
-        uint32_t accn = 0, nw = 0;
-        auto put = [&](uint32_t v, uint32_t nb) {
-            acc |= (uint64_t)(v & ((1u << nb) - 1u)) << accn;
-            accn += nb;
-            if (accn >= 32) {
-                sw[nw++] = (uint32_t)acc;
-                acc >>= 32;
-                accn -= 32;
-            }
-        };
-        auto step = [&](long long, uint32_t k) {
-            const EncRec r = rec[k];
-            const uint32_t nb = (x + r.dnb) >> 16;
-            put(x, nb);
-            bits += nb;
-            x = next_state(x, r, nb);
-        };
-        walk_keys(keys, istart, bottom, step);
-        if (p == 0 && istart >= lo) step(lo, k_lo);
-        if (x != s_exit[t]) atomicExch(err, 5);
-        if (p == 0) {
-            put(x & (O1_M - 1), O1_PB);  // the final state, then the end mark
-            put(1u, 1u);
-            bits += O1_PB + 1;
-        }
-        if (accn > 0) sw[nw] = (uint32_t)acc;
-    }
+    // the part's bits: [rw bits 0, rep_bits) then [sw bits cut, spec_bits)
+    const uint32_t bits = mode == 0 ? spec_bits : mode == 1 ? rep_bits + (spec_bits - cut) : rep_bits;
     // 4. offsets (the top part's bits come first), escapes below each part, placement
-    s_bits[t] = active ? bits : 0u;
-    s_esc[t] = active ? esc : 0u;
+    __syncthreads();  // the symbol transforms' space is reused for the counts
+    s_bits[t] = active ? (uint16_t)bits : (uint16_t)0;
+    s_esc[t] = active ? (uint16_t)esc : (uint16_t)0;
     __syncthreads();
     uint32_t off = 0, esc_below = 0;
     if (active) {
@@ -1665,20 +1698,34 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         // Output words [w0, wend).  Word w0 was zeroed by this part; the last word, when the part
         // ends inside it and a part follows, is the next part's first word (zeroed by it).  Both are
         // merged with atomicOr, every other word is this part's alone.
-        const uint32_t sh = off & 31u, nwords = (bits + 31) / 32;
         const uint32_t w0 = off >> 5, wend = (off + bits + 31) >> 5;
         const uint32_t shared_last = (p > 0 && ((off + bits) & 31u)) ? wend - 1 : 0xFFFFFFFFu;
-        auto store = [&](uint32_t wi, uint32_t v) {
+        uint32_t wi = w0;
+        auto store = [&](uint32_t v) {
             if (wi == w0 || wi == shared_last) atomicOr(ow + wi, v);
             else ow[wi] = v;
+            wi++;
         };
-        uint32_t prev = 0;
-        for (uint32_t j = 0; j < nwords; j++) {
-            const uint32_t cur = sw[j];
-            store(w0 + j, sh ? (cur << sh) | (j ? prev >> (32 - sh) : 0u) : cur);
-            prev = cur;
-        }
-        if (sh && w0 + nwords < wend) store(w0 + nwords, prev >> (32 - sh));
+        uint64_t acc = 0;
+        uint32_t accn = off & 31u;
+        // appends bits [b0, b1) of staging words src
+        auto append = [&](const uint32_t *src, uint32_t b0, uint32_t b1) {
+            for (uint32_t bp = b0; bp < b1; bp += 32) {
+                const uint32_t n = min(32u, b1 - bp), j = bp >> 5, sh = bp & 31u;
+                uint32_t v = sh ? __funnelshift_r(src[j], src[j + 1], sh) : src[j];
+                if (n < 32) v &= (1u << n) - 1u;
+                acc |= (uint64_t)v << accn;
+                accn += n;
+                if (accn >= 32) {
+                    store((uint32_t)acc);
+                    acc >>= 32;
+                    accn -= 32;
+                }
+            }
+        };
+        if (mode != 0) append(rw, 0, rep_bits);
+        if (mode != 2) append(sw, mode == 1 ? cut : 0u, spec_bits);
+        if (accn > 0) store((uint32_t)acc);
         if (p == 0) blen[chain] = ((unsigned long long)off + bits + 7) / 8;
         // 5. decode checkpoint at every ck_every-th part start: the state the decoder holds
         // before index a
@@ -2271,14 +2318,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint8_t *slots = pool.get<uint8_t>(soff.back() + 16);
         unsigned long long *blen = pool.get<unsigned long long>(nchains);
         {
-            std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
-            tr.mark("tables normalized");
-            std::vector<unsigned long long> maps(R), revs(R);
-            for (int r = 0; r < R; r++) {
-                auto mr = hot_contexts(hnf.data() + (size_t)r * O1_NCTX * O1_NSYM, kSpecSlots);
-                maps[r] = mr.first;
-                revs[r] = mr.second;
-            }
+            tr.mark("tables launched");
+            const std::vector<unsigned long long> maps(R, 0), revs(R, 0);  // every table is resident
             std::vector<int> chain_table((size_t)nchains);
             for (long long ch = 0; ch < nchains; ch++) chain_table[ch] = seg_region[ch / kMaxK];
             const std::vector<ChainCta> groups = chain_ctas(chain_table, maps, revs, (size_t)(kSpecThreads / ppc));
@@ -2287,13 +2328,15 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             SpecCta *d_ctas = h2d(pool, ctas, st);
             uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
             uint16_t *sparse = pool.get<uint16_t>(((size_t)N >> kSparseShift) + 2);
+            uint16_t *sparse_bits = pool.get<uint16_t>(((size_t)N >> kSparseShift) + 2);
             uint32_t *stage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
+            uint32_t *rstage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
             k_o1_keys<<<grid_for(N, 256, 148 * 16), 256, 0, st>>>(q, N, keys);
             FB2_CHECK_LAUNCH();
             enable_big_smem();
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
-                keys, d_segs, d_ctas, stab, stt, sparse, stage, slots, d_soff, blen, enc_part, o1ck, d_ck_off, ck_every,
-                d_err);
+                keys, d_segs, d_ctas, stab, stt, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
+                d_ck_off, ck_every, d_err);
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
         }
