@@ -1430,11 +1430,13 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t 
 //      staged bits into place (words shared with a neighbour are merged with atomicOr);
 //   5. every part start is a decode checkpoint: state, bit position, context and escape count.
 // The stream is bit-identical to a sequential encoder's (the tANS states are fully determined).
-// All 15 context state tables stay in shared memory, as 13-bit entries (state - 8192) packed into
-// words, next to the symbol transforms (deltaNbBits as a word, deltaFindState + 8192 as 16 bits).
+// All 15 context state tables stay in shared memory: the two contexts that carry most codes (from
+// the table set's histogram) as 16-bit states, the other 13 as 13-bit entries (state - 8192)
+// packed into words; one word per key holds the symbol transform.
 constexpr int kSpecThreads = 1024;
-constexpr unsigned kSpecPackWords = O1_NCTX * O1_M * O1_PB / 32 + 1;  // + 1: a read of word w + 1
-constexpr size_t kSpecSmem = (size_t)kSpecPackWords * 4 + (size_t)O1_NCTX * O1_NSYM * (4 + 2);
+constexpr int kSpecHot = 2;
+constexpr unsigned kSpecPackWords = (O1_NCTX - kSpecHot) * O1_M * O1_PB / 32 + 1;  // + 1: a read of w + 1
+constexpr size_t kSpecSmem = (size_t)kSpecHot * O1_M * 2 + (size_t)kSpecPackWords * 4 + (size_t)O1_NCTX * O1_NSYM * 4;
 constexpr int kSparseShift = 6;  // kept speculative states: every 64th index
 struct SpecCta {
     int table;
@@ -1484,43 +1486,78 @@ __device__ __forceinline__ void walk_keys(const uint16_t *__restrict__ keys, lon
     for (; i >= bottom; i--) f(i, (uint32_t)__ldg(keys + i));
 }
 
-// Per key (context << 8 | symbol) the encoder's symbol transform: the bit position of the
-// symbol's state-table block in the packed tables (13 x (8192 x context + deltaFindState)) and
-// deltaNbBits.
-struct EncRec {
-    int32_t b13;
-    uint32_t dnb;
-};
+// Per key (context << 8 | symbol) the encoder's symbol transform, as one word: deltaFindState +
+// 8192 (bits 0-13), minStatePlus - 8192 (14-27) and maxBitsOut (28-31); the emitted bit count of
+// state x is maxBitsOut - (x < minStatePlus), which is (x + deltaNbBits) >> 16 with deltaNbBits =
+// (maxBitsOut << 16) - minStatePlus.
+__host__ __device__ __forceinline__ uint32_t enc_word(const fse::SymTT &t) {
+    const uint32_t mbo = (t.deltaNbBits + 0xFFFFu) >> 16, msp = (mbo << 16) - t.deltaNbBits;
+    return (uint32_t)(t.deltaFindState + O1_M) | ((msp - O1_M) << 14) | (mbo << 28);
+}
 
 __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     const uint16_t *__restrict__ keys, const SegInfo *__restrict__ segs, const SpecCta *__restrict__ ctas,
-    const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, uint16_t *__restrict__ sparse,
+    const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, const uint32_t *__restrict__ thist,
+    uint16_t *__restrict__ sparse,
     uint16_t *__restrict__ sparse_bits, uint32_t *__restrict__ stage, uint32_t *__restrict__ rstage,
     uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
     unsigned long long *__restrict__ blen, uint32_t part, O1Ckpt *__restrict__ cks,
     const unsigned long long *__restrict__ ck_off, uint32_t ck_every, int *__restrict__ err) {
     extern __shared__ uint4 smem_raw[];
-    uint32_t *pk = reinterpret_cast<uint32_t *>(smem_raw);  // packed state tables
-    uint32_t *r_dnb = pk + kSpecPackWords;                   // deltaNbBits per key
-    uint16_t *r_dfs = reinterpret_cast<uint16_t *>(r_dnb + O1_NCTX * O1_NSYM);  // deltaFindState + 8192
+    uint16_t *hot = reinterpret_cast<uint16_t *>(smem_raw);           // kSpecHot 16-bit tables
+    uint32_t *pk = reinterpret_cast<uint32_t *>(hot + kSpecHot * O1_M);  // packed state tables
+    uint32_t *r_enc = pk + kSpecPackWords;                              // symbol transform per key
     // after the walks, the transforms' space holds the parts' bit and escape counts
-    uint16_t *s_bits = reinterpret_cast<uint16_t *>(r_dnb), *s_esc = s_bits + kSpecThreads;
+    uint16_t *s_bits = reinterpret_cast<uint16_t *>(r_enc), *s_esc = s_bits + kSpecThreads;
     __shared__ uint16_t s_exit[kSpecThreads + 1];
     __shared__ uint8_t s_chg[kSpecThreads + 1];
+    __shared__ unsigned long long s_map;  // table slot of every context (4 bits each)
+    __shared__ uint8_t s_rev[O1_NCTX];    // context of every slot
     const SpecCta w = ctas[blockIdx.x];
     const size_t tb = (size_t)w.table * O1_NCTX;
     const uint16_t *__restrict__ S = stab + tb * O1_M;
-    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) {
-        const fse::SymTT t0 = stt[tb * O1_NSYM + i];
-        r_dnb[i] = t0.deltaNbBits;
-        r_dfs[i] = (uint16_t)(t0.deltaFindState + O1_M);
+    if (threadIdx.x < 32) {
+        // codes per context in the table set's histogram; the two largest get the 16-bit slots
+        uint32_t tot[O1_NCTX];
+        for (int c = 0; c < O1_NCTX; c++) {
+            uint32_t v = 0;
+            for (int sy = threadIdx.x; sy < O1_NSYM; sy += 32) v += __ldg(thist + (tb + c) * O1_NSYM + sy);
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            tot[c] = v;
+        }
+        if (threadIdx.x == 0) {
+            int h0 = 0, h1 = 1;
+            if (tot[h1] > tot[h0]) h0 = 1, h1 = 0;
+            for (int c = 2; c < O1_NCTX; c++) {
+                if (tot[c] > tot[h0]) h1 = h0, h0 = c;
+                else if (tot[c] > tot[h1]) h1 = c;
+            }
+            unsigned long long m = 0;
+            int slot = kSpecHot;
+            s_rev[0] = (uint8_t)h0;
+            s_rev[1] = (uint8_t)h1;
+            for (int c = 0; c < O1_NCTX; c++) {
+                const int sl = c == h0 ? 0 : c == h1 ? 1 : slot++;
+                m |= (unsigned long long)sl << (4 * c);
+                if (sl >= kSpecHot) s_rev[sl] = (uint8_t)c;
+            }
+            s_map = m;
+        }
     }
-    // word wd holds the bits [32 wd, 32 wd + 32) of the entries (entry j at bit 13 j)
+    __syncthreads();
+    const unsigned long long smap = s_map;
+    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) r_enc[i] = enc_word(stt[tb * O1_NSYM + i]);
+    for (int i = threadIdx.x; i < kSpecHot * O1_M; i += blockDim.x)
+        hot[i] = __ldg(S + (size_t)s_rev[i / O1_M] * O1_M + (i % O1_M));
+    // word wd holds the bits [32 wd, 32 wd + 32) of the packed entries (entry j at bit 13 j; entry
+    // j is state u = j % 8192 of the context in slot kSpecHot + j / 8192)
+    constexpr unsigned kPacked = (O1_NCTX - kSpecHot) * O1_M;
     for (unsigned wd = threadIdx.x; wd < kSpecPackWords; wd += blockDim.x) {
         uint32_t v = 0;
-        const unsigned j0 = wd * 32 / O1_PB, j1 = min((wd * 32 + 31) / O1_PB, (unsigned)(O1_NCTX * O1_M - 1));
-        for (unsigned j = j0; j <= j1 && j < (unsigned)(O1_NCTX * O1_M); j++) {
-            const uint32_t e = (uint32_t)__ldg(S + j) - O1_M;  // 13 bits
+        const unsigned j0 = wd * 32 / O1_PB, j1 = min((wd * 32 + 31) / O1_PB, kPacked - 1);
+        for (unsigned j = j0; j <= j1 && j < kPacked; j++) {
+            const unsigned c = s_rev[kSpecHot + j / O1_M];
+            const uint32_t e = (uint32_t)__ldg(S + (size_t)c * O1_M + (j % O1_M)) - O1_M;  // 13 bits
             const int sh = (int)(j * O1_PB) - (int)(wd * 32);
             v |= sh >= 0 ? e << sh : e >> -sh;
         }
@@ -1551,24 +1588,38 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         s_exit[kSpecThreads] = 0;
     }
     __syncthreads();
+    // a key's transform word and table slot
+    struct EncRec {
+        uint32_t e, slot;
+    };
     auto rec_of = [&](uint32_t k) -> EncRec {
-        return EncRec{((int32_t)((k >> 8) << O1_PB) + (int32_t)r_dfs[k] - O1_M) * O1_PB, r_dnb[k]};
+        return EncRec{r_enc[k], (uint32_t)(smap >> (4 * (k >> 8))) & 15u};
+    };
+    auto nbits = [](uint32_t x, const EncRec r) -> uint32_t {
+        return (r.e >> 28) - ((x - (((r.e >> 14) & 0x3FFFu) + O1_M)) >> 31);
     };
     auto next_state = [&](uint32_t x, const EncRec r, uint32_t nb) -> uint32_t {
-        const uint32_t bit = (uint32_t)(r.b13 + (int32_t)(x >> nb) * O1_PB);
+        const uint32_t idx = (x >> nb) + (r.e & 0x3FFFu) - O1_M;  // within the context's table
+        if (r.slot < (uint32_t)kSpecHot) return hot[(r.slot << O1_PB) + idx];
+        const uint32_t bit = (((r.slot - kSpecHot) << O1_PB) + idx) * O1_PB;
         const uint32_t wd = bit >> 5;
         return O1_M + (__funnelshift_r(pk[wd], pk[wd + 1], bit & 31u) & (O1_M - 1));
     };
     auto init_state = [&](uint32_t k) -> uint32_t {
+        // FSE_initCState2: the state that codes symbol k with the fewest bits
         const EncRec r = rec_of(k);
-        const uint32_t nb = (r.dnb + (1u << 15)) >> 16;
-        return next_state((nb << 16) - r.dnb, r, nb);
+        const uint32_t mbo = r.e >> 28, msp = ((r.e >> 14) & 0x3FFFu) + O1_M;
+        const uint32_t dnb = (mbo << 16) - msp;
+        const uint32_t nb = (dnb + (1u << 15)) >> 16;
+        return next_state((nb << 16) - dnb, r, nb);
     };
     // the first code of a chain has context 0, so index lo is coded apart from the walks
     const long long istart = is_top ? hi - 2 : top;
     const long long bottom = p == 0 ? a + 1 : a;
     const uint32_t k_lo = p == 0 && active ? ((uint32_t)__ldg(keys + lo) & 0xFFu) : 0u;
-    // Bit writer into a part's staging words (LSB first, as the stream).
+    // Bit writer into a part's staging words (LSB first, as the stream).  The CTA's staging areas
+    // are interleaved (word j of thread t at j * kSpecThreads + t), so that the placement step's
+    // reads of the same word j by a warp share cache lines.
     struct Stager {
         uint32_t *w;
         uint64_t acc = 0;
@@ -1578,18 +1629,18 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
             accn += nb;
             bits += nb;
             if (accn >= 32) {
-                w[nw++] = (uint32_t)acc;
+                w[(size_t)(nw++) * kSpecThreads] = (uint32_t)acc;
                 acc >>= 32;
                 accn -= 32;
             }
         }
         __device__ void flush() {
-            if (accn > 0) w[nw] = (uint32_t)acc;
+            if (accn > 0) w[(size_t)nw * kSpecThreads] = (uint32_t)acc;
         }
     };
     const size_t stw = spec_stage_words(part);
-    uint32_t *sw = stage + ((size_t)blockIdx.x * kSpecThreads + t) * stw;   // speculative bits
-    uint32_t *rw = rstage + ((size_t)blockIdx.x * kSpecThreads + t) * stw;  // repaired bits
+    uint32_t *sw = stage + (size_t)blockIdx.x * kSpecThreads * stw + t;   // speculative bits
+    uint32_t *rw = rstage + (size_t)blockIdx.x * kSpecThreads * stw + t;  // repaired bits
     // 1. speculative pass: walk and emit from the guessed state, keeping the state and the bit
     //    count after every 64th index
     uint32_t esc = 0, spec_bits = 0, spec_exit = 0;
@@ -1609,7 +1660,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         }
         auto step = [&](long long i, uint32_t k) {
             const EncRec r = rec_of(k);
-            const uint32_t nb = (x + r.dnb) >> 16;
+            const uint32_t nb = nbits(x, r);
             sg.put(x, nb);
             x = next_state(x, r, nb);
             esc += (k & 0xFFu) == 0xFFu;
@@ -1651,7 +1702,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
             for (long long i = top; i >= a; i--) {
                 const uint32_t k = i == lo ? k_lo : (uint32_t)__ldg(keys + i);
                 const EncRec r = rec_of(k);
-                const uint32_t nb = (x + r.dnb) >> 16;
+                const uint32_t nb = nbits(x, r);
                 rg.put(x, nb);
                 x = next_state(x, r, nb);
                 repaired++;
@@ -1712,7 +1763,8 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         auto append = [&](const uint32_t *src, uint32_t b0, uint32_t b1) {
             for (uint32_t bp = b0; bp < b1; bp += 32) {
                 const uint32_t n = min(32u, b1 - bp), j = bp >> 5, sh = bp & 31u;
-                uint32_t v = sh ? __funnelshift_r(src[j], src[j + 1], sh) : src[j];
+                const uint32_t lo = src[(size_t)j * kSpecThreads];
+                uint32_t v = sh ? __funnelshift_r(lo, src[(size_t)(j + 1) * kSpecThreads], sh) : lo;
                 if (n < 32) v &= (1u << n) - 1u;
                 acc |= (uint64_t)v << accn;
                 accn += n;
@@ -2335,7 +2387,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             FB2_CHECK_LAUNCH();
             enable_big_smem();
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
-                keys, d_segs, d_ctas, stab, stt, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
+                keys, d_segs, d_ctas, stab, stt, rhist, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
                 d_ck_off, ck_every, d_err);
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
