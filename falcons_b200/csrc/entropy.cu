@@ -1797,7 +1797,7 @@ __device__ __noinline__ uint32_t far_entry(const uint32_t *__restrict__ tb, uint
 // starting bit position, state, context and escape offset).  The CTA's parts share one table set,
 // staged in shared memory as for k_o1_decode_smem.  Each part that ends at a checkpoint checks that
 // it arrived there (state, context, bit position, escapes); a mismatch sets err[1].
-constexpr int kPartThreads = 512;
+constexpr int kPartThreads = 1024;
 __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t *__restrict__ in,
                                                                  const DecChain *__restrict__ chains,
                                                                  const uint32_t *__restrict__ pstart,

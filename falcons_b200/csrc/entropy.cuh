@@ -57,7 +57,7 @@ struct EntropyTuning {
     bool per_segment_tables = false;   // one table set per segment (the reference's choice)
     std::vector<long long> regions;    // code positions where the statistics change (level starts);
                                        // segments of one region share a table set
-    uint32_t ckpt_part = 2048;         // symbols per decode part (power of two, 0 = no checkpoints)
+    uint32_t ckpt_part = 1024;         // symbols per decode part (power of two, 0 = no checkpoints)
 };
 
 EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cudaStream_t st);
