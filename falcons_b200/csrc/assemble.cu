@@ -197,6 +197,7 @@ std::vector<uint8_t> Assembler::index_frame() const {
 }
 
 size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
+    Trace tr("assemble");
     const size_t L = pos;
     std::vector<uint8_t> hb = host;  // extra host bytes: length word, frame header, block headers
     std::vector<Piece> out;
@@ -247,6 +248,7 @@ size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
             rem -= c;
         }
     }
+    tr.mark("pieces split");
     size_t total = 8 + zstd_raw_frame_size(L);
     if (with_index) {
         const std::vector<uint8_t> idx = index_frame();
@@ -263,10 +265,13 @@ size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
         }
         total += tail_len;
     }
+    tr.mark("index frame built");
     uint8_t *dh = h2d(pool, hb, st);
     for (size_t i : host_pieces) out[i].src = dh + reinterpret_cast<uintptr_t>(out[i].src);
     launch_gather(pool, out, d_out, st);
+    tr.mark("gather launched");
     FB2_CUDA(cudaStreamSynchronize(st));
+    tr.mark("gathered");
     return total;
 }
 

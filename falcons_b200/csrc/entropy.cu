@@ -749,6 +749,7 @@ __global__ void k_pick_u64(const unsigned long long *__restrict__ src, const uns
 
 GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
                       cudaStream_t st, uint32_t ckpt_part) {
+    Trace tr("gamma");
     const int G = (int)gstart.size() - 1;
     const long long T = (long long)gstart.back();
     GammaOut out;
@@ -772,6 +773,7 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     k_pick_u64<<<grid_for(G + 1, 256), 256, 0, st>>>(boff, d_gstart, G + 1, d_gb);
     FB2_CHECK_LAUNCH();
     const std::vector<unsigned long long> gb = d2h(d_gb, (size_t)G + 1, st);
+    tr.mark("group bits known");
     std::vector<unsigned long long> gword(G);
     unsigned long long words = 0;
     for (int g = 0; g < G; g++) {
@@ -814,7 +816,9 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
                                                                          ckpt_part ? ckpt_part : 4096u, cks, recs,
                                                                          d_order);
     FB2_CHECK_LAUNCH();
+    tr.mark("class blocks launched");
     std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
+    tr.mark("class blocks coded");
     for (size_t j = 0; j < jobs.size(); j++) {
         const int g = job_group[j];
         const size_t sz = (size_t)(hs[j] & ((1ULL << 56) - 1));

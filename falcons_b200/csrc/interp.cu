@@ -718,18 +718,23 @@ void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParam
     FB2_CHECK_LAUNCH();
 }
 
-// The y pass and the x pass of one level of a field with unit x step (direction 0), fused: one
+// The y pass and the x pass of one level of a field (direction 0; any grid step), fused: one
 // CTA per (z plane, tile of kFuseR rows x kFuseW columns) stages its tile plus a halo of kFuseHalo
 // rows and columns (every rule operand lies within 3 grid units of its target) in shared memory,
 // runs the y pass (ROW: odd rows, even columns; the halo columns' targets are recomputed so that
 // the x pass can read them) and then the x pass (LINE: odd columns) on the staged tile, and
-// writes the tile back once.  Codes and escape slots go to the positions the two passes have in
-// the code stream (InterpolationDecomposition.hpp:2294-2527 visiting order).
+// writes the tile back once.  When the level's z pass precedes them (3-D), a CTA of an odd plane
+// first predicts that plane's z-pass targets (even rows, even columns of the staged tile, halo
+// included) from the four even planes around it, read from global memory (this level never
+// writes those points).  Codes and escape slots go to the positions the passes have in the code
+// stream (InterpolationDecomposition.hpp:2294-2527 visiting order).
 struct FusedYX {
     PassLaunch y;     // ROW pass along y: rows t = 1 + 2 b (b < y.B), columns at even x
     PassLaunch late;  // its last-row pass (t = n - 1), when has_late
     PassLaunch x;     // LINE pass along x: lines (z, y)
-    int has_late;
+    PassLaunch z;     // ROW pass along z: planes t = 1 + 2 b (b < z.B) at even y and x, when has_z
+    PassLaunch zlate; // its last-plane pass (t = nz - 1), when has_zlate
+    int has_late, has_z, has_zlate;
 };
 constexpr int kFuseW = 64, kFuseR = 64, kFuseHalo = 4;
 constexpr int kFusePW = kFuseW + 2 * kFuseHalo, kFusePR = kFuseR + 2 * kFuseHalo;
@@ -748,10 +753,10 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
     const int xl = max(0, x0 - H), xr = min(nx, x1 + H), TW = xr - xl;
     const int yl = max(0, y0 - H), yr = min(ny, y1 + H), TR = yr - yl;
     T *plane = xf + a * F.x.sa;
-    const long long sy = F.x.sb;
+    const long long sy = F.x.sb, sx = F.x.step;  // element steps of one grid unit in y and x
     // stage rows [yl, yr) x columns [xl, xr) (tile row r, column c: y = yl + r, x = xl + c)
     constexpr int V = 16 / sizeof(T);
-    const bool vec = ((reinterpret_cast<uintptr_t>(plane + xl) & 15) == 0) && (sy % V == 0) && (TW % V == 0);
+    const bool vec = sx == 1 && ((reinterpret_cast<uintptr_t>(plane + xl) & 15) == 0) && (sy % V == 0) && (TW % V == 0);
     if (vec) {
         const int nq = TW / V;
         for (int i = threadIdx.x; i < TR * nq; i += blockDim.x) {
@@ -765,10 +770,55 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
     } else {
         for (int i = threadIdx.x; i < TR * TW; i += blockDim.x) {
             const int rr = i / TW, cc = i - rr * TW;
-            tile[rr * P + cc] = plane[(yl + rr) * sy + xl + cc];
+            tile[rr * P + cc] = plane[(yl + rr) * sy + (xl + cc) * sx];
         }
     }
     __syncthreads();
+    // z pass of an odd plane: even rows x even columns of the staged tile
+    const bool zplane = F.has_z && (a & 1);
+    if (zplane) {
+        const int nz = F.z.n, t = (int)a;
+        const bool zl = F.has_zlate && t == nz - 1;
+        const long long sz = F.x.sa;  // element step of one plane
+        const int re0 = (yl + 1) & ~1, ce0 = (xl + 1) & ~1;
+        const int nre = (yr - re0 + 1) / 2, nce = (xr - ce0 + 1) / 2;
+        const Rule r = row_rule(true, t, nz, F.z.skip);
+        const bool inner = t >= 3 && t <= nz - 5;
+        for (int i = threadIdx.x; i < nre * nce; i += blockDim.x) {
+            const int ri = i / nce, yg = re0 + 2 * ri, xg = ce0 + 2 * (i - ri * nce);
+            const T *col = xf + (long long)yg * sy + (long long)xg * sx;  // col[z * sz] is (z, yg, xg)
+            T pred;
+            if (inner) {
+                pred = cubic_pred<T>(col[(t - 3) * sz], col[(t - 1) * sz], col[(t + 1) * sz], col[(t + 3) * sz]);
+            } else {
+                const T o0 = col[r.o0 * sz];
+                const T o1 = r.f != F_EQUAL ? col[r.o1 * sz] : o0;
+                const T o2 = r.f >= F_QUAD1 ? col[r.o2 * sz] : o0;
+                const T o3 = r.f == F_CUBIC ? col[r.o3 * sz] : o0;
+                pred = apply_formula<T>(r.f, o0, o1, o2, o3);
+            }
+            const long long ay = yg >> 1, c = xg >> 1;
+            const long long p = zl ? F.zlate.p_base + ay * F.zlate.C + c
+                                   : F.z.p_base + (ay * F.z.rows_in_group + ((t - 1) >> 1) + F.z.b_off) * F.z.C + c;
+            T *xp = tile + (yg - yl) * P + (xg - xl);
+            if (!DECOMP) {
+                const bool own = yg >= y0 && yg < y1 && xg >= x0 && xg < x1;
+                T recon;
+                const T v = *xp;
+                const int q = quantize<T>(v, pred, qp, recon);
+                if (own) codes[p] = (int16_t)q;
+                if (q == -qp.radius) {
+                    if (own) esc[p] = v;
+                } else if (!F.z.skip) {
+                    *xp = recon;
+                }
+            } else {
+                const int q = codes[p];
+                *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
+            }
+        }
+        __syncthreads();
+    }
     // y pass: odd rows of [y0, y1) x even columns of [xl, xr); thread (column tc, row group g)
     {
         constexpr int NC = kFusePW / 2, NG = kFuseThreads / NC;
@@ -849,16 +899,17 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
         }
     }
     __syncthreads();
-    // write the tile back: every row, or (compress with a final x pass) the y pass's target rows
+    // write the tile back: every row, or (compress with a final x pass, no z targets in this plane)
+    // the y pass's target rows
     {
-        const bool odd_rows = !DECOMP && F.x.skip;
+        const bool odd_rows = !DECOMP && F.x.skip && !zplane;
         constexpr int NG = kFuseThreads / kFuseW;
         static_assert(kFuseThreads % kFuseW == 0, "whole row groups");
         const int cc = threadIdx.x % kFuseW, g = threadIdx.x / kFuseW;
         const int ys = odd_rows ? 2 : 1;
         if (x0 + cc < x1)
             for (int yy = y0 + (odd_rows ? 1 : 0) + ys * g; yy < y1; yy += ys * NG)
-                plane[yy * sy + x0 + cc] = tile[(yy - yl) * P + (x0 - xl) + cc];
+                plane[yy * sy + (x0 + cc) * sx] = tile[(yy - yl) * P + (x0 - xl) + cc];
     }
 }
 
@@ -882,8 +933,9 @@ bool fusable_yx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedY
     }
     if (y.B != y.n / 2 - (F.has_late ? 1 : 0)) return false;  // the passes cover every odd row
     const PassLaunch &x = ps[j];
-    if (x.kind != KIND_LINE || !x.cubic || x.level != y.level || x.step != 1 || x.A != y.A || x.sa != y.sa ||
-        x.sb != y.step || x.B != y.n || x.C != x.n / 2 || y.sc != 2 || y.C != (x.n - 1) / 2 + 1 || y.A > 65535 ||
+    if (x.kind != KIND_LINE || !x.cubic || x.level != y.level || x.step < 1 || x.A != y.A || x.sa != y.sa ||
+        x.sb != y.step || x.B != y.n || x.C != x.n / 2 || y.sc != 2 * x.step || y.C != (x.n - 1) / 2 + 1 ||
+        y.A > 65535 ||
         x.n < 2 || y.n < 2)
         return false;
     (void)elem;
@@ -901,14 +953,45 @@ void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QPara
     FB2_CHECK_LAUNCH();
 }
 
-// Runs the plan's passes in order, the fusable y + x pairs as one kernel.
+// Whether passes i (and i + 1) are the z pass that precedes the fusable y + x passes starting
+// right after it; fills F (z, zlate, y, late, x) and `used` (all of them).
+bool fusable_zyx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedYX &F, size_t &used) {
+    if (i >= ps.size()) return false;
+    const PassLaunch &z = ps[i];
+    if (z.kind != KIND_ROW || !z.cubic || z.skip || z.t0 != 1 || z.b_off != 0 || z.B != z.rows_in_group) return false;
+    size_t j = i + 1, u = 0;
+    PassLaunch zl{};
+    int has_zl = 0;
+    if (j < ps.size() && ps[j].kind == KIND_ROW && ps[j].t0 == z.n - 1 && ps[j].B == 1 && ps[j].rows_in_group == 1 &&
+        ps[j].p_base == z.p_base + z.A * z.B * z.C) {
+        zl = ps[j];
+        if (zl.b_off != 0 || zl.A != z.A || zl.C != z.C || zl.sa != z.sa || zl.sc != z.sc || zl.step != z.step ||
+            zl.level != z.level || zl.n != z.n || zl.skip != z.skip)
+            return false;
+        has_zl = 1;
+        j++;
+    }
+    if (z.B != z.n / 2 - has_zl) return false;
+    if (!fusable_yx(ps, j, elem, F, u)) return false;
+    if (z.level != F.y.level || z.n != F.y.A || z.step != F.y.sa || z.A != (F.y.n - 1) / 2 + 1 ||
+        z.sa != 2 * F.y.step || z.C != (F.x.n - 1) / 2 + 1 || z.sc != 2 * F.x.step || z.n < 2)
+        return false;
+    F.z = z;
+    F.zlate = zl;
+    F.has_z = 1;
+    F.has_zlate = has_zl;
+    used = j - i + u;
+    return true;
+}
+
+// Runs the plan's passes in order, the fusable z + y + x and y + x passes as one kernel.
 template <class T, bool DECOMP>
 void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, cudaStream_t st) {
     const std::vector<PassLaunch> &ps = plan.passes;
     for (size_t i = 0; i < ps.size();) {
-        FusedYX F;
+        FusedYX F{};
         size_t used = 0;
-        if (fusable_yx(ps, i, sizeof(T), F, used)) {
+        if (fusable_zyx(ps, i, sizeof(T), F, used) || fusable_yx(ps, i, sizeof(T), F, used)) {
             launch_fused_yx<T, DECOMP>(F, x, codes, esc, plan.levels[F.y.level], st);
             i += used;
         } else {

@@ -166,6 +166,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st, tune);
             tr.mark("entropy stage launched");
             if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
+            tr.mark("framed size checked");
             payload = as.run_framed(pool, d_pay, st);
             tr.mark("payload assembled");
             c.cmprAlgo = ALGO_INTERP;
