@@ -1871,12 +1871,26 @@ __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t 
     }
     const unsigned long long avail = n_ovf > ch.ovf + oi0 ? n_ovf - ch.ovf - oi0 : 0;
     const uint32_t nov = (uint32_t)min((unsigned long long)(ch.nesc - oi0), avail);
-    const int16_t *__restrict__ ov = ovf + ch.ovf + oi0;
     int16_t *o = out + ch.lo + start;
     const unsigned long long map = w.map;
     uint32_t oi = 0;
-    int q0 = nov > 0 ? (int)__ldg(ov) : 0;
-    int q1 = nov > 1 ? (int)__ldg(ov + 1) : 0;
+    // Escape values come in 16-byte chunks of eight (ovf is 16-byte aligned, with slack behind
+    // it); the chunk after the current one is loaded a whole chunk ahead, so that taking the next
+    // value never waits on memory.
+    const uint4 *ov4 = reinterpret_cast<const uint4 *>(ovf);
+    const long long eb = (long long)(ch.ovf + oi0);
+    long long ec = eb >> 3;
+    int ek = (int)(eb & 7);
+    auto echunk = [&](long long c) -> uint4 {
+        return (unsigned long long)(c << 3) < n_ovf ? __ldg(ov4 + c) : make_uint4(0, 0, 0, 0);
+    };
+    auto ext = [](const uint4 &u, int k) -> int {
+        const uint32_t wd = k < 4 ? (k < 2 ? u.x : u.y) : (k < 6 ? u.z : u.w);
+        return (int)(int16_t)(k & 1 ? wd >> 16 : wd & 0xFFFFu);
+    };
+    uint4 ecur = nov > 0 ? echunk(ec) : make_uint4(0, 0, 0, 0);
+    uint4 enxt = nov > 0 ? echunk(ec + 1) : make_uint4(0, 0, 0, 0);
+    int q0 = nov > 0 ? ext(ecur, ek) : 0;
     auto step = [&]() -> int {
         const uint32_t sl = (uint32_t)(map >> (4 * ctx)) & 15u;
         uint32_t e;
@@ -1887,8 +1901,13 @@ __global__ void __launch_bounds__(kPartThreads) k_o1_decode_parts(const uint8_t 
         ctx = esc ? 13u + (uint32_t)(code < 0) : ((e >> 17) & 15u);
         if (esc) {
             oi++;
-            q0 = q1;
-            q1 = oi + 1 < nov ? (int)__ldg(ov + oi + 1) : 0;
+            if (++ek == 8) {
+                ecur = enxt;
+                ec++;
+                enxt = echunk(ec + 1);
+                ek = 0;
+            }
+            q0 = oi < nov ? ext(ecur, ek) : 0;
         }
         state = (e & 0x1FFFu) + br.read((e >> 13) & 15u);
         return code;
@@ -2056,11 +2075,17 @@ __global__ void k_table_same(const uint8_t *__restrict__ in, const unsigned long
 // Escape (|code| >= 128) extraction in index order: tile count + scan + scatter of zz+1 values.
 __global__ void __launch_bounds__(kScanThreads) k_esc_tiles(const int16_t *__restrict__ q, long long n,
                                                            uint32_t *__restrict__ cnt) {
-    const long long base = (long long)blockIdx.x * kScanTile;
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     uint32_t c = 0;
-    for (int j = 0; j < kScanItems; j++) {
-        const long long i = base + (long long)j * kScanThreads + threadIdx.x;
-        if (i < n && o1_sym(q[i]) == O1_NSYM - 1) c++;
+    if (base + kScanItems <= n) {  // 32-byte aligned (the code arrays are 256-byte aligned)
+        const int4 *p4 = reinterpret_cast<const int4 *>(q + base);
+        const int4 a = __ldg(p4), b = __ldg(p4 + 1);
+        const int32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int j = 0; j < kScanItems; j++)
+            c += o1_sym((int16_t)(j & 1 ? w[j >> 1] >> 16 : w[j >> 1] & 0xFFFF)) == O1_NSYM - 1;
+    } else {
+        for (long long i = base; i < n && i < base + kScanItems; i++) c += o1_sym(q[i]) == O1_NSYM - 1;
     }
     __shared__ uint32_t sh[32];
     uint32_t tot;
@@ -2074,23 +2099,34 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_extract(const int16_t *__r
     const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     int16_t v[kScanItems];
     uint32_t c = 0;
+    static_assert(kScanItems == 16, "two 16-byte vectors per thread");
+    if (base + kScanItems <= n) {  // 32-byte aligned (the code arrays are 256-byte aligned)
+        const int4 *p4 = reinterpret_cast<const int4 *>(q + base);
+        const int4 a = __ldg(p4), b = __ldg(p4 + 1);
+        const int32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-        const long long i = base + j;
-        v[j] = i < n ? q[i] : (int16_t)0;
-        c += (i < n && o1_sym(v[j]) == O1_NSYM - 1);
+        for (int j = 0; j < kScanItems; j++) v[j] = (int16_t)(j & 1 ? w[j >> 1] >> 16 : w[j >> 1] & 0xFFFF);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kScanItems; j++) v[j] = base + j < n ? q[base + j] : (int16_t)0;
     }
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) c += (base + j < n && o1_sym(v[j]) == O1_NSYM - 1);
     __shared__ uint32_t sh[32];
+    // the tile's escapes are staged in shared memory in order, then leave as contiguous runs
+    __shared__ int16_t sv[kScanTile];
     uint32_t tot;
-    uint32_t r = block_excl_scan<uint32_t>(c, sh, tot) + tile_off[blockIdx.x];
+    uint32_t r = block_excl_scan<uint32_t>(c, sh, tot);
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
-        const long long i = base + j;
-        if (i < n && o1_sym(v[j]) == O1_NSYM - 1) {
-            vals[r] = zigzag((int)v[j]) + 1u;
-            raw[r] = v[j];
-            r++;
-        }
+        if (base + j < n && o1_sym(v[j]) == O1_NSYM - 1) sv[r++] = v[j];
+    }
+    __syncthreads();
+    const uint32_t t0 = tile_off[blockIdx.x];
+    for (uint32_t k = threadIdx.x; k < tot; k += blockDim.x) {
+        const int16_t e = sv[k];
+        vals[t0 + k] = zigzag((int)e) + 1u;
+        raw[t0 + k] = e;
     }
 }
 

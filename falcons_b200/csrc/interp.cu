@@ -487,13 +487,24 @@ __global__ void __launch_bounds__(1024) k_scan_u32(const unsigned *__restrict__ 
     __syncthreads();
     for (long long base = 0; base < n; base += 1024LL * kScanRun) {
         const long long i0 = base + (long long)threadIdx.x * kScanRun;
+        const bool whole = i0 + kScanRun <= n;  // 16-byte vectors (both arrays are 256-byte aligned)
         unsigned v[kScanRun];
         unsigned long long sum = 0;
+        if (whole) {
 #pragma unroll
-        for (int j = 0; j < kScanRun; j++) {
-            v[j] = i0 + j < n ? __ldg(in + i0 + j) : 0u;
-            sum += v[j];
+            for (int j = 0; j < kScanRun / 4; j++) {
+                const uint4 u = __ldg(reinterpret_cast<const uint4 *>(in + i0) + j);
+                v[4 * j] = u.x;
+                v[4 * j + 1] = u.y;
+                v[4 * j + 2] = u.z;
+                v[4 * j + 3] = u.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kScanRun; j++) v[j] = i0 + j < n ? __ldg(in + i0 + j) : 0u;
         }
+#pragma unroll
+        for (int j = 0; j < kScanRun; j++) sum += v[j];
         // inclusive warp scan of the run sums, then across warps
         unsigned long long s = sum;
 #pragma unroll
@@ -515,10 +526,19 @@ __global__ void __launch_bounds__(1024) k_scan_u32(const unsigned *__restrict__ 
         __syncthreads();
         const unsigned long long wprev = (threadIdx.x >> 5) ? warp_sums[(threadIdx.x >> 5) - 1] : 0;
         unsigned long long e = carry + wprev + s - sum;
+        if (whole) {
 #pragma unroll
-        for (int j = 0; j < kScanRun; j++) {
-            if (i0 + j < n) out[i0 + j] = e;
-            e += v[j];
+            for (int j = 0; j < kScanRun; j += 2) {
+                const unsigned long long e1 = e + v[j];
+                reinterpret_cast<ulonglong2 *>(out + i0)[j / 2] = make_ulonglong2(e, e1);
+                e = e1 + v[j + 1];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kScanRun; j++) {
+                if (i0 + j < n) out[i0 + j] = e;
+                e += v[j];
+            }
         }
         __syncthreads();
         if (threadIdx.x == 1023) carry += wprev + s;
