@@ -1080,7 +1080,8 @@ struct SegInfo {
 };
 
 __global__ void __launch_bounds__(1024) k_o1_hist(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
-                                                 uint32_t *__restrict__ hist, uint32_t *__restrict__ nvk) {
+                                                 uint32_t *__restrict__ hist, uint32_t *__restrict__ nvk,
+                                                 uint16_t *__restrict__ keys) {
     __shared__ uint32_t h[O1_NCTX * O1_NSYM];
     __shared__ uint32_t esc[kMaxK];
     const SegInfo sg = segs[blockIdx.x];
@@ -1098,7 +1099,9 @@ __global__ void __launch_bounds__(1024) k_o1_hist(const int16_t *__restrict__ q,
                 const unsigned long long i = sg.lo + r;
                 const int prev = r == c0 ? 0 : (int)q[i - 1];
                 const int s = o1_sym((int)q[i]);
-                atomicAdd(&h[o1_ctx(prev) * O1_NSYM + s], 1u);
+                const int c = o1_ctx(prev);
+                atomicAdd(&h[c * O1_NSYM + s], 1u);
+                keys[i] = (uint16_t)((c << 8) | s);
                 ne += s == O1_NSYM - 1;
             }
         }
@@ -1453,13 +1456,8 @@ struct SpecCta {
 // Staging words of one part: 13 bits per code at most, plus the final state and end mark.
 __host__ __device__ __forceinline__ size_t spec_stage_words(uint32_t part) { return ((size_t)part * 13 + 64) / 32 + 4; }
 
-// keys[i] = context of code i-1 (8 bits) | symbol of code i (8 bits)
-__global__ void k_o1_keys(const int16_t *__restrict__ q, long long n, uint16_t *__restrict__ keys) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int prev = i > 0 ? (int)q[i - 1] : 0;
-        keys[i] = (uint16_t)((o1_ctx(prev) << 8) | o1_sym((int)q[i]));
-    }
-}
+// keys[i] = context of code i (from code i-1; 0 at a chain's first code) << 8 | symbol of code i,
+// written by k_o1_hist.
 
 // Calls f(i, keys[i]) for i = top down to bottom, reading the keys through aligned 16-byte vectors
 // (8 keys) fetched two vectors ahead.
@@ -2358,7 +2356,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         unsigned long long *d_ck_off = o1ck ? h2d(pool, ck_off, st) : nullptr;
         uint32_t *hist = pool.get<uint32_t>((size_t)S * O1_NCTX * O1_NSYM);
         uint32_t *nvk = pool.get<uint32_t>((size_t)S * kMaxK);
-        k_o1_hist<<<(unsigned)S, 1024, 0, st>>>(q, d_segs, hist, nvk);
+        uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
+        k_o1_hist<<<(unsigned)S, 1024, 0, st>>>(q, d_segs, hist, nvk, keys);
         FB2_CHECK_LAUNCH();
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
@@ -2418,13 +2417,10 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             std::vector<SpecCta> ctas;
             for (const ChainCta &c : groups) ctas.push_back(SpecCta{c.table, c.first, c.count, ppc, c.map, c.rev});
             SpecCta *d_ctas = h2d(pool, ctas, st);
-            uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
             uint16_t *sparse = pool.get<uint16_t>(((size_t)N >> kSparseShift) + 2);
             uint16_t *sparse_bits = pool.get<uint16_t>(((size_t)N >> kSparseShift) + 2);
             uint32_t *stage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
             uint32_t *rstage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
-            k_o1_keys<<<grid_for(N, 256, 148 * 16), 256, 0, st>>>(q, N, keys);
-            FB2_CHECK_LAUNCH();
             enable_big_smem();
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
                 keys, d_segs, d_ctas, stab, stt, rhist, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
