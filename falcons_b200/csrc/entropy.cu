@@ -721,15 +721,22 @@ __device__ __forceinline__ int find_group(const unsigned long long *gstart, int 
 }
 
 // MSB-first packing of k low bits of each value into word-aligned per-group regions (zeroed).
-__global__ void k_gamma_pack(const uint32_t *__restrict__ v, const uint8_t *__restrict__ cls,
-                             const unsigned long long *__restrict__ boff, long long n,
-                             const unsigned long long *__restrict__ gstart, int G,
-                             const unsigned long long *__restrict__ gword, uint32_t *__restrict__ words) {
+__global__ void __launch_bounds__(256) k_gamma_pack(const uint32_t *__restrict__ v, const uint8_t *__restrict__ cls,
+                                                    const unsigned long long *__restrict__ boff, long long n,
+                                                    const unsigned long long *__restrict__ gstart, int G,
+                                                    const unsigned long long *__restrict__ gword,
+                                                    uint32_t *__restrict__ words) {
+    __shared__ unsigned long long s_gs[1025];  // the group starts, when there are few groups
+    const bool in_smem = G + 1 <= 1025;
+    if (in_smem)
+        for (int g = threadIdx.x; g <= G; g += blockDim.x) s_gs[g] = gstart[g];
+    __syncthreads();
+    const unsigned long long *gs = in_smem ? s_gs : gstart;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int k = cls[i];
         if (k == 0) continue;
-        const int g = find_group(gstart, G, (unsigned long long)i);
-        const unsigned long long b = boff[i] - boff[gstart[g]];
+        const int g = find_group(gs, G, (unsigned long long)i);
+        const unsigned long long b = boff[i] - boff[gs[g]];
         const uint32_t m = v[i] & ((1u << k) - 1u);
         const unsigned long long w = gword[g] + (b >> 5);
         const int o = (int)(b & 31);
@@ -785,7 +792,7 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     uint32_t *wbuf = pool.get<uint32_t>(words + 4);
     FB2_CUDA(cudaMemsetAsync(wbuf, 0, (words + 4) * 4, st));
     unsigned long long *d_gword = h2d(pool, gword, st);
-    k_gamma_pack<<<grid_for(T, 256), 256, 0, st>>>(d_vals, cls, boff, T, d_gstart, G, d_gword, wbuf);
+    k_gamma_pack<<<grid_for(T, 256, 148 * 8), 256, 0, st>>>(d_vals, cls, boff, T, d_gstart, G, d_gword, wbuf);
     FB2_CHECK_LAUNCH();
     for (int g = 0; g < G; g++) out.man_ptr[g] = reinterpret_cast<const uint8_t *>(wbuf + gword[g]);
     // FSE class blocks
@@ -881,37 +888,59 @@ void add_class_pieces(Assembler &as, const GammaOut &go, int g, CkptCollector *c
     }
 }
 
-__global__ void k_gamma_unpack(const uint8_t *__restrict__ cls, const unsigned long long *__restrict__ boff,
-                               long long n, const unsigned long long *__restrict__ gstart, int G,
-                               const unsigned long long *__restrict__ gman, const uint8_t *__restrict__ base,
-                               const unsigned long long *__restrict__ gman_len, uint32_t *__restrict__ v,
-                               int *__restrict__ err, const unsigned long long *__restrict__ gdst,
-                               int16_t *__restrict__ ovf) {
+// Gamma decode of n values in index order: value i = (1 << k) | k mantissa bits (MSB first, at
+// the group's running bit offset boff), k = cls[i].  The group starts (and, when there are few
+// groups, the group tables) sit in shared memory; the mantissa bits come from at most two
+// aligned words.
+constexpr int kUnpackGroupsSmem = 1024;
+__global__ void __launch_bounds__(256) k_gamma_unpack(const uint8_t *__restrict__ cls,
+                                                      const unsigned long long *__restrict__ boff, long long n,
+                                                      const unsigned long long *__restrict__ gstart, int G,
+                                                      const unsigned long long *__restrict__ gman,
+                                                      const uint8_t *__restrict__ base,
+                                                      const unsigned long long *__restrict__ gman_len,
+                                                      uint32_t *__restrict__ v, int *__restrict__ err,
+                                                      const unsigned long long *__restrict__ gdst,
+                                                      int16_t *__restrict__ ovf) {
+    __shared__ unsigned long long s_gs[kUnpackGroupsSmem + 1];
+    const bool in_smem = G + 1 <= kUnpackGroupsSmem;
+    if (in_smem)
+        for (int g = threadIdx.x; g <= G; g += blockDim.x) s_gs[g] = gstart[g];
+    __syncthreads();
+    const unsigned long long *gs = in_smem ? s_gs : gstart;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int k = cls[i];
+        // the last group whose start is at or before i
+        int lo = 0, hi = G - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (gs[mid] <= (unsigned long long)i) lo = mid;
+            else hi = mid - 1;
+        }
+        const int g = lo;
         uint32_t m = 0;
         if (k > 31) {
             atomicExch(err, 2);
         } else if (k > 0) {
-            const int g = find_group(gstart, G, (unsigned long long)i);
-            const unsigned long long b = boff[i] - boff[gstart[g]];
-            const uint8_t *p = base + gman[g];
-            const unsigned long long lenb = gman_len[g];
-            const unsigned long long byte0 = b >> 3;
-            if (((b + k + 7) >> 3) > lenb) {
+            const unsigned long long bb = boff[i] - boff[gs[g]];
+            const unsigned long long byte0 = bb >> 3;
+            if (((bb + k + 7) >> 3) > gman_len[g]) {
                 atomicExch(err, 3);
             } else {
-                unsigned long long acc = 0;
-                const int nbytes = (int)((((b & 7) + k) + 7) >> 3);
-                for (int j = 0; j < nbytes; j++) acc = (acc << 8) | p[byte0 + j];
-                const int drop = nbytes * 8 - (int)(b & 7) - k;
-                m = (uint32_t)((acc >> drop) & ((1ull << k) - 1));
+                const uintptr_t a = reinterpret_cast<uintptr_t>(base + gman[g] + byte0);
+                const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+                const unsigned lead = (unsigned)(a & 3);                 // bytes before the first one
+                const unsigned need = lead + (unsigned)((((bb & 7) + k) + 7) >> 3);  // bytes from w[0]
+                const uint32_t w0 = __byte_perm(w[0], 0, 0x0123);
+                const uint32_t w1 = need > 4 ? __byte_perm(w[1], 0, 0x0123) : 0u;
+                const unsigned long long be = ((unsigned long long)w0 << 32) | w1;  // big-endian bytes
+                const unsigned off = lead * 8 + (unsigned)(bb & 7);
+                m = (uint32_t)((be << off) >> (64 - k));
             }
         }
         const uint32_t val = (k <= 31) ? ((1u << k) | m) : 0u;
         if (ovf) {  // escape values: zigzag + 1 gamma-coded, written in place as int16
-            const int g = find_group(gstart, G, (unsigned long long)i);
-            ovf[gdst[g] + ((unsigned long long)i - gstart[g])] = (int16_t)unzz(val - 1u);
+            ovf[gdst[g] + ((unsigned long long)i - gs[g])] = (int16_t)unzz(val - 1u);
         } else {
             v[i] = val;
         }
@@ -2185,7 +2214,7 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     unsigned long long *d_gstart = h2d(pool, gstart, st);
     unsigned long long *d_gman = h2d(pool, gman, st);
     unsigned long long *d_glen = h2d(pool, glen, st);
-    k_gamma_unpack<<<grid_for(T, 256), 256, 0, st>>>(cls, boff, T, d_gstart, G, d_gman, d, d_glen, d_vals, d_err,
+    k_gamma_unpack<<<grid_for(T, 256, 148 * 8), 256, 0, st>>>(cls, boff, T, d_gstart, G, d_gman, d, d_glen, d_vals, d_err,
                                                     d_gdst, d_ovf);
     FB2_CHECK_LAUNCH();
 }
