@@ -173,11 +173,27 @@ size_t Assembler::index_frame_size() const {
 }
 
 std::vector<uint8_t> Assembler::index_frame() const {
-    std::vector<std::pair<unsigned long long, std::pair<const uint8_t *, size_t>>> e;
-    for (auto &r : host_refs) e.push_back({pieces[r.first].dst, {host.data() + r.second, (size_t)pieces[r.first].len}});
-    for (auto &sh : shadows) e.push_back({sh.first, {sh.second.data(), sh.second.size()}});
-    std::sort(e.begin(), e.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
-    std::vector<uint8_t> c(16);
+    // host pieces and shadows are each recorded in offset order: merge them
+    using Entry = std::pair<unsigned long long, std::pair<const uint8_t *, size_t>>;
+    std::vector<Entry> e1, e2, e;
+    e1.reserve(host_refs.size());
+    e2.reserve(shadows.size());
+    for (auto &r : host_refs) e1.push_back({pieces[r.first].dst, {host.data() + r.second, (size_t)pieces[r.first].len}});
+    for (auto &sh : shadows) e2.push_back({sh.first, {sh.second.data(), sh.second.size()}});
+    e.resize(e1.size() + e2.size());
+    auto less = [](const Entry &a, const Entry &b) { return a.first < b.first; };
+    if (std::is_sorted(e1.begin(), e1.end(), less) && std::is_sorted(e2.begin(), e2.end(), less)) {
+        std::merge(e1.begin(), e1.end(), e2.begin(), e2.end(), e.begin(), less);
+    } else {
+        std::copy(e1.begin(), e1.end(), e.begin());
+        std::copy(e2.begin(), e2.end(), e.begin() + (long)e1.size());
+        std::stable_sort(e.begin(), e.end(), less);
+    }
+    size_t total = 16;
+    for (auto &x : e) total += 12 + x.second.second;
+    std::vector<uint8_t> c;
+    c.reserve(total);
+    c.resize(16);
     const uint32_t magic = kSkippableMagic, tag = kIndexTag, count = (uint32_t)e.size();
     memcpy(c.data() + 8, &tag, 4);
     memcpy(c.data() + 12, &count, 4);
@@ -199,8 +215,11 @@ std::vector<uint8_t> Assembler::index_frame() const {
 size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
     Trace tr("assemble");
     const size_t L = pos;
-    std::vector<uint8_t> hb = host;  // extra host bytes: length word, frame header, block headers
+    std::vector<uint8_t> hb;  // the host bytes, then the length word, frame header, block headers
+    hb.reserve(host.size() + 64 + 3 * (pos / kZstdBlock + 2) + (with_index ? index_frame_size() + tail_host.size() : 0));
+    hb.insert(hb.end(), host.begin(), host.end());
     std::vector<Piece> out;
+    out.reserve(pieces.size() + pieces.size() / 4 + pos / kZstdBlock + tail.size() + 16);
     auto add_host = [&](const uint8_t *b, size_t n, unsigned long long dst) {
         const size_t off = hb.size();
         hb.insert(hb.end(), b, b + n);

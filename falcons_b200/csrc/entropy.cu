@@ -512,13 +512,15 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
     }
 }
 
-// One warp per 64 Ki block: lane 0 reads the table header and builds the decode table in shared
-// memory (zfse/fse_decompress.c FSE_buildDTable), then the block decodes either as one sequence
-// (lane 0, two interleaved states, FSE_decompress_usingDTable_generic) or, when the stream carries
-// checkpoints for it, as independent parts of `part` symbols, one per lane, each starting from its
-// checkpoint and verified against the next one (a mismatch sets err[1] and the caller decodes again
-// without checkpoints).
-__global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restrict__ in,
+// One CTA of kFseDecThreads per 64 Ki block: thread 0 reads the table header, the first warp
+// builds the decode table in shared memory (zfse/fse_decompress.c FSE_buildDTable), then the block
+// decodes either as one sequence (thread 0, two interleaved states,
+// FSE_decompress_usingDTable_generic) or, when the stream carries checkpoints for it, as
+// independent parts of `part` symbols, one per thread, each starting from its checkpoint and
+// verified against the next one (a mismatch sets err[1] and the caller decodes again without
+// checkpoints).
+constexpr int kFseDecThreads = 64;  // parts of a block decode one per thread
+__global__ void __launch_bounds__(kFseDecThreads) k_fse_decode_blocks(const uint8_t *__restrict__ in,
                                                          const BlockJob *__restrict__ jobs,
                                                          uint8_t *__restrict__ cls, int *__restrict__ err,
                                                          uint32_t part, const FseCkpt *__restrict__ cks) {
@@ -527,6 +529,8 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
     __shared__ int16_t s_norm[256];
     __shared__ uint32_t s_scan[257], s_next[256];
     __shared__ unsigned tl_sh, hdr_sh, maxsv_sh, high_sh;
+    extern __shared__ uint4 s_out4[];  // the block's symbols (FBLK bytes), copied out at the end
+    uint8_t *s_out = reinterpret_cast<uint8_t *>(s_out4);
     const BlockJob jb = jobs[blockIdx.x];
     uint8_t *dst = cls + jb.src;
     const uint8_t *p = in + jb.in;
@@ -566,10 +570,10 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
         maxsv_sh = maxSV;
         if (!ok) atomicExch(err, 1);
     }
-    __syncwarp();
+    __syncthreads();
     const unsigned tl = tl_sh;
     if (tl == 0xFFFFFFFFu) return;
-    {
+    if (threadIdx.x < 32) {  // the table, by the first warp
         const unsigned lane = threadIdx.x, L = 1u << tl, maxSV = maxsv_sh;
         const uint32_t step = fse::table_step(L), mask = L - 1, high = high_sh;
         const unsigned per = (L + 31) / 32, j0 = min(L, lane * per), j1 = min(L, j0 + per);
@@ -614,6 +618,7 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
             __syncwarp();
         }
     }
+    __syncthreads();
     const uint8_t *sp = p + hdr_sh;
     const uint32_t ssz = (uint32_t)(size - hdr_sh);
     const unsigned n = jb.n;
@@ -644,17 +649,21 @@ __global__ void __launch_bounds__(32) k_fse_decode_blocks(const uint8_t *__restr
         for (; i + 1 < end; i += 2) {
             const fse::DEntry e0 = dt[s0];
             const fse::DEntry e1 = dt[s1];
-            dst[i] = e0.symbol;
-            dst[i + 1] = e1.symbol;
+            s_out[i] = e0.symbol;
+            s_out[i + 1] = e1.symbol;
             s0 = e0.newState + br.read(e0.nbBits);
             s1 = e1.newState + br.read(e1.nbBits);
         }
-        if (i < end) dst[i] = dt[s0].symbol;
+        if (i < end) s_out[i] = dt[s0].symbol;
         if (q + 1 < nparts) {
             const FseCkpt c = cks[jb.ck + q];
             if (c.s0 != s0 || c.s1 != s1 || br.pos != br.start_bit(sp) + (int32_t)c.bitpos) atomicExch(err + 1, 1);
         }
     }
+    // the symbols leave in consecutive bytes across the CTA (each thread's part decoded into
+    // shared memory, so that no warp store scatters over the parts)
+    __syncthreads();
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) dst[i] = s_out[i];
 }
 
 // Walks an fse_enc record sequence (host bytes) for n symbols starting at `off`; appends jobs.
@@ -2201,7 +2210,8 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     }
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
-    k_fse_decode_blocks<<<(unsigned)jobs.size(), 32, 0, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, FBLK));
+    k_fse_decode_blocks<<<(unsigned)jobs.size(), kFseDecThreads, FBLK, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
     FB2_CHECK_LAUNCH();
     unsigned long long *boff = pool.get<unsigned long long>(T + 1);
     void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
@@ -2494,11 +2504,16 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         for (auto b : h_blen)
             if (b == ~0ULL) throw std::runtime_error("tANS chain overflow");
         as.val<uint64_t>((uint64_t)S);
+        as.host.reserve(as.host.size() + (size_t)S * (16 + 16 * K + 32));
+        as.pieces.reserve(as.pieces.size() + (size_t)S * (K + 8) + 64);
         for (long long g = 0; g < S; g++) {
-            as.val<uint64_t>(segs[g].n);
-            as.val<uint64_t>((uint64_t)K);
-            for (int k = 0; k < K; k++) as.val<uint64_t>(h_blen[g * kMaxK + k]);
-            for (int k = 0; k < K; k++) as.val<uint64_t>(h_nvk[g * kMaxK + k]);
+            // the segment's header words (N, K, chain lengths, escape counts) in one piece
+            uint64_t hw[2 + 2 * kMaxK];
+            hw[0] = segs[g].n;
+            hw[1] = (uint64_t)K;
+            for (int k = 0; k < K; k++) hw[2 + k] = h_blen[g * kMaxK + k];
+            for (int k = 0; k < K; k++) hw[2 + K + k] = h_nvk[g * kMaxK + k];
+            as.bytes(hw, (size_t)(2 + 2 * K) * 8);
             as.dev(nf + (size_t)seg_region[g] * O1_NCTX * O1_NSYM, O1_NCTX * O1_NSYM * 2);
             for (int k = 0; k < K; k++) as.dev(slots + soff[g * kMaxK + k], h_blen[g * kMaxK + k]);
             const unsigned long long ne = gstart[g + 1] - gstart[g];
