@@ -761,7 +761,7 @@ constexpr int kFusePW = kFuseW + 2 * kFuseHalo, kFusePR = kFuseR + 2 * kFuseHalo
 constexpr int kFuseThreads = 256;
 
 template <class T, bool DECOMP>
-__global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *__restrict__ xf,
+__global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fused(const FusedYX F, T *__restrict__ xf,
                                                            int16_t *__restrict__ codes, T *__restrict__ esc,
                                                            const QParams qp) {
     __shared__ __align__(16) T tile[kFusePR * kFusePW];
@@ -778,13 +778,16 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
     constexpr int V = 16 / sizeof(T);
     const bool vec = sx == 1 && ((reinterpret_cast<uintptr_t>(plane + xl) & 15) == 0) && (sy % V == 0) && (TW % V == 0);
     if (vec) {
-        const int nq = TW / V;
-        for (int i = threadIdx.x; i < TR * nq; i += blockDim.x) {
-            const int rr = i / nq, qq = i - rr * nq;
-            const unsigned sa = (unsigned)__cvta_generic_to_shared(tile + rr * P + qq * V);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
-                         "l"(plane + (yl + rr) * sy + xl + qq * V)
-                         : "memory");
+        // thread (vector slot qq of a row, row group); kFusePW / V slots per row at most
+        constexpr int NQ = kFusePW / V, NG = kFuseThreads / NQ;
+        const int nq = TW / V, qq = threadIdx.x % NQ, g = threadIdx.x / NQ;
+        if (qq < nq && g < NG) {
+            const T *src = plane + (long long)(yl + g) * sy + xl + qq * V;
+            T *dstp = tile + g * P + qq * V;
+            for (int rr = g; rr < TR; rr += NG, src += NG * sy, dstp += NG * P) {
+                const unsigned sa = (unsigned)__cvta_generic_to_shared(dstp);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
+            }
         }
         asm volatile("cp.async.wait_all;\n" ::: "memory");
     } else {
@@ -804,8 +807,10 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
         const int nre = (yr - re0 + 1) / 2, nce = (xr - ce0 + 1) / 2;
         const Rule r = row_rule(true, t, nz, F.z.skip);
         const bool inner = t >= 3 && t <= nz - 5;
-        for (int i = threadIdx.x; i < nre * nce; i += blockDim.x) {
-            const int ri = i / nce, yg = re0 + 2 * ri, xg = ce0 + 2 * (i - ri * nce);
+        constexpr int NCZ = kFusePW / 2, NGZ = kFuseThreads / NCZ;  // thread (column, row group)
+        const int czi = threadIdx.x % NCZ, gz = threadIdx.x / NCZ;
+        for (int ri = gz; ri < nre && czi < nce && gz < NGZ; ri += NGZ) {
+            const int yg = re0 + 2 * ri, xg = ce0 + 2 * czi;
             const T *col = xf + (long long)yg * sy + (long long)xg * sx;  // col[z * sz] is (z, yg, xg)
             T pred;
             if (inner) {
@@ -845,6 +850,9 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
         const int ce0 = (xl + 1) & ~1;
         const int tc = threadIdx.x % NC, g = threadIdx.x / NC;
         const int xg = ce0 + 2 * tc;
+        // code position of (row t, column xg): main rows p0 + ((t - 1) / 2 - y0 / 2) * C
+        const long long c = xg >> 1;
+        const long long p0 = F.y.p_base + ((long long)a * F.y.rows_in_group + (y0 >> 1) + F.y.b_off) * F.y.C + c;
         for (int tr = g; tr < kFuseR / 2 && g < NG && xg < xr; tr += NG) {
             const int t = y0 + 1 + 2 * tr;
             if (t >= y1) break;
@@ -861,9 +869,7 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
                 const T o3 = r.f == F_CUBIC ? col[r.o3 * P] : o0;
                 pred = apply_formula<T>(r.f, o0, o1, o2, o3);
             }
-            const long long c = xg >> 1;
-            const long long p = late ? F.late.p_base + a * F.late.C + c
-                                     : F.y.p_base + (a * F.y.rows_in_group + ((t - 1) >> 1) + F.y.b_off) * F.y.C + c;
+            const long long p = late ? F.late.p_base + a * F.late.C + c : p0 + (long long)tr * F.y.C;
             T *xp = tile + (t - yl) * P + (xg - xl);
             if (!DECOMP) {
                 const bool own = xg >= x0 && xg < x1;
@@ -890,6 +896,7 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
         const int odd = nx / 2, tlo = 3, thi = 2 * odd - 5;
         const int k = threadIdx.x % NO, g = threadIdx.x / NO;
         const int t = x0 + 1 + 2 * k;
+        const long long px0 = F.x.p_base + ((long long)a * F.x.B + y0) * F.x.C + ((t - 1) >> 1);
         for (int yy = y0 + g; yy < y1 && t < x1; yy += NG) {
             const T *row = tile + (yy - yl) * P - xl;  // row[x]
             T pred;
@@ -903,7 +910,7 @@ __global__ void __launch_bounds__(kFuseThreads) k_yx_fused(const FusedYX F, T *_
                 const T o3 = r.f == F_CUBIC ? row[r.o3] : o0;
                 pred = apply_formula<T>(r.f, o0, o1, o2, o3);
             }
-            const long long p = F.x.p_base + (a * F.x.B + yy) * F.x.C + ((t - 1) >> 1);
+            const long long p = px0 + (long long)(yy - y0) * F.x.C;
             T *xp = tile + (yy - yl) * P + (t - xl);
             if (!DECOMP) {
                 T recon;
