@@ -92,23 +92,26 @@ __host__ __device__ __forceinline__ uint32_t fse_ckpt_count(uint32_t n, uint32_t
 // header; the CTA builds the coding tables in shared memory (the state table with warp match
 // ranks, the symbol transforms per symbol, and, where it fits, the next-state table); two warps
 // then code the two state chains (symbols n-3 .. 0, each coded by the state of its index parity)
-// side by side, recording for every symbol its emitted bits and their count instead of packing
-// them; the CTA then packs in parallel: a block scan of the bit counts gives every symbol its bit
-// position, each thread writes the bits of one run of symbols (words shared with a neighbour
-// merged with atomicOr), and thread 0 appends the two final states and the end mark.  (The
+// side by side, recording for every symbol only the state before it (the emitted bits are its low
+// bits, their count follows from the state and the symbol); the CTA then packs in parallel: a
+// block scan of the bit counts gives every symbol its bit position, each thread writes the bits of
+// one run of symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends
+// the two final states and the end mark.  (The
 // chains of these skewed class streams converge too slowly for a speculative split.)  Writes the
 // complete fse_enc record ([1][u32 len][data] | [0][raw] | [2][sym]) to the block's slot; the
-// record flag goes into bits 56-63 of `sizes`.  `recs` is scratch of kFseRecWords words per block.
+// record flag goes into bits 56-63 of `sizes`.  `recs` is scratch of kFseRecWords words per block
+// (the 16-bit step records of both chains).
 constexpr unsigned kFseMaxLog = 11;               // the block coder's table log never exceeds 11
 // Next-state table of the chains (dynamic shared memory): for every symbol s from the smallest
-// to the largest present one and every state x, the coded state minus L (bits 0-10) and the
-// number of emitted bits (bits 11-14), so that a chain step is one table load.  Blocks whose
-// table would not fit (symbol span x L x 2 bytes) take the state-table path.
+// to the largest present one and every state x, twice the coded state minus L, which is the byte
+// offset of that state in a table row, so that a chain step is one add and one table load.
+// Blocks whose table would not fit (symbol span x L x 2 bytes) take the state-table path.
 constexpr size_t kFseNxtBytes = 40 * 1024;
-// Per-chain record scratch (words): a chain's records are indexed by step plus the chain's lead
-// (the steps that its first 16-byte symbol word holds above the chain's start).
+// Per-chain record scratch (16-bit records): a chain's records are indexed by step plus the
+// chain's lead (the steps that its first 16-byte symbol word holds above the chain's start).
 constexpr unsigned kFseChainRec = FBLK / 2 + 32;
-constexpr unsigned kFseRecWords = 2 * kFseChainRec;
+constexpr unsigned kFseRecWords = kFseChainRec;  // both chains, 2 records per word
+static_assert(kFseChainRec % 8 == 0, "records of whole symbol words are stored as 16-byte vectors");
 struct FseSmem {
     uint32_t count[256];
     uint32_t cumul[257];
@@ -119,7 +122,7 @@ struct FseSmem {
     uint8_t sym[1 << kFseMaxLog];
 };
 
-__global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__restrict__ cls,
+__global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__restrict__ cls,
                                                           const BlockJob *__restrict__ jobs,
                                                           uint8_t *__restrict__ slots,
                                                           unsigned long long *__restrict__ sizes,
@@ -289,19 +292,17 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                 if (!w.count[sy]) continue;
                 const fse::SymTT t = w.sym_tt[sy];
                 const uint32_t nb = (x + t.deltaNbBits) >> 16;
-                nxt[e] = (uint16_t)((w.state_table[(int32_t)(x >> nb) + t.deltaFindState] - L) | (nb << 11));
+                nxt[e] = (uint16_t)((w.state_table[(int32_t)(x >> nb) + t.deltaFindState] - L) << 1);
             }
             __syncthreads();
         }
         if ((threadIdx.x & 31u) == 0 && threadIdx.x < 64) {
             // The two state chains, one per warp: chain k codes the symbols i <= n - 3 of parity k
             // from the top down (step j codes symbol top - 2 j), starting from the state that
-            // symbol n-1 or n-2 (of parity k) initialised.  Each step records the state before
-            // it minus L (bits 0-10, table log <= 11; its low bits are the emitted ones), the state
-            // after it minus L (bits 11-21, the decoder's state there, from which the pack step
-            // takes the checkpoint states) and the number of emitted bits (22-25).
+            // symbol n-1 or n-2 (of parity k) initialised.  Each step records twice the state
+            // before it minus L (16 bits, table log <= 11): its low bits are the emitted ones, and
+            // the record of the chain's next step holds the state after it.
             const unsigned k = threadIdx.x >> 5;
-            const uint32_t smask = L - 1;
             uint32_t v;  // the state minus L
             {
                 const unsigned i0 = ((n - 1) % 2 == k) ? n - 1 : n - 2;
@@ -315,36 +316,40 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
             else s_i1 = v;
             const int top = (int)n - 3 - (int)(((n - 3) & 1u) != k);
             const unsigned m = top >= 0 ? (unsigned)top / 2 + 1 : 0;  // steps
-            uint32_t *rk = rec + k * kFseChainRec;
+            uint16_t *rk = reinterpret_cast<uint16_t *>(rec) + k * kFseChainRec;
             unsigned lead = 0;
             if (fast && m > 0) {
                 // The chain's symbols are every other byte of the aligned 16-byte words from the one
                 // holding symbol `top` down: eight steps per word (whole words loaded three words
                 // ahead), the first word holding `lead` steps above the chain's start.  A step is
-                // one load from the next-state table; the records of whole words leave as two
-                // 16-byte stores.
+                // one add and one load from the next-state table (its entries and the row offsets
+                // are byte offsets); the records of a whole word leave as one 16-byte store.
                 const uintptr_t a0 = reinterpret_cast<uintptr_t>(src + top);
                 const unsigned par = (unsigned)(a0 & 1u), sh = 8u * par;
                 lead = (14u + par - (unsigned)(a0 & 15u)) >> 1;
                 const unsigned nv = lead + m;
                 const uint4 *wp = reinterpret_cast<const uint4 *>(a0 & ~(uintptr_t)15);  // word g at wp - g
-                const uint16_t *tb = nxt;  // shared memory: row of symbol s at (s - minSV) << tl
+                // shared memory: the row of symbol s at byte (s - minSV) << (tl + 1)
+                const unsigned char *tb = reinterpret_cast<const unsigned char *>(nxt);
+                const unsigned rsh = tl + 1;
+                auto step = [&](uint32_t o, uint32_t v2) -> uint32_t {
+                    return *reinterpret_cast<const uint16_t *>(tb + o + v2);
+                };
                 // the chain's bytes of a word at even offsets 14, 12, .., 0 (descending steps), as the
-                // row offsets of their symbols in the next-state table
+                // byte offsets of their rows in the next-state table
                 auto offsets = [&](const uint4 &q, uint32_t *o) {
                     const uint32_t h0 = __funnelshift_r(q.x, q.y, sh), h1 = __funnelshift_r(q.y, q.z, sh);
                     const uint32_t h2 = __funnelshift_r(q.z, q.w, sh), h3 = q.w >> sh;
-                    o[0] = (((h3 >> 16) & 0xFFu) - minSV) << tl;
-                    o[1] = ((h3 & 0xFFu) - minSV) << tl;
-                    o[2] = (((h2 >> 16) & 0xFFu) - minSV) << tl;
-                    o[3] = ((h2 & 0xFFu) - minSV) << tl;
-                    o[4] = (((h1 >> 16) & 0xFFu) - minSV) << tl;
-                    o[5] = ((h1 & 0xFFu) - minSV) << tl;
-                    o[6] = (((h0 >> 16) & 0xFFu) - minSV) << tl;
-                    o[7] = ((h0 & 0xFFu) - minSV) << tl;
+                    o[0] = (((h3 >> 16) & 0xFFu) - minSV) << rsh;
+                    o[1] = ((h3 & 0xFFu) - minSV) << rsh;
+                    o[2] = (((h2 >> 16) & 0xFFu) - minSV) << rsh;
+                    o[3] = ((h2 & 0xFFu) - minSV) << rsh;
+                    o[4] = (((h1 >> 16) & 0xFFu) - minSV) << rsh;
+                    o[5] = ((h1 & 0xFFu) - minSV) << rsh;
+                    o[6] = (((h0 >> 16) & 0xFFu) - minSV) << rsh;
+                    o[7] = ((h0 & 0xFFu) - minSV) << rsh;
                 };
-                // the record of a step from the state before it and its table entry
-                auto record = [](uint32_t v0, uint32_t e) -> uint32_t { return v0 | (e << 11); };
+                uint32_t v2 = v << 1;  // twice the state minus L
                 // steps [t0, t1) of word g one at a time (the partial first and last words)
                 auto partial = [&](unsigned g, unsigned t0, unsigned t1) {
                     uint32_t o[8];
@@ -352,22 +357,19 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
 #pragma unroll
                     for (unsigned t = 0; t < 8; t++) {
                         if (t < t0 || t >= t1) continue;
-                        const uint32_t e = tb[o[t] + v];
-                        rk[8 * g + t] = record(v, e);
-                        v = e & 0x7FFu;
+                        rk[8 * g + t] = (uint16_t)v2;
+                        v2 = step(o[t], v2);
                     }
                 };
                 const unsigned gs = lead ? 1u : 0u, ge = nv >> 3;  // the whole words [gs, ge)
                 if (lead) partial(0, lead, min(8u, nv));
                 if (gs < ge) {
-                    // Whole words, software-pipelined: the lookup of the next step is issued before
-                    // the record of the current one is formed, so that only the lookups and the
-                    // masking of their states stay on the chain.
+                    // Whole words; the symbol words are loaded three words ahead and their row
+                    // offsets formed a word ahead, so that only the adds and lookups stay on the chain.
                     uint4 q1 = gs + 1 < ge ? wp[-(int)(gs + 1)] : make_uint4(0, 0, 0, 0);
                     uint4 q2 = gs + 2 < ge ? wp[-(int)(gs + 2)] : make_uint4(0, 0, 0, 0);
                     uint32_t o[8];
                     offsets(wp[-(int)gs], o);
-                    uint32_t e = tb[o[0] + v];
                     for (unsigned g = gs; g < ge; g++) {
                         const uint4 qn = q1;
                         q1 = q2;
@@ -377,21 +379,17 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                         uint32_t r[8];
 #pragma unroll
                         for (int t = 0; t < 8; t++) {
-                            const uint32_t vn = e & 0x7FFu;
-                            uint32_t en = 0;
-                            if (t < 7) en = tb[o[t + 1] + vn];
-                            else if (g + 1 < ge) en = tb[on[0] + vn];
-                            r[t] = record(v, e);
-                            v = vn;
-                            e = en;
+                            r[t] = v2;
+                            v2 = step(o[t], v2);
                         }
-                        reinterpret_cast<uint4 *>(rk + 8 * g)[0] = make_uint4(r[0], r[1], r[2], r[3]);
-                        reinterpret_cast<uint4 *>(rk + 8 * g)[1] = make_uint4(r[4], r[5], r[6], r[7]);
+                        *reinterpret_cast<uint4 *>(rk + 8 * g) =
+                            make_uint4(r[0] | (r[1] << 16), r[2] | (r[3] << 16), r[4] | (r[5] << 16), r[6] | (r[7] << 16));
 #pragma unroll
                         for (int t = 0; t < 8; t++) o[t] = on[t];
                     }
                 }
                 if (ge >= gs && 8 * ge < nv && (ge > 0 || !lead)) partial(ge, 0, nv - 8 * ge);
+                v = v2 >> 1;
             } else if (m > 0) {
                 // the state-table path: the symbol transform of the next symbol and the symbol
                 // after it are loaded ahead, so that only the state table lookup stays on the chain
@@ -404,7 +402,7 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                     ya = __ldg(src + max(i - 4, 0));
                     const uint32_t nba = (sA + ta.deltaNbBits) >> 16;
                     const uint32_t xa = w.state_table[(int32_t)(sA >> nba) + ta.deltaFindState];
-                    rk[j] = (sA - L) | ((xa & smask) << 11) | (nba << 22);
+                    rk[j] = (uint16_t)((sA - L) << 1);
                     sA = xa;
                     ta = na;
                 }
@@ -426,9 +424,27 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
         // the record of emission position e: even positions belong to the chain of n-3's parity
         const unsigned ka = (n - 3) & 1u;
         const unsigned offA = ka * kFseChainRec + s_lead[ka], offB = (ka ^ 1u) * kFseChainRec + s_lead[ka ^ 1u];
-        auto R = [&](unsigned e) -> uint32_t { return rec[((e & 1u) ? offB : offA) + (e >> 1)]; };
+        const uint16_t *rec16 = reinterpret_cast<const uint16_t *>(rec);
+        // the state minus L before emission position e (symbol n - 3 - e)
+        auto V = [&](unsigned e) -> uint32_t { return rec16[((e & 1u) ? offB : offA) + (e >> 1)] >> 1; };
+        // the number of bits that state v + L emits for symbol sy
+        const uint32_t Lb = 1u << tl;
+        auto NB = [&](uint32_t v, unsigned sy) -> uint32_t { return (v + Lb + w.sym_tt[sy].deltaNbBits) >> 16; };
+        // records and symbols are read kPackBatch at a time, all loads of a batch before its uses
+        constexpr unsigned kPackBatch = 8;
         uint32_t cnt = 0;
-        for (unsigned e = e0; e < e1; e++) cnt += R(e) >> 22;
+        for (unsigned e = e0; e < e1; e += kPackBatch) {
+            uint32_t vv[kPackBatch], sy[kPackBatch];
+#pragma unroll
+            for (unsigned u = 0; u < kPackBatch; u++) {
+                const unsigned ee = min(e + u, e1 - 1);
+                vv[u] = V(ee);
+                sy[u] = src[n - 3 - ee];
+            }
+#pragma unroll
+            for (unsigned u = 0; u < kPackBatch; u++)
+                if (e + u < e1) cnt += NB(vv[u], sy[u]);
+        }
         uint32_t sym_bits;  // bits of all symbols
         const uint32_t off = block_excl_scan<uint32_t>(cnt, s_sh, sym_bits);
         const uint32_t total = sym_bits + 2 * tl + 1;
@@ -450,22 +466,34 @@ __global__ void __launch_bounds__(256) k_fse_encode_blocks(const uint8_t *__rest
                 first = false;
             };
             uint32_t pos = off;
-            for (unsigned e = e0; e < e1; e++) {
-                const unsigned i = n - 3 - e;
-                const uint32_t r = R(e), nb = r >> 22;
-                acc |= (uint64_t)(r & ((1u << nb) - 1u)) << accn;
-                accn += nb;
-                pos += nb;
-                if (ck && i > 0 && (i & (part - 1)) == 0) {
-                    // decoder states before symbol i: after symbol i (even chain), after i + 1 (odd)
-                    const uint32_t odd = i + 1 <= n - 3 ? (R(e - 1) >> 11) & 0x7FFu : ((n - 2) & 1 ? s_i1 : s_i0);
-                    ck[i / part - 1] = FseCkpt{pos, (uint16_t)((r >> 11) & 0x7FFu), (uint16_t)odd};
+            for (unsigned e = e0; e < e1; e += kPackBatch) {
+                uint32_t vv[kPackBatch], sy[kPackBatch];
+#pragma unroll
+                for (unsigned u = 0; u < kPackBatch; u++) {
+                    const unsigned ee = min(e + u, e1 - 1);
+                    vv[u] = V(ee);
+                    sy[u] = src[n - 3 - ee];
                 }
-                if (accn >= 32) {
-                    flush_word((uint32_t)acc);
-                    wi++;
-                    acc >>= 32;
-                    accn -= 32;
+#pragma unroll
+                for (unsigned u = 0; u < kPackBatch; u++) {
+                    if (e + u >= e1) break;
+                    const unsigned i = n - 3 - (e + u);
+                    const uint32_t v = vv[u], nb = NB(v, sy[u]);
+                    acc |= (uint64_t)(v & ((1u << nb) - 1u)) << accn;
+                    accn += nb;
+                    pos += nb;
+                    if (ck && i > 0 && (i & (part - 1)) == 0) {
+                        // decoder states before symbol i: the states after symbol i (the state
+                        // before symbol i - 2 of its chain) and after symbol i + 1 (before i - 1)
+                        const uint32_t odd = i + 1 <= n - 3 ? V(e + u + 1) : ((n - 2) & 1 ? s_i1 : s_i0);
+                        ck[i / part - 1] = FseCkpt{pos, (uint16_t)V(e + u + 2), (uint16_t)odd};
+                    }
+                    if (accn >= 32) {
+                        flush_word((uint32_t)acc);
+                        wi++;
+                        acc >>= 32;
+                        accn -= 32;
+                    }
                 }
             }
             if (e1 > e0 && accn > 0) atomicOr(bw + wi, (uint32_t)acc);
@@ -2809,6 +2837,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
     tr.mark("chains done");
     if (he[1] && ck) {
         // a checkpoint did not match the stream: decode again, sequentially
+        if (tr.on) std::fprintf(stderr, "[falcons trace] decode checkpoint mismatch: decoding sequentially\n");
         return entropy_decode(ctx, d_in, h, n, d_codes, st, nullptr);
     }
     if (he[0]) throw std::invalid_argument("Invalid or corrupted Falcons entropy payload");

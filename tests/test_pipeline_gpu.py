@@ -206,10 +206,11 @@ def _ckpt_frame(buf):
     return pos, int(o1_part), int(fse_part), int(n_o1), int(n_fse)
 
 
-def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference):
+def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference, monkeypatch, capfd):
     """Streams carry decode checkpoints (a skippable frame the reference ignores); the GPU decodes
-    every chain and FSE block as independent parts from them, and a damaged checkpoint frame only
-    makes it decode sequentially, with the same result."""
+    every chain and FSE block as independent parts from them (every checkpoint the encoder wrote
+    matches the stream), and a damaged checkpoint frame only makes it decode sequentially, with the
+    same result."""
     import torch
     from falcons_b200 import api, device as D, synth
     x = synth.spectral_field((128, 128, 128), seed=6)
@@ -222,9 +223,13 @@ def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference):
     y_ref = reference.decompress(buf.tobytes(), np.float32, x.size).ravel()
     y, _ = api.falcons.decompress(buf, np.float32, x.shape)
     np.testing.assert_array_equal(np.asarray(y).ravel(), y_ref)
+    monkeypatch.setenv("FALCONS_TRACE", "1")
+    capfd.readouterr()
     yd, _ = D.decompress(torch.from_numpy(buf.copy()).to(cuda), torch.float32)
     torch.cuda.synchronize()
     np.testing.assert_array_equal(yd.cpu().numpy(), y_ref)
+    assert "checkpoint mismatch" not in capfd.readouterr().err
+    monkeypatch.delenv("FALCONS_TRACE")
     arr = pos + 32
     damaged = []
     b1 = buf.copy()                                   # a chain checkpoint's state
@@ -239,11 +244,16 @@ def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference):
     b4 = buf.copy()                                   # a count that does not match the stream
     b4[pos + 16] ^= 1
     damaged.append(b4)
-    for bad in damaged:
+    for j, bad in enumerate(damaged):
         yb, _ = api.falcons.decompress(bad, np.float32, x.shape)
         np.testing.assert_array_equal(np.asarray(yb).ravel(), y_ref)
+        monkeypatch.setenv("FALCONS_TRACE", "1")
+        capfd.readouterr()
         ybd, _ = D.decompress(torch.from_numpy(bad.copy()).to(cuda), torch.float32)
         torch.cuda.synchronize()
         np.testing.assert_array_equal(ybd.cpu().numpy(), y_ref)
+        if j < 3:  # a damaged state or bit position is caught by the part that ends there
+            assert "checkpoint mismatch" in capfd.readouterr().err
+        monkeypatch.delenv("FALCONS_TRACE")
     # the reference decoder skips the frame, damaged or not
     np.testing.assert_array_equal(reference.decompress(damaged[0].tobytes(), np.float32, x.size).ravel(), y_ref)
