@@ -1505,11 +1505,18 @@ __global__ void __launch_bounds__(kChainThreads) k_o1_decode_smem(const uint8_t 
 // The stream is bit-identical to a sequential encoder's (the tANS states are fully determined).
 // All 15 context state tables stay in shared memory: the two contexts that carry most codes (from
 // the table set's histogram) as 16-bit states, the other 13 as 13-bit entries (state - 8192)
-// packed into words; one word per key holds the symbol transform.
+// packed into words; one word per key holds the symbol transform.  k_spec_image lays this out once
+// per table set in global memory, and every CTA copies it in.
 constexpr int kSpecThreads = 1024;
 constexpr int kSpecHot = 2;
 constexpr unsigned kSpecPackWords = (O1_NCTX - kSpecHot) * O1_M * O1_PB / 32 + 1;  // + 1: a read of w + 1
-constexpr size_t kSpecSmem = (size_t)kSpecHot * O1_M * 2 + (size_t)kSpecPackWords * 4 + (size_t)O1_NCTX * O1_NSYM * 4;
+constexpr size_t kSpecSmem =
+    ((size_t)kSpecHot * O1_M * 2 + (size_t)kSpecPackWords * 4 + (size_t)O1_NCTX * O1_NSYM * 4 + 15) & ~(size_t)15;
+// Which table slot every context of a table set takes (4 bits each; slots 0 and 1 are the 16-bit
+// tables).
+struct SpecMeta {
+    unsigned long long map;
+};
 constexpr int kSparseShift = 6;  // kept speculative states: every 64th index
 struct SpecCta {
     int table;
@@ -1554,6 +1561,33 @@ __device__ __forceinline__ void walk_keys(const uint16_t *__restrict__ keys, lon
     for (; i >= bottom; i--) f(i, (uint32_t)__ldg(keys + i));
 }
 
+// As walk_keys, but stops (and returns true) at the first index for which f returns true.
+template <class F>
+__device__ __forceinline__ bool walk_keys_until(const uint16_t *__restrict__ keys, long long top, long long bottom,
+                                                F &&f) {
+    long long i = top;
+    for (; i >= bottom && (i & 7) != 7; i--)
+        if (f(i, (uint32_t)__ldg(keys + i))) return true;
+    if (i - 7 >= bottom) {
+        const uint4 *kv = reinterpret_cast<const uint4 *>(keys);
+        const uint4 z = make_uint4(0, 0, 0, 0);
+        uint4 v0 = __ldg(kv + ((i - 7) >> 3));
+        uint4 v1 = i - 15 >= 0 ? __ldg(kv + ((i - 15) >> 3)) : z;
+        while (i - 7 >= bottom) {
+            const uint4 v2 = i - 23 >= 0 ? __ldg(kv + ((i - 23) >> 3)) : z;
+            if (f(i, v0.w >> 16) || f(i - 1, v0.w & 0xFFFFu) || f(i - 2, v0.z >> 16) || f(i - 3, v0.z & 0xFFFFu) ||
+                f(i - 4, v0.y >> 16) || f(i - 5, v0.y & 0xFFFFu) || f(i - 6, v0.x >> 16) || f(i - 7, v0.x & 0xFFFFu))
+                return true;
+            i -= 8;
+            v0 = v1;
+            v1 = v2;
+        }
+    }
+    for (; i >= bottom; i--)
+        if (f(i, (uint32_t)__ldg(keys + i))) return true;
+    return false;
+}
+
 // Per key (context << 8 | symbol) the encoder's symbol transform, as one word: deltaFindState +
 // 8192 (bits 0-13), minStatePlus - 8192 (14-27) and maxBitsOut (28-31); the emitted bit count of
 // state x is maxBitsOut - (x < minStatePlus), which is (x + deltaNbBits) >> 16 with deltaNbBits =
@@ -1563,9 +1597,92 @@ __host__ __device__ __forceinline__ uint32_t enc_word(const fse::SymTT &t) {
     return (uint32_t)(t.deltaFindState + O1_M) | ((msp - O1_M) << 14) | (mbo << 28);
 }
 
+// The chain encoder's shared-memory image of table set blockIdx.y (kSpecSmem bytes at image +
+// blockIdx.y * kSpecSmem / 4, laid out as k_o1_encode_spec's dynamic shared memory), filled by all
+// blocks of the grid's x dimension: the 16-bit tables of the two contexts with the most codes in
+// the set's histogram, the other contexts' 13-bit packed entries, and the transform word of every key.
+__global__ void __launch_bounds__(256) k_spec_image(const uint16_t *__restrict__ stab,
+                                                    const fse::SymTT *__restrict__ stt,
+                                                    const uint32_t *__restrict__ thist, uint32_t *__restrict__ image,
+                                                    SpecMeta *__restrict__ meta) {
+    __shared__ uint32_t s_tot[O1_NCTX];
+    __shared__ uint8_t s_rev[O1_NCTX];  // context of every slot
+    const size_t tb = (size_t)blockIdx.y * O1_NCTX;
+    const uint16_t *__restrict__ S = stab + tb * O1_M;
+    if (threadIdx.x < O1_NCTX) s_tot[threadIdx.x] = 0;
+    __syncthreads();
+    {
+        // codes per context: 16 threads per context, 16 symbols each
+        const unsigned c = threadIdx.x / 16, s0 = (threadIdx.x % 16) * 16;
+        if (c < (unsigned)O1_NCTX) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int u = 0; u < 16; u++) v += __ldg(thist + (tb + c) * O1_NSYM + s0 + u);
+            atomicAdd(&s_tot[c], v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int h0 = 0, h1 = 1;
+        if (s_tot[h1] > s_tot[h0]) h0 = 1, h1 = 0;
+        for (int c = 2; c < O1_NCTX; c++) {
+            if (s_tot[c] > s_tot[h0]) h1 = h0, h0 = c;
+            else if (s_tot[c] > s_tot[h1]) h1 = c;
+        }
+        unsigned long long m = 0;
+        int slot = kSpecHot;
+        s_rev[0] = (uint8_t)h0;
+        s_rev[1] = (uint8_t)h1;
+        for (int c = 0; c < O1_NCTX; c++) {
+            const int sl = c == h0 ? 0 : c == h1 ? 1 : slot++;
+            m |= (unsigned long long)sl << (4 * c);
+            if (sl >= kSpecHot) s_rev[sl] = (uint8_t)c;
+        }
+        if (blockIdx.x == 0) meta[blockIdx.y].map = m;
+    }
+    __syncthreads();
+    uint32_t *img = image + (size_t)blockIdx.y * (kSpecSmem / 4);
+    uint32_t *hot2 = img;                                    // 16-bit tables, two entries per word
+    uint32_t *pk = img + kSpecHot * O1_M / 2;                // packed state tables
+    uint32_t *r_enc = pk + kSpecPackWords;                   // symbol transform per key
+    constexpr unsigned kHotWords = kSpecHot * O1_M / 2, kKeys = O1_NCTX * O1_NSYM;
+    constexpr unsigned kPacked = (O1_NCTX - kSpecHot) * O1_M;
+    const unsigned total = kHotWords + kSpecPackWords + kKeys;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        if (i < kHotWords) {
+            const unsigned e = 2 * i;  // entries e, e + 1 of the same context
+            const uint16_t *row = S + (size_t)s_rev[e / O1_M] * O1_M + (e % O1_M);
+            hot2[i] = (uint32_t)__ldg(row) | ((uint32_t)__ldg(row + 1) << 16);
+        } else if (i < kHotWords + kSpecPackWords) {
+            // word wd holds the bits [32 wd, 32 wd + 32) of the packed entries (entry j at bit 13 j;
+            // entry j is state u = j % 8192 of the context in slot kSpecHot + j / 8192)
+            const unsigned wd = i - kHotWords;
+            uint32_t v = 0;
+            const unsigned j0 = wd * 32 / O1_PB, j1 = min((wd * 32 + 31) / O1_PB, kPacked - 1);
+            uint32_t ev[4];  // a word spans at most 4 entries
+#pragma unroll
+            for (unsigned u = 0; u < 4; u++) {
+                const unsigned j = min(j0 + u, kPacked - 1);
+                ev[u] = (uint32_t)__ldg(S + (size_t)s_rev[kSpecHot + j / O1_M] * O1_M + (j % O1_M)) - O1_M;  // 13 bits
+            }
+#pragma unroll
+            for (unsigned u = 0; u < 4; u++) {
+                const unsigned j = j0 + u;
+                if (j > j1 || j >= kPacked) break;
+                const int sh = (int)(j * O1_PB) - (int)(wd * 32);
+                v |= sh >= 0 ? ev[u] << sh : ev[u] >> -sh;
+            }
+            pk[wd] = v;
+        } else {
+            const unsigned k = i - kHotWords - kSpecPackWords;
+            r_enc[k] = enc_word(stt[tb * O1_NSYM + k]);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     const uint16_t *__restrict__ keys, const SegInfo *__restrict__ segs, const SpecCta *__restrict__ ctas,
-    const uint16_t *__restrict__ stab, const fse::SymTT *__restrict__ stt, const uint32_t *__restrict__ thist,
+    const uint32_t *__restrict__ image, const SpecMeta *__restrict__ meta,
     uint16_t *__restrict__ sparse,
     uint16_t *__restrict__ sparse_bits, uint32_t *__restrict__ stage, uint32_t *__restrict__ rstage,
     uint8_t *__restrict__ slots, const unsigned long long *__restrict__ slot_off,
@@ -1579,57 +1696,11 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
     uint16_t *s_bits = reinterpret_cast<uint16_t *>(r_enc), *s_esc = s_bits + kSpecThreads;
     __shared__ uint16_t s_exit[kSpecThreads + 1];
     __shared__ uint8_t s_chg[kSpecThreads + 1];
-    __shared__ unsigned long long s_map;  // table slot of every context (4 bits each)
-    __shared__ uint8_t s_rev[O1_NCTX];    // context of every slot
     const SpecCta w = ctas[blockIdx.x];
-    const size_t tb = (size_t)w.table * O1_NCTX;
-    const uint16_t *__restrict__ S = stab + tb * O1_M;
-    if (threadIdx.x < 32) {
-        // codes per context in the table set's histogram; the two largest get the 16-bit slots
-        uint32_t tot[O1_NCTX];
-        for (int c = 0; c < O1_NCTX; c++) {
-            uint32_t v = 0;
-            for (int sy = threadIdx.x; sy < O1_NSYM; sy += 32) v += __ldg(thist + (tb + c) * O1_NSYM + sy);
-            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            tot[c] = v;
-        }
-        if (threadIdx.x == 0) {
-            int h0 = 0, h1 = 1;
-            if (tot[h1] > tot[h0]) h0 = 1, h1 = 0;
-            for (int c = 2; c < O1_NCTX; c++) {
-                if (tot[c] > tot[h0]) h1 = h0, h0 = c;
-                else if (tot[c] > tot[h1]) h1 = c;
-            }
-            unsigned long long m = 0;
-            int slot = kSpecHot;
-            s_rev[0] = (uint8_t)h0;
-            s_rev[1] = (uint8_t)h1;
-            for (int c = 0; c < O1_NCTX; c++) {
-                const int sl = c == h0 ? 0 : c == h1 ? 1 : slot++;
-                m |= (unsigned long long)sl << (4 * c);
-                if (sl >= kSpecHot) s_rev[sl] = (uint8_t)c;
-            }
-            s_map = m;
-        }
-    }
-    __syncthreads();
-    const unsigned long long smap = s_map;
-    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) r_enc[i] = enc_word(stt[tb * O1_NSYM + i]);
-    for (int i = threadIdx.x; i < kSpecHot * O1_M; i += blockDim.x)
-        hot[i] = __ldg(S + (size_t)s_rev[i / O1_M] * O1_M + (i % O1_M));
-    // word wd holds the bits [32 wd, 32 wd + 32) of the packed entries (entry j at bit 13 j; entry
-    // j is state u = j % 8192 of the context in slot kSpecHot + j / 8192)
-    constexpr unsigned kPacked = (O1_NCTX - kSpecHot) * O1_M;
-    for (unsigned wd = threadIdx.x; wd < kSpecPackWords; wd += blockDim.x) {
-        uint32_t v = 0;
-        const unsigned j0 = wd * 32 / O1_PB, j1 = min((wd * 32 + 31) / O1_PB, kPacked - 1);
-        for (unsigned j = j0; j <= j1 && j < kPacked; j++) {
-            const unsigned c = s_rev[kSpecHot + j / O1_M];
-            const uint32_t e = (uint32_t)__ldg(S + (size_t)c * O1_M + (j % O1_M)) - O1_M;  // 13 bits
-            const int sh = (int)(j * O1_PB) - (int)(wd * 32);
-            v |= sh >= 0 ? e << sh : e >> -sh;
-        }
-        pk[wd] = v;
+    const unsigned long long smap = meta[w.table].map;  // table slot of every context (4 bits each)
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(image + (size_t)w.table * (kSpecSmem / 4));
+        for (unsigned i = threadIdx.x; i < kSpecSmem / 16; i += blockDim.x) smem_raw[i] = __ldg(src + i);
     }
     const int t = threadIdx.x;
     const int ci = t / w.ppc, p = t % w.ppc;
@@ -1766,20 +1837,27 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         if (need && round <= nparts + 2) {
             Stager rg{rw};
             uint32_t x = E;
-            bool met = false;
-            for (long long i = top; i >= a; i--) {
-                const uint32_t k = i == lo ? k_lo : (uint32_t)__ldg(keys + i);
+            // the kept state of the next 64th index below, loaded one kept index ahead
+            long long ck_i = top & ~63LL;
+            uint32_t ck_x = ck_i >= a ? sparse[ck_i >> 6] : 0u;
+            auto rstep = [&](long long i, uint32_t k) -> bool {
                 const EncRec r = rec_of(k);
                 const uint32_t nb = nbits(x, r);
                 rg.put(x, nb);
                 x = next_state(x, r, nb);
                 repaired++;
-                if (((uint32_t)i & 63u) == 0 && sparse[i >> 6] == (uint16_t)x) {
-                    met = true;
+                if (i != ck_i) return false;
+                if (ck_x == x) {
                     cut = sparse_bits[i >> 6];
-                    break;
+                    return true;
                 }
-            }
+                ck_i -= 64;
+                ck_x = ck_i >= a ? sparse[ck_i >> 6] : 0u;
+                return false;
+            };
+            // index lo (a chain's first code, context 0) is coded apart from the walk
+            bool met = walk_keys_until(keys, top, p == 0 ? a + 1 : a, rstep);
+            if (!met && p == 0) met = rstep(lo, k_lo);
             if (!met && p == 0) {
                 rg.put(x & (O1_M - 1), O1_PB);
                 rg.put(1u, 1u);
@@ -1827,19 +1905,31 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         };
         uint64_t acc = 0;
         uint32_t accn = off & 31u;
-        // appends bits [b0, b1) of staging words src
+        // appends bits [b0, b1) of staging words src, loading kBatch + 1 staging words (those
+        // inside the part's staging column) before placing kBatch words
+        constexpr uint32_t kBatch = 8;
         auto append = [&](const uint32_t *src, uint32_t b0, uint32_t b1) {
-            for (uint32_t bp = b0; bp < b1; bp += 32) {
-                const uint32_t n = min(32u, b1 - bp), j = bp >> 5, sh = bp & 31u;
-                const uint32_t lo = src[(size_t)j * kSpecThreads];
-                uint32_t v = sh ? __funnelshift_r(lo, src[(size_t)(j + 1) * kSpecThreads], sh) : lo;
-                if (n < 32) v &= (1u << n) - 1u;
-                acc |= (uint64_t)v << accn;
-                accn += n;
-                if (accn >= 32) {
-                    store((uint32_t)acc);
-                    acc >>= 32;
-                    accn -= 32;
+            const uint32_t sh = b0 & 31u;
+            for (uint32_t bp = b0; bp < b1; bp += 32 * kBatch) {
+                const uint32_t j0 = bp >> 5;
+                uint32_t wv[kBatch + 1];
+#pragma unroll
+                for (uint32_t u = 0; u <= kBatch; u++)
+                    wv[u] = j0 + u < (uint32_t)stw ? src[(size_t)(j0 + u) * kSpecThreads] : 0u;
+#pragma unroll
+                for (uint32_t u = 0; u < kBatch; u++) {
+                    const uint32_t q = bp + 32 * u;
+                    if (q >= b1) break;
+                    const uint32_t n = min(32u, b1 - q);
+                    uint32_t v = sh ? __funnelshift_r(wv[u], wv[u + 1], sh) : wv[u];
+                    if (n < 32) v &= (1u << n) - 1u;
+                    acc |= (uint64_t)v << accn;
+                    accn += n;
+                    if (accn >= 32) {
+                        store((uint32_t)acc);
+                        acc >>= 32;
+                        accn -= 32;
+                    }
                 }
             }
         };
@@ -2464,6 +2554,14 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         FB2_CUDA(cudaMemsetAsync(d_err, 0, 32, st));
         k_o1_ctable<<<ntab, kTabThreads, 0, st>>>(nf, stab, stt, spread, d_err);
         FB2_CHECK_LAUNCH();
+        // the chain encoder's shared-memory image of every table set
+        uint32_t *image = pool.get<uint32_t>((size_t)R * (kSpecSmem / 4));
+        SpecMeta *meta = pool.get<SpecMeta>((size_t)R);
+        {
+            const unsigned items = kSpecHot * O1_M / 2 + kSpecPackWords + O1_NCTX * O1_NSYM;
+            k_spec_image<<<dim3((items + 255) / 256, (unsigned)R), 256, 0, st>>>(stab, stt, rhist, image, meta);
+            FB2_CHECK_LAUNCH();
+        }
         // chain output slots
         const long long nchains = S * kMaxK;
         std::vector<unsigned long long> soff(nchains + 1, 0);
@@ -2490,7 +2588,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             uint32_t *rstage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
             enable_big_smem();
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
-                keys, d_segs, d_ctas, stab, stt, rhist, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
+                keys, d_segs, d_ctas, image, meta, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
                 d_ck_off, ck_every, d_err);
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
