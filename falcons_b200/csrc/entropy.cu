@@ -1145,38 +1145,90 @@ struct SegInfo {
     int pad;
 };
 
-__global__ void __launch_bounds__(1024) k_o1_hist(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
-                                                 uint32_t *__restrict__ hist, uint32_t *__restrict__ nvk,
-                                                 uint16_t *__restrict__ keys) {
-    __shared__ uint32_t h[O1_NCTX * O1_NSYM];
+// Per segment: the count of every (context, symbol) key of its chains (a chain's first code has
+// context 0) and every chain's escape count; writes every code's key (context << 8 | symbol) for
+// the chain encoder.  Codes are read 8 at a time as 16-byte vectors when q is 16-byte aligned (the
+// code before a vector comes from the lane below), runs of equal keys within a vector are counted
+// with one atomic, and the lanes of a warp spread their atomics over kHistCopies histograms.
+constexpr int kHistCopies = 4;
+constexpr size_t kHistSmem = (size_t)kHistCopies * O1_NCTX * O1_NSYM * 4;
+__global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
+                                                    uint32_t *__restrict__ hist, uint32_t *__restrict__ nvk,
+                                                    uint16_t *__restrict__ keys, int vec) {
+    extern __shared__ uint32_t hs[];  // kHistCopies histograms of O1_NCTX * O1_NSYM keys
     __shared__ uint32_t esc[kMaxK];
+    constexpr int HN = O1_NCTX * O1_NSYM;
     const SegInfo sg = segs[blockIdx.x];
-    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) h[i] = 0;
+    for (int i = threadIdx.x; i < kHistCopies * HN; i += blockDim.x) hs[i] = 0;
     if (threadIdx.x < kMaxK) esc[threadIdx.x] = 0;
     __syncthreads();
+    const unsigned lane = threadIdx.x & 31u;
+    uint32_t *h = hs + (lane % kHistCopies) * HN;
     for (int k = 0; k < sg.K; k++) {
-        const unsigned long long c0 = (unsigned long long)k * sg.cs;
-        const unsigned long long c1 = min(c0 + sg.cs, sg.n);
+        const long long b = (long long)(sg.lo + (unsigned long long)k * sg.cs);
+        const long long e = (long long)(sg.lo + min((unsigned long long)k * sg.cs + sg.cs, sg.n));
+        if (e <= b) continue;
+        // codes [b, hb) and [tb, e) one per thread, whole vectors [hb, tb) one per thread
+        long long hb = e, tb = e;
+        if (vec) {
+            hb = min(e, (b + 7) & ~7LL);
+            tb = max(hb, e & ~7LL);
+        }
         uint32_t ne = 0;
-        // warp-uniform loop (the escape count is reduced over the warp after it)
-        for (unsigned long long rb = c0 + (threadIdx.x & ~31u); rb < c1; rb += blockDim.x) {
-            const unsigned long long r = rb + (threadIdx.x & 31);
-            if (r < c1) {
-                const unsigned long long i = sg.lo + r;
-                const int prev = r == c0 ? 0 : (int)q[i - 1];
-                const int s = o1_sym((int)q[i]);
-                const int c = o1_ctx(prev);
-                atomicAdd(&h[c * O1_NSYM + s], 1u);
-                keys[i] = (uint16_t)((c << 8) | s);
-                ne += s == O1_NSYM - 1;
+        const long long nh = hb - b, nt = e - tb;
+        for (long long j = threadIdx.x; j < nh + nt; j += blockDim.x) {
+            const long long i = j < nh ? b + j : tb + (j - nh);
+            const int prev = i == b ? 0 : (int)q[i - 1];
+            const int sy = o1_sym((int)q[i]);
+            const uint32_t key = (uint32_t)(o1_ctx(prev) << 8) | (uint32_t)sy;
+            atomicAdd(&h[key], 1u);
+            keys[i] = (uint16_t)key;
+            ne += sy == O1_NSYM - 1;
+        }
+        const long long v0 = hb >> 3, v1 = tb >> 3;
+        const uint4 *q4 = reinterpret_cast<const uint4 *>(q);
+        uint4 *k4 = reinterpret_cast<uint4 *>(keys);
+        for (long long vb = v0 + (threadIdx.x & ~31u); vb < v1; vb += blockDim.x) {  // warp-uniform
+            const long long vi = vb + lane;
+            const bool act = vi < v1;
+            const uint4 w = act ? __ldg(q4 + vi) : make_uint4(0, 0, 0, 0);
+            const uint32_t below = __shfl_up_sync(0xffffffffu, w.w >> 16, 1);
+            if (!act) continue;
+            int prev = 0;  // the code before this vector (context 0 at the chain's start)
+            if (vi * 8 > b) prev = lane ? (int)(int16_t)below : (int)q[vi * 8 - 1];
+            const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+            uint32_t kk[8];
+            uint32_t rkey = ~0u, rn = 0;
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const int code = (int)(int16_t)(ww[m >> 1] >> (16 * (m & 1)));
+                const int sy = o1_sym(code);
+                const uint32_t key = (uint32_t)(o1_ctx(prev) << 8) | (uint32_t)sy;
+                kk[m] = key;
+                ne += sy == O1_NSYM - 1;
+                if (key == rkey) {
+                    rn++;
+                } else {
+                    if (rn) atomicAdd(&h[rkey], rn);
+                    rkey = key;
+                    rn = 1;
+                }
+                prev = code;
             }
+            atomicAdd(&h[rkey], rn);
+            k4[vi] = make_uint4(kk[0] | (kk[1] << 16), kk[2] | (kk[3] << 16), kk[4] | (kk[5] << 16), kk[6] | (kk[7] << 16));
         }
         ne = __reduce_add_sync(0xffffffffu, ne);
-        if ((threadIdx.x & 31) == 0 && ne) atomicAdd(&esc[k], ne);
+        if (lane == 0 && ne) atomicAdd(&esc[k], ne);
     }
     __syncthreads();
-    uint32_t *gh = hist + (size_t)blockIdx.x * O1_NCTX * O1_NSYM;
-    for (int i = threadIdx.x; i < O1_NCTX * O1_NSYM; i += blockDim.x) gh[i] = h[i];
+    uint32_t *gh = hist + (size_t)blockIdx.x * HN;
+    for (int i = threadIdx.x; i < HN; i += blockDim.x) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int c = 0; c < kHistCopies; c++) v += hs[c * HN + i];
+        gh[i] = v;
+    }
     if (threadIdx.x < kMaxK) nvk[blockIdx.x * kMaxK + threadIdx.x] = esc[threadIdx.x];
 }
 
@@ -2195,6 +2247,7 @@ void enable_big_smem() {
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_parts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kDecSlots * O1_M * 4));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_encode_spec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpecSmem));
+    FB2_CUDA(cudaFuncSetAttribute(k_o1_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHistSmem));
     done = true;
 }
 
@@ -2514,7 +2567,9 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint32_t *hist = pool.get<uint32_t>((size_t)S * O1_NCTX * O1_NSYM);
         uint32_t *nvk = pool.get<uint32_t>((size_t)S * kMaxK);
         uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
-        k_o1_hist<<<(unsigned)S, 1024, 0, st>>>(q, d_segs, hist, nvk, keys);
+        enable_big_smem();
+        k_o1_hist<<<(unsigned)S, 1024, kHistSmem, st>>>(q, d_segs, hist, nvk, keys,
+                                                       (reinterpret_cast<uintptr_t>(q) & 15) == 0);
         FB2_CHECK_LAUNCH();
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
