@@ -2,9 +2,10 @@
 
 Python access to the two CPU checkers of the CUDA path:
 
-* ``Restatement`` wraps ``oracle/liboracle.so``, the plain-C restatement of the reference's
-  interpolation decomposition (oracle/interp_oracle.c).  It is built by ``make -C oracle``
-  and needs no reference sources, so it is available on any machine with gcc.
+* ``Restatement`` wraps ``oracle/liboracle.so``, the plain-C restatements of the reference's
+  interpolation decomposition (oracle/interp_oracle.c) and of its 1-D blockwise Lorenzo +
+  Huffman path (oracle/lorenzo_oracle.c).  It is built by ``make -C oracle`` and needs no
+  reference sources, so it is available on any machine with gcc.
 * ``Reference`` wraps ``oracle/_ref/libfalcons_ref.so`` (scalar, serial) or
   ``libfalcons_ref_omp.so`` (AVX2 + OpenMP), built from the reference's own headers by
   ``make -C oracle ref``.  It exists only where the reference sources were present at
@@ -36,7 +37,8 @@ DEFAULT_ANCHOR = {1: 4096, 2: 128, 3: 32, 4: 16}
 
 def ensure_restatement() -> str:
     """Build liboracle.so if missing (gcc only)."""
-    src = [os.path.join(HERE, "interp_oracle.c"), os.path.join(HERE, "interp_oracle_impl.h")]
+    src = [os.path.join(HERE, f) for f in ("interp_oracle.c", "interp_oracle_impl.h", "lorenzo_oracle.c",
+                                           "lorenzo_oracle_impl.h", "Makefile")]
     if (not os.path.exists(RESTATEMENT_SO)
             or any(os.path.getmtime(s) > os.path.getmtime(RESTATEMENT_SO) for s in src)):
         subprocess.check_call(["make", "-s", "-C", HERE, "restatement"])
@@ -74,10 +76,60 @@ class InterpResult:
 
 
 class Restatement:
-    """The C restatement of the interpolation decomposition."""
+    """The C restatements: the interpolation decomposition, and the 1-D Lorenzo + Huffman path."""
 
     def __init__(self, path: str | None = None):
         self.lib = ctypes.CDLL(path or ensure_restatement())
+        for name in ("oracle_lorenzo_payload_f32", "oracle_lorenzo_payload_f64", "oracle_lorenzo_decode_f32",
+                     "oracle_lorenzo_decode_f64", "oracle_huffman_encode", "oracle_huffman_decode"):
+            getattr(self.lib, name).restype = ctypes.c_longlong
+
+    def lorenzo_payload(self, x: np.ndarray, eb: float, radius: int = 32768, block: int = 5):
+        """(payload, reconstruction) of the 1-D blockwise Lorenzo path: the bytes the reference
+        hands to its trailing zstd stage (FalconsGenericCompressor.hpp:64-81)."""
+        x = np.ascontiguousarray(x).ravel()
+        cap = 4096 + x.size * (x.itemsize + 8) + 2 * 65540
+        out = np.empty(cap, np.uint8)
+        recon = np.empty_like(x)
+        ct = _ctype(x.dtype)
+        n = getattr(self.lib, f"oracle_lorenzo_payload_{_sfx(x.dtype)}")(
+            _ptr(x, ct), ctypes.c_size_t(x.size), ctypes.c_double(eb), ctypes.c_int(radius), ctypes.c_int(block),
+            _ptr(out, ctypes.c_uint8), ctypes.c_size_t(cap), _ptr(recon, ct))
+        if n < 0:
+            raise RuntimeError(f"oracle lorenzo payload failed: {n}")
+        return out[:n].tobytes(), recon
+
+    def lorenzo_decode(self, payload: bytes, n: int, dtype, block: int = 5) -> np.ndarray:
+        buf = np.frombuffer(payload, np.uint8)
+        out = np.empty(n, dtype)
+        used = getattr(self.lib, f"oracle_lorenzo_decode_{_sfx(dtype)}")(
+            _ptr(buf, ctypes.c_uint8), ctypes.c_size_t(len(payload)), ctypes.c_size_t(n), ctypes.c_int(block),
+            _ptr(out, _ctype(dtype)))
+        if used < 0:
+            raise ValueError(f"oracle lorenzo decode failed: {used}")
+        if used != len(payload):
+            raise ValueError(f"oracle lorenzo decode: {len(payload) - used} trailing bytes")
+        return out
+
+    def huffman_encode(self, sym: np.ndarray) -> bytes:
+        """One Huffman record (HuffmanEncoder<int>::save + encode) of symbols in [0, 65536)."""
+        sym = np.ascontiguousarray(sym, np.int32)
+        cap = 64 + 2 * 65540 + sym.size * 5
+        out = np.empty(cap, np.uint8)
+        n = self.lib.oracle_huffman_encode(_ptr(sym, ctypes.c_int32), ctypes.c_size_t(sym.size),
+                                           _ptr(out, ctypes.c_uint8), ctypes.c_size_t(cap))
+        if n < 0:
+            raise RuntimeError(f"oracle huffman encode failed: {n}")
+        return out[:n].tobytes()
+
+    def huffman_decode(self, rec: bytes, n: int) -> np.ndarray:
+        buf = np.frombuffer(rec, np.uint8)
+        out = np.empty(max(n, 1), np.int32)
+        used = self.lib.oracle_huffman_decode(_ptr(buf, ctypes.c_uint8), ctypes.c_size_t(len(rec)), ctypes.c_size_t(n),
+                                              _ptr(out, ctypes.c_int32))
+        if used < 0:
+            raise ValueError(f"oracle huffman decode failed: {used}")
+        return out[:n]
 
     def _call(self, name, *args):
         rc = getattr(self.lib, name)(*args)
@@ -137,6 +189,29 @@ def ref_conf(algo=ALGO_INTERP, eb_mode=EB_ABS, abs_eb=1e-3, rel_eb=0.0, interp=I
     """A reference Config with the defaults of include/Falcons/utils/Config.hpp:482-511."""
     return RefConf(algo, eb_mode, abs_eb, rel_eb, psnr, l2, interp, direction, anchor, int(openmp), alpha, beta,
                    65536, 1, 0, 1, 0, 0)
+
+
+def lorenzo_ref_conf(abs_eb: float, quantbin: int = 65536) -> RefConf:
+    """The Config the interpolation tuner hands to the 1-D Lorenzo path
+    (api/impl/FalconsAlgoInterp.hpp:479-490): Lorenzo orders 1 and 2, no regression, block 5."""
+    c = ref_conf(ALGO_LORENZO_REG, EB_ABS, abs_eb)
+    c.lorenzo, c.lorenzo2, c.regression, c.regression2, c.blockSize = 1, 1, 0, 0, 5
+    c.quantbinCnt = quantbin
+    return c
+
+
+ZSTD_MAGIC = b"\x28\xb5\x2f\xfd"
+
+
+def lossless_section(stream: bytes, max_header: int = 4096) -> int:
+    """Offset of the Lossless_zstd section ([u64 raw length][zstd frame],
+    lossless/Lossless_zstd.hpp:29-45) after a stream's Config header."""
+    for h in range(0, min(max_header, len(stream) - 12)):
+        if stream[h + 8:h + 12] == ZSTD_MAGIC:
+            raw = int.from_bytes(stream[h:h + 8], "little")
+            if 0 < raw < (1 << 40):
+                return h
+    raise ValueError("no zstd section found")
 
 
 def reference_available(omp: bool = False) -> bool:
@@ -244,6 +319,35 @@ class Reference:
         if n < 0:
             self._err("ref rlefse decode")
         return out[:n_codes].copy()
+
+    def lorenzo_payload(self, x: np.ndarray, eb: float, quantbin: int = 65536):
+        """(payload, buffer after compress) of the reference's 1-D blockwise Lorenzo path, stage by
+        stage: the bytes FalconsGenericCompressor hands to zstd, without the dispatcher's lossless
+        choice.  The path compresses a padded copy (utils/BlockwiseIterator.hpp:202-221), so the
+        buffer comes back unchanged; the reconstruction is lorenzo_decode's."""
+        x = np.ascontiguousarray(x).ravel()
+        cap = 4096 + x.size * (x.itemsize + 8) + 2 * 65540
+        out = np.empty(cap, np.uint8)
+        after = np.empty_like(x)
+        fn = getattr(self.lib, f"ref_lorenzo_payload_{_sfx(x.dtype)}")
+        fn.restype = ctypes.c_longlong
+        ct = _ctype(x.dtype)
+        n = fn(_ptr(x, ct), ctypes.c_size_t(x.size), ctypes.c_double(eb), ctypes.c_int(quantbin),
+               _ptr(out, ctypes.c_uint8), ctypes.c_size_t(cap), _ptr(after, ct))
+        if n < 0:
+            self._err("ref lorenzo payload")
+        return out[:n].tobytes(), after
+
+    def lorenzo_decode(self, payload: bytes, n: int, dtype) -> np.ndarray:
+        buf = np.frombuffer(payload, np.uint8)
+        out = np.empty(n, dtype)
+        fn = getattr(self.lib, f"ref_lorenzo_decode_{_sfx(dtype)}")
+        fn.restype = ctypes.c_longlong
+        used = fn(_ptr(buf, ctypes.c_uint8), ctypes.c_size_t(len(payload)), ctypes.c_size_t(n),
+                  _ptr(out, _ctype(dtype)))
+        if used < 0:
+            self._err("ref lorenzo decode")
+        return out
 
     def zstd_compress(self, raw: bytes) -> bytes:
         src = np.frombuffer(raw, np.uint8)

@@ -13,6 +13,11 @@
 //   ref_interp_decompress_<t>   decomposition/InterpolationDecomposition.hpp:48
 //   ref_rlefse_encode/decode    encoder/RleFseEncoder.hpp:850-1079
 //   ref_zstd_compress/decompress lossless/Lossless_zstd.hpp:29-78
+//   ref_lorenzo_payload_<t>     the pre-zstd payload of the 1-D blockwise Lorenzo path as the
+//                               tuner configures it (api/impl/FalconsAlgoInterp.hpp:229-262,
+//                               479-490; compressor/FalconsGenericCompressor.hpp:64-81), without
+//                               the dispatcher's choice between it and a lossless stream
+//   ref_lorenzo_decode_<t>      its decoder (FalconsGenericCompressor.hpp decompress steps)
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -312,5 +317,106 @@ long long ref_zstd_decompress(const uint8_t *src, size_t n, uint8_t *dst, size_t
         g_err = e.what();
         return -1;
     }
+}
+}
+
+// ---- the 1-D blockwise Lorenzo path, stage by stage
+template <class T>
+static auto lorenzo_decomposition(const Config &conf) {
+    std::vector<std::shared_ptr<concepts::PredictorInterface<T, 1>>> predictors;
+    predictors.push_back(std::make_shared<LorenzoPredictor<T, 1, 1>>(conf.absErrorBound));
+    predictors.push_back(std::make_shared<LorenzoPredictor<T, 1, 2>>(conf.absErrorBound));
+    return make_decomposition_blockwise<T, 1>(conf, ComposedPredictor<T, 1>(predictors),
+                                              LinearQuantizer<T>(conf.absErrorBound, conf.quantbinCnt / 2));
+}
+
+template <class T>
+static Config lorenzo_conf(size_t n, double eb, int quantbin) {
+    Config conf(n);
+    conf.cmprAlgo = ALGO_LORENZO_REG;
+    conf.errorBoundMode = EB_ABS;
+    conf.absErrorBound = eb;
+    conf.lorenzo = true;
+    conf.lorenzo2 = true;
+    conf.regression = false;
+    conf.regression2 = false;
+    conf.openmp = false;
+    conf.blockSize = 5;
+    conf.quantbinCnt = quantbin;
+    return conf;
+}
+
+template <class T>
+static long long do_lorenzo_payload(const T *x, size_t n, double eb, int quantbin, uint8_t *out, size_t cap,
+                                    T *after) {
+    try {
+        Config conf = lorenzo_conf<T>(n, eb, quantbin);
+        auto dec = lorenzo_decomposition<T>(conf);
+        std::vector<T> work(x, x + n);
+        auto [q, nq] = dec.compress(conf, work.data());
+        std::vector<uchar> buf(std::max<size_t>(4096, 64 + nq * (sizeof(T) + 8) + 2 * 65540));
+        uchar *p = buf.data();
+        dec.save(p);
+        write<uint64_t>(nq, p);
+        HuffmanEncoder<int> enc;
+        enc.preprocess_encode(q, nq, dec.get_out_range().second);
+        enc.save(p);
+        enc.encode(q, nq, p);
+        enc.postprocess_encode();
+        delete[] q;
+        const size_t len = p - buf.data();
+        if (len > cap) {
+            g_err = "capacity";
+            return -1;
+        }
+        memcpy(out, buf.data(), len);
+        if (after) memcpy(after, work.data(), n * sizeof(T));  // the input buffer after compress
+        return static_cast<long long>(len);
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+template <class T>
+static long long do_lorenzo_decode(const uint8_t *in, size_t len, size_t n, T *out) {
+    try {
+        Config conf = lorenzo_conf<T>(n, 0.0, 65536);
+        LinearQuantizer<T> quantizer;
+        std::vector<std::shared_ptr<concepts::PredictorInterface<T, 1>>> predictors;
+        predictors.push_back(std::make_shared<LorenzoPredictor<T, 1, 1>>());
+        predictors.push_back(std::make_shared<LorenzoPredictor<T, 1, 2>>());
+        auto dec = make_decomposition_blockwise<T, 1>(conf, ComposedPredictor<T, 1>(predictors), quantizer);
+        const uchar *p = in;
+        size_t rem = len;
+        dec.load(p, rem);
+        uint64_t nq = 0;
+        read(nq, p, rem);
+        if (nq != n) throw std::invalid_argument("code count");
+        HuffmanEncoder<int> enc;
+        enc.load(p, rem);
+        int *q = enc.decode(p, nq);
+        enc.postprocess_decode();
+        dec.decompress(conf, q, out);
+        delete[] q;
+        return static_cast<long long>(p - in);
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+extern "C" {
+long long ref_lorenzo_payload_f32(const float *x, size_t n, double eb, int qb, uint8_t *o, size_t cap, float *r) {
+    return do_lorenzo_payload<float>(x, n, eb, qb, o, cap, r);
+}
+long long ref_lorenzo_payload_f64(const double *x, size_t n, double eb, int qb, uint8_t *o, size_t cap, double *r) {
+    return do_lorenzo_payload<double>(x, n, eb, qb, o, cap, r);
+}
+long long ref_lorenzo_decode_f32(const uint8_t *in, size_t len, size_t n, float *out) {
+    return do_lorenzo_decode<float>(in, len, n, out);
+}
+long long ref_lorenzo_decode_f64(const uint8_t *in, size_t len, size_t n, double *out) {
+    return do_lorenzo_decode<double>(in, len, n, out);
 }
 }

@@ -1,7 +1,8 @@
 """Generates the golden fixtures of tests/golden from the reference build (oracle/_ref).
 
 Run from the repository root where the reference sources are available:
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py            (every fixture)
+    make -C oracle ref && python tests/golden/make_golden.py lorenzo    (the 1-D Lorenzo ones only)
 Each case stores its seeded input, so the fixtures do not depend on the generators.
 """
 import os
@@ -45,8 +46,51 @@ STREAM_CASES = [
 ]
 
 
+LORENZO_CASES = [
+    # name, n, dtype, kind, eb (absolute), quantbinCnt
+    ("walk_f32", 3001, np.float32, "walk", 1e-2, 65536),
+    ("spiky_f64", 1237, np.float64, "spikes", 1e-6, 65536),
+    ("const_f32", 17, np.float32, "const", 1e-3, 65536),
+    ("sine_f32_q16384", 2003, np.float32, "sine", 1e-4, 16384),
+    ("sine_f64_stream", 6000, np.float64, "sine", 1e-4, 65536),
+]
+
+
+def lorenzo_series(kind, n, dtype, seed):
+    rng = np.random.default_rng(seed)
+    t = np.arange(n, dtype=np.float64)
+    if kind == "walk":
+        x = np.cumsum(rng.normal(size=n))
+    elif kind == "spikes":
+        x = np.sin(0.05 * t) + 1e-6 * rng.normal(size=n)
+        x[rng.random(n) < 0.02] = 1e20
+    elif kind == "const":
+        x = np.zeros(n)
+    else:
+        x = 10 * np.sin(0.01 * t) + 1e-3 * rng.normal(size=n)
+    return x.astype(dtype)
+
+
+def lorenzo_fixtures(out):
+    """The 1-D blockwise Lorenzo path: input, the payload before zstd, the reconstruction, and the
+    whole reference stream."""
+    for name, n, dt, kind, eb, qb in LORENZO_CASES:
+        x = lorenzo_series(kind, n, dt, len(name))
+        payload, _ = R.lorenzo_payload(x, eb, qb)
+        recon = R.lorenzo_decode(payload, n, dt)
+        stream = R.compress(x, oracle.lorenzo_ref_conf(eb, qb))
+        np.savez_compressed(os.path.join(HERE, f"lorenzo_{name}.npz"), x=x, eb=eb, radius=qb // 2, block=5,
+                            payload=np.frombuffer(payload, np.uint8), recon=recon,
+                            stream=np.frombuffer(stream, np.uint8))
+        out["lorenzo_" + name] = len(payload)
+
+
 def main():
     out = {}
+    if sys.argv[1:] == ["lorenzo"]:
+        lorenzo_fixtures(out)
+        print(out)
+        return
     for name, shape, dt, algo, d, a, b, rel in INTERP_CASES:
         x = field(shape, dt, len(name))
         eb = rel * float(x.max() - x.min())
@@ -70,6 +114,7 @@ def main():
         enc = R.rlefse_encode(q)
         np.savez_compressed(os.path.join(HERE, f"rlefse_{name}.npz"), codes=q, payload=np.frombuffer(enc, np.uint8))
         out["rlefse_" + name] = len(enc)
+    lorenzo_fixtures(out)
     print(out)
 
 
