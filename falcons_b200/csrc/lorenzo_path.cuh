@@ -1,0 +1,21 @@
+// Decode entry of the 1-D blockwise Lorenzo + Huffman path (lorenzo.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/falcons_b200.h"
+#include "assemble.cuh"
+
+namespace fb2 {
+
+// Whether a stream's Config selects the Lorenzo path this build decodes: a 1-D field, Lorenzo
+// order 1 and / or 2 (composed per block when both are on), no regression predictor.
+bool lorenzo_stream_supported(const falcons_config &c);
+
+// Decodes the logical payload (host view `view` for its headers, device copy d_flat for its bulk)
+// into d_out (c.num values); throws std::invalid_argument on a malformed payload.
+template <class T>
+void lorenzo_decompress(const falcons_config &c, const ByteView &view, const uint8_t *d_flat, T *d_out,
+                        cudaStream_t st);
+
+}  // namespace fb2

@@ -19,6 +19,7 @@
 #include "assemble.cuh"
 #include "entropy.cuh"
 #include "interp.cuh"
+#include "lorenzo_path.cuh"
 #include "pipeline.cuh"
 #include "stream.hpp"
 #include "tuner.cuh"
@@ -244,6 +245,10 @@ void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_ou
         if (L != c.num * sizeof(T)) throw std::runtime_error("Decompressed data size does not match the original data size");
         FB2_CUDA(cudaMemcpyAsync(d_out, d_flat, L, cudaMemcpyDeviceToDevice, st));
         FB2_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
+    if (c.cmprAlgo == ALGO_LORENZO_REG) {  // FalconsDispatcher.hpp:147-148
+        lorenzo_decompress<T>(c, view, d_flat, d_out, st);
         return;
     }
     if (c.cmprAlgo != ALGO_INTERP)

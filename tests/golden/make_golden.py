@@ -72,16 +72,18 @@ def lorenzo_series(kind, n, dtype, seed):
 
 
 def lorenzo_fixtures(out):
-    """The 1-D blockwise Lorenzo path: input, the payload before zstd, the reconstruction, and the
-    whole reference stream."""
+    """The 1-D blockwise Lorenzo path: input, the payload before zstd, its reconstruction, the
+    whole reference stream and the reference's decode of it (the dispatcher may store tiny or
+    incompressible series losslessly)."""
     for name, n, dt, kind, eb, qb in LORENZO_CASES:
         x = lorenzo_series(kind, n, dt, len(name))
         payload, _ = R.lorenzo_payload(x, eb, qb)
         recon = R.lorenzo_decode(payload, n, dt)
         stream = R.compress(x, oracle.lorenzo_ref_conf(eb, qb))
+        stream_recon = R.decompress(stream, dt, n).ravel()
         np.savez_compressed(os.path.join(HERE, f"lorenzo_{name}.npz"), x=x, eb=eb, radius=qb // 2, block=5,
                             payload=np.frombuffer(payload, np.uint8), recon=recon,
-                            stream=np.frombuffer(stream, np.uint8))
+                            stream=np.frombuffer(stream, np.uint8), stream_recon=stream_recon)
         out["lorenzo_" + name] = len(payload)
 
 
