@@ -1,4 +1,4 @@
-// Decode entry of the 1-D blockwise Lorenzo + Huffman path (lorenzo.cu).
+// Entries of the 1-D blockwise Lorenzo + Huffman path (lorenzo.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -11,6 +11,11 @@ namespace fb2 {
 // Whether a stream's Config selects the Lorenzo path this build decodes: a 1-D field, Lorenzo
 // order 1 and / or 2 (composed per block when both are on), no regression predictor.
 bool lorenzo_stream_supported(const falcons_config &c);
+
+// Writes [u64 payload bytes][zstd raw-block frame of the payload] of field d_x (c.num values, not
+// modified) to d_pay; returns the bytes written; throws std::length_error past pcap.
+template <class T>
+size_t lorenzo_compress(const falcons_config &c, const T *d_x, uint8_t *d_pay, size_t pcap, cudaStream_t st);
 
 // Decodes the logical payload (host view `view` for its headers, device copy d_flat for its bulk)
 // into d_out (c.num values); throws std::invalid_argument on a malformed payload.

@@ -107,15 +107,25 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     resolve_error_bound<T>(ctx, c, d_x, st);
     tr.mark("error bound resolved");
     if (c.absErrorBound == 0) c.cmprAlgo = ALGO_LOSSLESS;
-    if (c.cmprAlgo == ALGO_LORENZO_REG || c.cmprAlgo == ALGO_NOPRED)
-        throw std::invalid_argument("unsupported on GPU build: ALGO_LORENZO_REG and ALGO_NOPRED are not implemented");
+    if (c.cmprAlgo == ALGO_NOPRED) throw std::invalid_argument("unsupported on GPU build: ALGO_NOPRED is not implemented");
+    if (c.cmprAlgo == ALGO_LORENZO_REG && !lorenzo_stream_supported(c))
+        throw std::invalid_argument(
+            "unsupported on GPU build: ALGO_LORENZO_REG other than 1-D Lorenzo (orders 1 and / or 2, no regression)");
     const size_t hs = config_size(c);
     if (cap < hs + 16) throw std::invalid_argument("The buffer for compressed data is not large enough.");
     uint8_t *d_pay = d_out + hs;
     const size_t pcap = cap - hs;
     size_t payload = 0;
     const size_t raw_bytes = (size_t)c.num * sizeof(T);
-    if (c.cmprAlgo != ALGO_LOSSLESS) {
+    if (c.cmprAlgo == ALGO_LORENZO_REG) {
+        try {
+            // FalconsAlgoLorenzoReg.hpp:67-76 (the 1-D blockwise Lorenzo path; the field is not modified)
+            payload = lorenzo_compress<T>(c, d_x, d_pay, pcap, st);
+            tr.mark("payload assembled");
+        } catch (std::length_error &) {
+            c.cmprAlgo = ALGO_LOSSLESS;  // FalconsDispatcher.hpp:100-118
+        }
+    } else if (c.cmprAlgo != ALGO_LOSSLESS) {
         try {
             if (c.interpAnchorStride < 0) c.interpAnchorStride = (int)default_anchor(c.N);
             if (c.cmprAlgo == ALGO_INTERP_LORENZO) {

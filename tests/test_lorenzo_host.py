@@ -42,6 +42,19 @@ def host_decoder():
                 ctypes.c_size_t(n), block, l1, l2, out.ctypes.data_as(ctypes.POINTER(ct)))
         return rc, out
 
+    def encode(x, eb, radius=32768, block=5, l1=1, l2=1):
+        x = np.ascontiguousarray(x)
+        cap = 4096 + x.size * (x.itemsize + 8) + 2 * 65540
+        out = np.empty(cap, np.uint8)
+        ct = ctypes.c_float if x.dtype == np.float32 else ctypes.c_double
+        fn = lib.lzh_encode_f32 if x.dtype == np.float32 else lib.lzh_encode_f64
+        fn.restype = ctypes.c_longlong
+        n = fn(x.ctypes.data_as(ctypes.POINTER(ct)), ctypes.c_size_t(x.size), ctypes.c_double(eb), radius, block,
+               l1, l2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.c_size_t(cap))
+        assert n >= 0, n
+        return out[:n].tobytes()
+
+    decode.encode = encode
     return decode
 
 
@@ -53,6 +66,34 @@ def test_decoder_matches_reference(host_decoder, reference, kind, n, dtype, eb, 
     rc, y = host_decoder(payload, n, dtype)
     assert rc == 0
     assert same_bits(y, reference.lorenzo_decode(payload, n, dtype))
+
+
+@pytest.mark.parametrize("kind,n,dtype,eb,quantbin", CASES,
+                         ids=[f"{c[0]}-{c[1]}-{np.dtype(c[2]).name}-{c[3]:g}-{c[4]}" for c in CASES])
+def test_encoder_matches_reference(host_decoder, reference, kind, n, dtype, eb, quantbin):
+    """The encoder functions (blockwise quantization, Huffman lengths in the reference's heap
+    order, canonical codes, the table flag, packing) give the reference's payload bytes."""
+    x = series(kind, n, dtype, seed=n)
+    payload, _ = reference.lorenzo_payload(x, eb, quantbin)
+    assert host_decoder.encode(x, eb, quantbin // 2) == payload
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "lorenzo_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_encoder_matches_golden(host_decoder, path):
+    g = np.load(path)
+    assert host_decoder.encode(g["x"], float(g["eb"]), int(g["radius"]), int(g["block"])) == g["payload"].tobytes()
+
+
+@pytest.mark.parametrize("l1,l2", [(1, 0), (0, 1)])
+def test_single_predictor_encoder(host_decoder, reference, l1, l2):
+    x = series("sine", 20000, np.float32, 11)
+    conf = oracle.lorenzo_ref_conf(1e-3)
+    conf.lorenzo, conf.lorenzo2 = l1, l2
+    stream = reference.compress(x, conf)
+    h = oracle.lossless_section(stream)
+    payload = reference.zstd_decompress(stream[h:], int.from_bytes(stream[h:h + 8], "little"))
+    assert host_decoder.encode(x, 1e-3, 32768, 5, l1, l2) == payload
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "lorenzo_*.npz"))),
