@@ -274,8 +274,9 @@ void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st)
             }
         }
     }
-    // N == 1 also trials the blockwise Lorenzo predictor (FalconsAlgoInterp.hpp:479-493); that
-    // predictor is not part of this build, so 1-D fields always keep interpolation.
+    // N == 1 also trials the blockwise Lorenzo predictor (FalconsAlgoInterp.hpp:479-493); its
+    // encoder is built (lorenzo.cu, for explicit ALGO_LORENZO_REG requests) but its trial here is
+    // not, so 1-D fields keep interpolation.
     c.cmprAlgo = ALGO_INTERP;
 }
 
