@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "lorenzo.cuh"
 #include "lorenzo_path.cuh"
+#include "stream.hpp"
 
 namespace fb2 {
 namespace {
@@ -56,6 +57,20 @@ __global__ void k_lz_quantize(const T *__restrict__ x, unsigned long long n, dou
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const int e = lz::quantize_blocks<T>(x, (size_t)n, eb, radius, block, composed, sel_all, codes, sel, unpred,
                                          (uint32_t)n, n_unpred);
+    if (e) atomicExch(err, 32 + e);
+}
+
+// The tuner's trial: B independent sample blocks of V points, one thread each (every block starts
+// from the two zero values before it, as each of the reference's per-block compress calls does).
+template <class T>
+__global__ void k_lz_quantize_many(const T *__restrict__ x, long long B, long long V, double eb, int radius,
+                                   int block, int32_t *__restrict__ codes, int32_t *__restrict__ sel,
+                                   T *__restrict__ unpred, uint32_t *__restrict__ n_unpred, int *__restrict__ err) {
+    const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const long long nblk = (V + block - 1) / block;
+    const int e = lz::quantize_blocks<T>(x + b * V, (size_t)V, eb, radius, block, 1, 0, codes + b * V, sel + b * nblk,
+                                         unpred + b * V, (uint32_t)V, n_unpred + b);
     if (e) atomicExch(err, 32 + e);
 }
 
@@ -160,6 +175,67 @@ void lorenzo_decompress(const falcons_config &c, const ByteView &view, const uin
     if (e[0]) throw std::invalid_argument("Invalid or corrupted Falcons Lorenzo payload");
 }
 
+namespace {
+
+// A Huffman record built on the device: its code lengths (device), packed bits (device) and the
+// header values the host writes.
+struct BuiltRecord {
+    const uint8_t *lens;
+    const uint8_t *packed;
+    uint32_t lo, ns;
+    int table;
+    unsigned long long nbytes;
+};
+
+// Builds the records of the symbol arrays syms[k] (device, counts[k] symbols each): histograms on
+// the grid, one code book per CTA, one packing thread per record.  Synchronizes the stream.
+std::vector<BuiltRecord> build_records(Pool &pool, const std::vector<const int32_t *> &syms,
+                                       const std::vector<size_t> &counts, int *d_err, cudaStream_t st) {
+    constexpr size_t kStates = 65538;
+    std::vector<BookJob> jobs;
+    for (size_t k = 0; k < syms.size(); k++) {
+        unsigned long long *hist = pool.get<unsigned long long>(65537);
+        FB2_CUDA(cudaMemsetAsync(hist, 0, 65537 * sizeof(unsigned long long), st));
+        k_lz_hist<<<grid_for((long long)counts[k], 256, 148 * 8), 256, 0, st>>>(
+            syms[k], (unsigned long long)counts[k], hist, d_err);
+        FB2_CHECK_LAUNCH();
+        jobs.push_back(BookJob{hist, (unsigned long long)counts[k], pool.get<lz::HuffNode>(2 * kStates),
+                               pool.get<int>(2 * kStates + 1), pool.get<uint8_t>(kStates),
+                               pool.get<uint32_t>(kStates), pool.get<unsigned long long>(4)});
+    }
+    BookJob *d_jobs = h2d(pool, jobs, st);
+    k_lz_book<<<(unsigned)jobs.size(), 32, 0, st>>>(d_jobs, (int)jobs.size(), d_err);
+    FB2_CHECK_LAUNCH();
+    std::vector<BuiltRecord> out;
+    for (size_t k = 0; k < jobs.size(); k++) {
+        const std::vector<unsigned long long> info = d2h(jobs[k].info, 4, st);
+        if (d2h(d_err, 1, st)[0]) throw std::runtime_error("Lorenzo encoding failed");
+        BuiltRecord r{jobs[k].lens, nullptr, (uint32_t)info[0], (uint32_t)info[1], (int)info[2], (info[3] + 7) / 8};
+        uint8_t *packed = pool.get<uint8_t>((size_t)r.nbytes + 16);
+        FB2_CUDA(cudaMemsetAsync(packed, 0, (size_t)r.nbytes + 16, st));
+        k_lz_pack<<<1, 32, 0, st>>>(syms[k], (unsigned long long)counts[k], r.lo, jobs[k].lens, jobs[k].codes,
+                                    packed);
+        FB2_CHECK_LAUNCH();
+        r.packed = packed;
+        out.push_back(r);
+    }
+    return out;
+}
+
+// A record's header (HuffmanEncoder::save) and its bits (HuffmanEncoder::encode).
+void record_header(Assembler &as, const BuiltRecord &r) {
+    as.val<int32_t>((int32_t)(((uint32_t)r.table << 31) | r.lo));
+    const uint8_t be[4] = {(uint8_t)(r.ns >> 24), (uint8_t)(r.ns >> 16), (uint8_t)(r.ns >> 8), (uint8_t)r.ns};
+    as.bytes(be, 4);
+    as.dev(r.lens, r.ns);
+}
+void record_bits(Assembler &as, const BuiltRecord &r) {
+    as.val<uint64_t>(r.nbytes);
+    as.dev(r.packed, (size_t)r.nbytes);
+}
+
+}  // namespace
+
 template <class T>
 size_t lorenzo_compress(const falcons_config &c, const T *d_x, uint8_t *d_pay, size_t pcap, cudaStream_t st) {
     if (!lorenzo_stream_supported(c))
@@ -183,73 +259,89 @@ size_t lorenzo_compress(const falcons_config &c, const T *d_x, uint8_t *d_pay, s
                                        c.lorenzo2 && !c.lorenzo ? 1 : 0, codes, sel, unpred, d_nu, d_err);
     FB2_CHECK_LAUNCH();
     // the records: the selection (composed predictors only), then the codes
-    struct Rec {
-        const int32_t *sym;
-        size_t count;
-        BookJob job;
-    };
-    std::vector<Rec> recs;
-    auto add = [&](const int32_t *sym, size_t count) {
-        constexpr size_t kStates = 65538;
-        Rec r{sym, count, {}};
-        unsigned long long *hist = pool.get<unsigned long long>(65537);
-        FB2_CUDA(cudaMemsetAsync(hist, 0, 65537 * sizeof(unsigned long long), st));
-        k_lz_hist<<<grid_for((long long)count, 256, 148 * 8), 256, 0, st>>>(sym, (unsigned long long)count, hist,
-                                                                            d_err);
-        FB2_CHECK_LAUNCH();
-        r.job = BookJob{hist, (unsigned long long)count, pool.get<lz::HuffNode>(2 * kStates),
-                        pool.get<int>(2 * kStates + 1), pool.get<uint8_t>(kStates), pool.get<uint32_t>(kStates),
-                        pool.get<unsigned long long>(4)};
-        recs.push_back(r);
-    };
-    if (composed && nblocks) add(sel, nblocks);
-    add(codes, n);
-    std::vector<BookJob> jobs;
-    for (const Rec &r : recs) jobs.push_back(r.job);
-    BookJob *d_jobs = h2d(pool, jobs, st);
-    k_lz_book<<<(unsigned)jobs.size(), 32, 0, st>>>(d_jobs, (int)jobs.size(), d_err);
-    FB2_CHECK_LAUNCH();
-    std::vector<std::vector<unsigned long long>> info;
-    for (const Rec &r : recs) info.push_back(d2h(r.job.info, 4, st));
-    const std::vector<uint32_t> h_nu = d2h(d_nu, 1, st);
-    const std::vector<int> h_err = d2h(d_err, 1, st);
-    if (h_err[0]) throw std::runtime_error("Lorenzo encoding failed");
+    std::vector<const int32_t *> syms;
+    std::vector<size_t> counts;
+    if (composed && nblocks) {
+        syms.push_back(sel);
+        counts.push_back(nblocks);
+    }
+    syms.push_back(codes);
+    counts.push_back(n);
+    const std::vector<BuiltRecord> rec = build_records(pool, syms, counts, d_err, st);
+    const uint32_t nu = d2h(d_nu, 1, st)[0];
     tr.mark("code books built");
-    // payload pieces
+    // FalconsGenericCompressor.hpp:64-81: decomposition (selection, quantizer), code count, codes
     Assembler as;
     as.with_index = false;
-    auto record = [&](size_t k) {
-        const Rec &r = recs[k];
-        const unsigned long long lo = info[k][0], ns = info[k][1], table = info[k][2], bits = info[k][3];
-        const unsigned long long nbytes = (bits + 7) / 8;
-        uint8_t *packed = pool.get<uint8_t>((size_t)nbytes + 16);
-        FB2_CUDA(cudaMemsetAsync(packed, 0, (size_t)nbytes + 16, st));
-        k_lz_pack<<<1, 32, 0, st>>>(r.sym, (unsigned long long)r.count, (uint32_t)lo, r.job.lens, r.job.codes, packed);
-        FB2_CHECK_LAUNCH();
-        as.val<int32_t>((int32_t)(((uint32_t)table << 31) | (uint32_t)lo));
-        const uint8_t be[4] = {(uint8_t)(ns >> 24), (uint8_t)(ns >> 16), (uint8_t)(ns >> 8), (uint8_t)ns};
-        as.bytes(be, 4);
-        as.dev(r.job.lens, (size_t)ns);
-        as.val<uint64_t>(nbytes);
-        as.dev(packed, (size_t)nbytes);
-    };
-    size_t k = 0;
     if (composed) {
         as.val<uint64_t>((uint64_t)nblocks);
-        if (nblocks) record(k++);
+        if (nblocks) {
+            record_header(as, rec[0]);
+            record_bits(as, rec[0]);
+        }
     }
     as.val<uint8_t>(0b10);  // LinearQuantizer::save
     as.val<double>(eb);
     as.val<int32_t>(radius);
-    as.val<int32_t>((int32_t)h_nu[0]);
-    as.dev(unpred, (size_t)h_nu[0] * sizeof(T));
+    as.val<int32_t>((int32_t)nu);
+    as.dev(unpred, (size_t)nu * sizeof(T));
     as.val<uint64_t>((uint64_t)n);
-    record(k);
+    record_header(as, rec.back());
+    record_bits(as, rec.back());
     if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
     const size_t out = as.run_framed(pool, d_pay, st);
     tr.mark("payload assembled");
     return out;
 }
+
+template <class T>
+double lorenzo_trial_ratio(const T *d_blocks, long long B, long long V, double eb, int quantbin, cudaStream_t st) {
+    Trace tr("lorenzo trial");
+    constexpr int kBlock = 5;
+    const long long nblk = (V + kBlock - 1) / kBlock;
+    const int radius = quantbin / 2;
+    Pool pool(st);
+    int32_t *codes = pool.get<int32_t>((size_t)(B * V) + 1);
+    int32_t *sel = pool.get<int32_t>((size_t)(B * nblk) + 1);
+    T *unpred = pool.get<T>((size_t)(B * V) + 1);
+    uint32_t *d_nu = pool.get<uint32_t>((size_t)B);
+    int *d_err = pool.get<int>(1);
+    FB2_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    k_lz_quantize_many<T><<<(unsigned)((B + 31) / 32), 32, 0, st>>>(d_blocks, B, V, eb, radius, kBlock, codes, sel,
+                                                                    unpred, d_nu, d_err);
+    FB2_CHECK_LAUNCH();
+    const std::vector<BuiltRecord> rec =
+        build_records(pool, {sel, codes}, {(size_t)(B * nblk), (size_t)(B * V)}, d_err, st);
+    const std::vector<uint32_t> nu = d2h(d_nu, (size_t)B, st);
+    unsigned long long nu_all = 0;
+    for (uint32_t u : nu) nu_all += u;
+    // lorenzo_compress_test (FalconsAlgoInterp.hpp:229-262): the decomposition's save (the
+    // selection of all blocks, the quantizer with the unpredictable values of all blocks), the
+    // encoder's save, the code count, the encoder's bits; then zstd
+    Assembler as;
+    as.with_index = false;
+    as.val<uint64_t>((uint64_t)(B * nblk));
+    record_header(as, rec[0]);
+    record_bits(as, rec[0]);
+    as.val<uint8_t>(0b10);
+    as.val<double>(eb);
+    as.val<int32_t>(radius);
+    as.val<int32_t>((int32_t)nu_all);
+    for (long long b = 0; b < B; b++) as.dev(unpred + b * V, (size_t)nu[b] * sizeof(T));
+    record_header(as, rec[1]);
+    as.val<uint64_t>((uint64_t)(B * V));
+    record_bits(as, rec[1]);
+    uint8_t *d_buf = pool.get<uint8_t>((size_t)as.pos + 16);
+    as.run(pool, d_buf, st);
+    const std::vector<uint8_t> h = d2h(d_buf, (size_t)as.pos, st);
+    std::vector<uint8_t> z(zstd_compress_bound(h.size()) + 16);
+    const size_t zs = zstd_compress(h.data(), h.size(), z.data(), z.size(), 3) + sizeof(size_t);
+    tr.mark("trial compressed");
+    return (double)((size_t)V * (size_t)B * sizeof(T)) / (double)zs;
+}
+
+template double lorenzo_trial_ratio<float>(const float *, long long, long long, double, int, cudaStream_t);
+template double lorenzo_trial_ratio<double>(const double *, long long, long long, double, int, cudaStream_t);
 
 template size_t lorenzo_compress<float>(const falcons_config &, const float *, uint8_t *, size_t, cudaStream_t);
 template size_t lorenzo_compress<double>(const falcons_config &, const double *, uint8_t *, size_t, cudaStream_t);

@@ -117,6 +117,12 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     const size_t pcap = cap - hs;
     size_t payload = 0;
     const size_t raw_bytes = (size_t)c.num * sizeof(T);
+    if (c.cmprAlgo == ALGO_INTERP_LORENZO) {
+        if (c.interpAnchorStride < 0) c.interpAnchorStride = (int)default_anchor(c.N);
+        // sets interpAlgo/direction/alpha/beta and cmprAlgo = ALGO_INTERP, or (1-D fields) the
+        // Lorenzo path's Config with cmprAlgo = ALGO_LORENZO_REG
+        tune_interp<T>(ctx, c, d_x, st);
+    }
     if (c.cmprAlgo == ALGO_LORENZO_REG) {
         try {
             // FalconsAlgoLorenzoReg.hpp:67-76 (the 1-D blockwise Lorenzo path; the field is not modified)
@@ -128,9 +134,6 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     } else if (c.cmprAlgo != ALGO_LOSSLESS) {
         try {
             if (c.interpAnchorStride < 0) c.interpAnchorStride = (int)default_anchor(c.N);
-            if (c.cmprAlgo == ALGO_INTERP_LORENZO) {
-                tune_interp<T>(ctx, c, d_x, st);  // sets interpAlgo/direction/alpha/beta, cmprAlgo = ALGO_INTERP
-            }
             if (c.cmprAlgo != ALGO_INTERP)
                 throw std::invalid_argument("unsupported on GPU build: the tuner chose a non-interpolation algorithm");
             long long dims[4];

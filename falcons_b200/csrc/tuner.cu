@@ -14,6 +14,7 @@
 
 #include "assemble.cuh"
 #include "interp.cuh"
+#include "lorenzo_path.cuh"
 #include "stream.hpp"
 #include "tuner.cuh"
 
@@ -219,6 +220,7 @@ void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st)
     dim3 grid((unsigned)std::min<long long>((V + 255) / 256, 4096), (unsigned)B);
     k_cut_block<T><<<grid, 256, 0, st>>>(d_x, g, d_st, side, V, blocks);
     FB2_CHECK_LAUNCH();
+    const falcons_config lorenzo_base = c;  // FalconsAlgoInterp.hpp:340 (before the interpolation trials)
 
     InterpParams base;
     base.eb = c.absErrorBound;
@@ -274,9 +276,36 @@ void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st)
             }
         }
     }
-    // N == 1 also trials the blockwise Lorenzo predictor (FalconsAlgoInterp.hpp:479-493); its
-    // encoder is built (lorenzo.cu, for explicit ALGO_LORENZO_REG requests) but its trial here is
-    // not, so 1-D fields keep interpolation.
+    // N == 1 also trials the blockwise Lorenzo predictor (FalconsAlgoInterp.hpp:479-498) and keeps
+    // it when it beats interpolation by 10 % (both ratios below 50); below relErrorBound 1.01e-6 a
+    // ratio above 5 is retried with 16384 quantization bins, kept when 2 % better (:524-533).
+    if (N == 1 && best < 50) {
+        double lr = lorenzo_trial_ratio<T>(blocks, B, V, c.absErrorBound, c.quantbinCnt, st);
+        if (lr >= best * 1.1 && lr < 50) {
+            int qb = c.quantbinCnt;
+            if (c.relErrorBound < 1.01e-6 && lr > 5 && qb != 16384) {
+                const double r2 = lorenzo_trial_ratio<T>(blocks, B, V, c.absErrorBound, 16384, st);
+                if (r2 > lr * 1.02) {
+                    lr = r2;
+                    qb = 16384;
+                }
+            }
+            // the trial's Config (Lorenzo orders 1 and 2, no regression, serial) with the field's
+            // dims set back: Config::setDims resets the block size to 128 for 1-D and predDim to N
+            // (utils/Config.hpp:165-181), so the field is coded in blocks of 128, the trial's 5 not kept
+            c = lorenzo_base;
+            c.cmprAlgo = ALGO_LORENZO_REG;
+            c.lorenzo = 1;
+            c.lorenzo2 = 1;
+            c.regression = 0;
+            c.regression2 = 0;
+            c.openmp = 0;
+            c.quantbinCnt = qb;
+            c.blockSize = 128;
+            c.predDim = 1;
+            return;
+        }
+    }
     c.cmprAlgo = ALGO_INTERP;
 }
 

@@ -349,6 +349,22 @@ class Reference:
             self._err("ref lorenzo decode")
         return out
 
+    def lorenzo_trial(self, blocks: np.ndarray, eb: float, quantbin: int = 65536):
+        """(buffer before zstd, ratio) of the tuner's Lorenzo trial over sample blocks (rows of
+        `blocks`), as lorenzo_compress_test computes them."""
+        blocks = np.ascontiguousarray(blocks)
+        B, V = blocks.shape
+        cap = 4096 + blocks.size * (blocks.itemsize + 8) + 2 * 65540
+        out = np.empty(cap, np.uint8)
+        n = ctypes.c_longlong(0)
+        fn = getattr(self.lib, f"ref_lorenzo_trial_{_sfx(blocks.dtype)}")
+        fn.restype = ctypes.c_double
+        r = fn(_ptr(blocks, _ctype(blocks.dtype)), ctypes.c_size_t(B), ctypes.c_size_t(V), ctypes.c_double(eb),
+               ctypes.c_int(quantbin), _ptr(out, ctypes.c_uint8), ctypes.c_size_t(cap), ctypes.byref(n))
+        if r < 0:
+            self._err("ref lorenzo trial")
+        return out[:n.value].tobytes(), r
+
     def zstd_compress(self, raw: bytes) -> bytes:
         src = np.frombuffer(raw, np.uint8)
         cap = len(raw) + len(raw) // 128 + 1024

@@ -18,6 +18,9 @@
 //                               479-490; compressor/FalconsGenericCompressor.hpp:64-81), without
 //                               the dispatcher's choice between it and a lossless stream
 //   ref_lorenzo_decode_<t>      its decoder (FalconsGenericCompressor.hpp decompress steps)
+//   ref_lorenzo_trial_<t>       the interpolation tuner's Lorenzo trial over sample blocks
+//                               (lorenzo_compress_test, FalconsAlgoInterp.hpp:229-262): its buffer
+//                               before zstd, rebuilt stage by stage, and its own ratio
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -418,5 +421,57 @@ long long ref_lorenzo_decode_f32(const uint8_t *in, size_t len, size_t n, float 
 }
 long long ref_lorenzo_decode_f64(const uint8_t *in, size_t len, size_t n, double *out) {
     return do_lorenzo_decode<double>(in, len, n, out);
+}
+}
+
+template <class T>
+static double do_lorenzo_trial(const T *blocks, size_t B, size_t V, double eb, int quantbin, uint8_t *out, size_t cap,
+                               long long *out_len) {
+    try {
+        Config conf = lorenzo_conf<T>(V, eb, quantbin);
+        // the trial's buffer, stage by stage as lorenzo_compress_test writes it
+        auto dec = lorenzo_decomposition<T>(conf);
+        std::vector<int> total;
+        std::vector<std::vector<T>> sampled;
+        for (size_t b = 0; b < B; b++) {
+            std::vector<T> blk(blocks + b * V, blocks + (b + 1) * V);
+            sampled.push_back(blk);
+            auto [q, nq] = dec.compress(conf, blk.data());
+            total.insert(total.end(), q, q + nq);
+            delete[] q;
+        }
+        HuffmanEncoder<int> enc;
+        enc.preprocess_encode(total, conf.quantbinCnt);
+        std::vector<uchar> buf(std::max<size_t>(4096, 64 + total.size() * (sizeof(T) + 8) + 2 * 65540));
+        uchar *p = buf.data();
+        dec.save(p);
+        enc.save(p);
+        write<size_t>(total.size(), p);
+        enc.encode(total, p);
+        enc.postprocess_encode();
+        const size_t len = p - buf.data();
+        if (len > cap) {
+            g_err = "capacity";
+            return -1;
+        }
+        memcpy(out, buf.data(), len);
+        *out_len = (long long)len;
+        // and the reference's own ratio
+        std::vector<uchar> zbuf(std::max<size_t>(1 << 20, 4 * len + 65536));
+        return lorenzo_compress_test<T, 1>(sampled, conf, zbuf.data(), zbuf.size());
+    } catch (std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+extern "C" {
+double ref_lorenzo_trial_f32(const float *b, size_t B, size_t V, double eb, int qb, uint8_t *o, size_t cap,
+                             long long *len) {
+    return do_lorenzo_trial<float>(b, B, V, eb, qb, o, cap, len);
+}
+double ref_lorenzo_trial_f64(const double *b, size_t B, size_t V, double eb, int qb, uint8_t *o, size_t cap,
+                             long long *len) {
+    return do_lorenzo_trial<double>(b, B, V, eb, qb, o, cap, len);
 }
 }

@@ -87,10 +87,35 @@ def lorenzo_fixtures(out):
         out["lorenzo_" + name] = len(payload)
 
 
+TUNED_LORENZO_CASES = [
+    # name, n, dtype, eb (absolute): 1-D fields on which the reference's ALGO_INTERP_LORENZO tuner
+    # switches to the blockwise Lorenzo path (the last one with 16384 quantization bins)
+    ("spikes_f32", 20000, np.float32, 0.1),
+    ("spikes_f64", 20000, np.float64, 0.01),
+    ("spikes_f32_q16384", 50000, np.float32, 0.1),
+]
+
+
+def tuned_lorenzo_fixtures(out):
+    """The tuner's choice of the Lorenzo path: input and the reference's whole stream (its payload
+    is the stream's zstd section; its Config carries the chosen bins and block size)."""
+    for name, n, dt, eb in TUNED_LORENZO_CASES:
+        t = np.arange(n, dtype=np.float64)
+        rng = np.random.default_rng(n)
+        x = np.sin(0.05 * t)
+        x[rng.random(n) < 0.02] = 1e20
+        x = x.astype(dt)
+        stream = R.compress(x, oracle.ref_conf(algo=oracle.ALGO_INTERP_LORENZO, abs_eb=eb))
+        np.savez_compressed(os.path.join(HERE, f"tunedlz_{name}.npz"), x=x, eb=eb,
+                            stream=np.frombuffer(stream, np.uint8))
+        out["tunedlz_" + name] = len(stream)
+
+
 def main():
     out = {}
     if sys.argv[1:] == ["lorenzo"]:
         lorenzo_fixtures(out)
+        tuned_lorenzo_fixtures(out)
         print(out)
         return
     for name, shape, dt, algo, d, a, b, rel in INTERP_CASES:
@@ -117,6 +142,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"rlefse_{name}.npz"), codes=q, payload=np.frombuffer(enc, np.uint8))
         out["rlefse_" + name] = len(enc)
     lorenzo_fixtures(out)
+    tuned_lorenzo_fixtures(out)
     print(out)
 
 

@@ -60,8 +60,20 @@ struct Out {
     }
 };
 
-// One Huffman record of sym[0, n) (save, then encode) with the encoder functions of lorenzo.cuh.
+// A Huffman record of sym[0, n) with the encoder functions of lorenzo.cuh: its header
+// (HuffmanEncoder::save) into `head`, its bits (HuffmanEncoder::encode) into `bits`.
+int record_parts(Out &head, Out &bitsout, const int32_t *sym, size_t n);
+
+// One Huffman record of sym[0, n) (save, then encode).
 int record(Out &o, const int32_t *sym, size_t n) {
+    Out h, b;
+    const int e = record_parts(h, b, sym, n);
+    o.put(h.b.data(), h.b.size());
+    o.put(b.b.data(), b.b.size());
+    return e;
+}
+
+int record_parts(Out &o, Out &ob, const int32_t *sym, size_t n) {
     using namespace fb2::lz;
     std::vector<unsigned long long> hist(65536, 0);
     for (size_t i = 0; i < n; i++) {
@@ -88,11 +100,49 @@ int record(Out &o, const int32_t *sym, size_t n) {
     unsigned long long bits = 0;
     for (size_t i = 0; i < n; i++) bits += lens[sym[i] - lo];
     const unsigned long long nbytes = (bits + 7) / 8;
-    o.put(&nbytes, 8);
+    ob.put(&nbytes, 8);
     std::vector<uint8_t> packed(nbytes + 1, 0);
     huff_pack(sym, 0, n, lo, lens.data(), codes.data(), 0, packed.data());
-    o.put(packed.data(), nbytes);
+    ob.put(packed.data(), nbytes);
     return 0;
+}
+
+// The tuner's trial buffer over B blocks of V points in the layout lorenzo.cu's
+// lorenzo_trial_ratio writes: [u64 selections][selection record][quantizer header + the
+// unpredictable values of all blocks][codes record header][u64 codes][codes record bits].
+template <class T>
+long long trial(const T *blocks, size_t B, size_t V, double eb, int radius, uint8_t *out, size_t cap) {
+    using namespace fb2::lz;
+    const size_t nblk = (V + 4) / 5;
+    std::vector<int32_t> codes(B * V + 1), sel(B * nblk + 1);
+    std::vector<T> unpred(B * V + 1);
+    std::vector<uint32_t> nu(B, 0);
+    for (size_t b = 0; b < B; b++) {
+        const int e = quantize_blocks<T>(blocks + b * V, V, eb, radius, 5, 1, 0, codes.data() + b * V,
+                                         sel.data() + b * nblk, unpred.data() + b * V, (uint32_t)V, &nu[b]);
+        if (e) return -e;
+    }
+    Out o, ch, cb;
+    const uint64_t ns = B * nblk;
+    o.put(&ns, 8);
+    if (record(o, sel.data(), B * nblk)) return -30;
+    const uint8_t uid = 2;
+    const int32_t r = radius;
+    int32_t u = 0;
+    for (uint32_t v : nu) u += (int32_t)v;
+    o.put(&uid, 1);
+    o.put(&eb, 8);
+    o.put(&r, 4);
+    o.put(&u, 4);
+    for (size_t b = 0; b < B; b++) o.put(unpred.data() + b * V, nu[b] * sizeof(T));
+    if (record_parts(ch, cb, codes.data(), B * V)) return -31;
+    o.put(ch.b.data(), ch.b.size());
+    const uint64_t nc = B * V;
+    o.put(&nc, 8);
+    o.put(cb.b.data(), cb.b.size());
+    if (o.b.size() > cap) return -1;
+    memcpy(out, o.b.data(), o.b.size());
+    return (long long)o.b.size();
 }
 
 template <class T>
@@ -129,6 +179,12 @@ long long encode(const T *x, size_t n, double eb, int radius, int block, int l1,
 }  // namespace
 
 extern "C" {
+long long lzh_trial_f32(const float *b, size_t B, size_t V, double eb, int radius, uint8_t *out, size_t cap) {
+    return trial<float>(b, B, V, eb, radius, out, cap);
+}
+long long lzh_trial_f64(const double *b, size_t B, size_t V, double eb, int radius, uint8_t *out, size_t cap) {
+    return trial<double>(b, B, V, eb, radius, out, cap);
+}
 long long lzh_encode_f32(const float *x, size_t n, double eb, int radius, int block, int l1, int l2, uint8_t *out,
                          size_t cap) {
     return encode<float>(x, n, eb, radius, block, l1, l2, out, cap);

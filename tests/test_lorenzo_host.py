@@ -54,7 +54,21 @@ def host_decoder():
         assert n >= 0, n
         return out[:n].tobytes()
 
+    def trial(blocks, eb, radius=32768):
+        blocks = np.ascontiguousarray(blocks)
+        B, V = blocks.shape
+        cap = 4096 + blocks.size * (blocks.itemsize + 8) + 2 * 65540
+        out = np.empty(cap, np.uint8)
+        ct = ctypes.c_float if blocks.dtype == np.float32 else ctypes.c_double
+        fn = lib.lzh_trial_f32 if blocks.dtype == np.float32 else lib.lzh_trial_f64
+        fn.restype = ctypes.c_longlong
+        n = fn(blocks.ctypes.data_as(ctypes.POINTER(ct)), ctypes.c_size_t(B), ctypes.c_size_t(V),
+               ctypes.c_double(eb), radius, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ctypes.c_size_t(cap))
+        assert n >= 0, n
+        return out[:n].tobytes()
+
     decode.encode = encode
+    decode.trial = trial
     return decode
 
 
@@ -132,3 +146,31 @@ def test_damaged_payloads_are_rejected(host_decoder, restatement):
     bad = bytearray(payload)
     bad[12] = 0xFF  # the selection record's state count (big-endian, most significant byte)
     assert host_decoder(bytes(bad), x.size, np.float64)[0] != 0
+
+
+@pytest.mark.parametrize("kind,B,V,dtype,eb,quantbin", [
+    ("walk", 12, 513, np.float32, 1e-2, 65536), ("sine", 7, 1025, np.float64, 1e-6, 65536),
+    ("noise", 5, 257, np.float32, 1e-4, 65536), ("spikes", 9, 129, np.float64, 1e-3, 65536),
+    ("walk", 4, 4097, np.float32, 1e-3, 16384)])
+def test_tuner_trial_layout_and_ratio(host_decoder, reference, kind, B, V, dtype, eb, quantbin):
+    """The tuner's Lorenzo trial (lorenzo_compress_test): the buffer laid out as lorenzo.cu's
+    lorenzo_trial_ratio writes it is the reference's byte for byte (its quantizer header comes
+    before the code count, unlike the stream), and the reference's ratio is the input bytes over
+    the zstd size of that buffer plus its length word."""
+    blocks = np.stack([series(kind, V, dtype, seed=b) for b in range(B)])
+    ref_buf, ref_ratio = reference.lorenzo_trial(blocks, eb, quantbin)
+    assert host_decoder.trial(blocks, eb, quantbin // 2) == ref_buf
+    zs = len(reference.zstd_compress(ref_buf))
+    assert ref_ratio == pytest.approx(blocks.nbytes / zs, rel=0, abs=0)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "tunedlz_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_encoder_matches_tuned_streams(host_decoder, path):
+    """The encoder functions at the tuner's final Config (block size 128, the chosen bins) give the
+    payload of the reference's own tuned stream."""
+    from test_lorenzo_oracle import tuned_fixture
+    x, eb, c, payload = tuned_fixture(path)
+    assert host_decoder.encode(x, eb, c.quantbinCnt // 2, 128) == payload
+    rc, y = host_decoder(payload, x.size, x.dtype, 128)
+    assert rc == 0

@@ -150,3 +150,35 @@ def test_decoder_rejects_damaged_payloads(restatement):
     bad[8 + 4] ^= 0xFF  # the selection record's state count
     with pytest.raises(ValueError):
         restatement.lorenzo_decode(bytes(bad), x.size, np.float32)
+
+
+TUNED = sorted(glob.glob(os.path.join(GOLDEN, "tunedlz_*.npz")))
+
+
+def tuned_fixture(path):
+    """(input, eb, the reference stream's Config, its payload) of a tuner-choice fixture."""
+    import pyarrow as pa
+    from falcons_b200 import api
+    g = np.load(path)
+    s = g["stream"].tobytes()
+    h = oracle.lossless_section(s)
+    payload = pa.decompress(s[h + 8:], int.from_bytes(s[h:h + 8], "little"), codec="zstd", asbytes=True)
+    return g["x"], float(g["eb"]), api.read_config(g["stream"]), payload
+
+
+@pytest.mark.parametrize("path", TUNED, ids=lambda p: os.path.basename(p))
+def test_tuned_lorenzo_streams_match_oracle(restatement, path):
+    """1-D fields on which the reference's ALGO_INTERP_LORENZO tuner switches to the Lorenzo path
+    (FalconsAlgoInterp.hpp:479-537): the stream's Config carries the Lorenzo orders 1 and 2, the
+    chosen bins and block size 128 (Config::setDims, utils/Config.hpp:165-181, undoes the trial's
+    5), and its payload is the oracle's for that Config."""
+    x, eb, c, payload = tuned_fixture(path)
+    assert c.cmprAlgo == 0 and c.blockSize == 128 and c.lorenzo and c.lorenzo2 and not c.regression
+    ours, recon = restatement.lorenzo_payload(x, eb, radius=c.quantbinCnt // 2, block=128)
+    assert ours == payload
+    assert same_bits(restatement.lorenzo_decode(payload, x.size, x.dtype, block=128), recon)
+
+
+def test_tuned_fixtures_cover_both_bin_counts():
+    bins = {tuned_fixture(p)[2].quantbinCnt for p in TUNED}
+    assert bins == {65536, 16384}

@@ -130,3 +130,28 @@ def test_unsupported_lorenzo_configs_are_rejected(cuda):
     conf2.conf.regression = 0
     with pytest.raises(ValueError):  # N > 1
         api.falcons.compress(x2, conf2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "tunedlz_*.npz"))),
+                         ids=lambda p: os.path.basename(p))
+def test_tuner_picks_lorenzo_like_reference(cuda, restatement, path):
+    """ALGO_INTERP_LORENZO on 1-D fields where the reference's tuner switches to the Lorenzo path:
+    the same choice (bins, block size 128), the reference's payload byte for byte, and the
+    oracle's reconstruction; the reference stream decodes to the same values."""
+    from falcons_b200 import api
+    from test_lorenzo_oracle import tuned_fixture
+    x, eb, ref_conf, payload = tuned_fixture(path)
+    conf = api.falconsConfig(x.size)
+    conf.cmprAlgo = api.falconsAlgorithm.INTERP_LORENZO
+    conf.errorBoundMode = api.falconsErrorBoundMode.ABS
+    conf.absErrorBound = eb
+    buf, _ = api.falcons.compress(x.copy(), conf, copy=True)
+    c = api.read_config(buf)
+    assert c.cmprAlgo == api.falconsAlgorithm.LORENZO_REG
+    assert c.quantbinCnt == ref_conf.quantbinCnt and c.blockSize == 128
+    assert stream_payload(buf) == payload
+    y, _ = api.falcons.decompress(buf, x.dtype, x.shape)
+    assert same_bits(y, restatement.lorenzo_decode(payload, x.size, x.dtype, block=128))
+    yr, _ = api.falcons.decompress(np.load(path)["stream"], x.dtype, x.shape)
+    assert same_bits(yr, y)
