@@ -172,12 +172,12 @@ int falcons_interp_decompress(falcons_ctx *ctx, int dtype, const size_t *dims, i
         void *ws = ctx->c.work.get(fb2::interp_workspace_bytes(plan, es));
         cudaStream_t st = pick(ctx, stream);
         if (dtype == FALCONS_DTYPE_F32)
-            fb2::interp_decompress<float>(plan, d_codes, static_cast<const float *>(d_unpred),
+            fb2::interp_decompress<float>(plan, d_codes, static_cast<const float *>(d_unpred), (long long)n_unpred,
                                           static_cast<float *>(d_out), ws, st);
         else
-            fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred),
-                                           static_cast<double *>(d_out), ws, st);
-        if (!stream) FB2_CUDA(cudaStreamSynchronize(st));
+            fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred), (long long)n_unpred,
+                                          static_cast<double *>(d_out), ws, st);
+        fb2::interp_decompress_check(plan, es, ws, (long long)n_unpred, st);
     });
 }
 
@@ -203,11 +203,12 @@ int falcons_interp_decompress_noalloc(int dtype, const size_t *dims, int N, cons
         void *ws = fb2::static_scratch_current_device();
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         if (dtype == FALCONS_DTYPE_F32)
-            fb2::interp_decompress<float>(plan, d_codes, static_cast<const float *>(d_unpred),
+            fb2::interp_decompress<float>(plan, d_codes, static_cast<const float *>(d_unpred), (long long)n_unpred,
                                           static_cast<float *>(d_out), ws, st);
         else
-            fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred),
-                                           static_cast<double *>(d_out), ws, st);
+            fb2::interp_decompress<double>(plan, d_codes, static_cast<const double *>(d_unpred), (long long)n_unpred,
+                                          static_cast<double *>(d_out), ws, st);
+        fb2::interp_decompress_check(plan, es, ws, (long long)n_unpred, st);
     });
 }
 

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <string>
 
 #include "interp.cuh"
 
@@ -556,7 +557,7 @@ template <class T, bool DECOMP>
 __global__ void __launch_bounds__(kTileThreads) k_esc_scatter(const int16_t *__restrict__ codes, long long n, int esc_code,
                                                               const unsigned long long *__restrict__ tile_off,
                                                               T *__restrict__ esc, T *__restrict__ unpred,
-                                                              long long n_anchor) {
+                                                              long long n_anchor, unsigned long long n_esc_max) {
     const unsigned long long t0 = tile_off[blockIdx.x], t1 = tile_off[blockIdx.x + 1];
     if (t0 == t1) return;
     const long long base = (long long)blockIdx.x * kTile + threadIdx.x * 16;
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(kTileThreads) k_esc_scatter(const int16_t *__r
         mask &= mask - 1;
         const long long i = base + j;
         if (!DECOMP) unpred[n_anchor + r] = esc[i];
-        else esc[i] = unpred[n_anchor + r];
+        else if (r < n_esc_max) esc[i] = unpred[n_anchor + r];  // a list too short is reported by the host
         r++;
     }
 }
@@ -1060,6 +1061,19 @@ AnchorGrid anchor_grid(const InterpPlan &plan) {
 
 size_t interp_workspace_bytes(const InterpPlan &plan, int elem_size) { return ws_layout(plan, elem_size).bytes; }
 
+void interp_decompress_check(const InterpPlan &plan, int elem_size, const void *d_ws, long long n_unpred,
+                             cudaStream_t st) {
+    const WsLayout w = ws_layout(plan, elem_size);
+    unsigned long long total = 0;
+    if (w.ntiles > 0) {
+        FB2_CUDA(cudaMemcpyAsync(&total, static_cast<const char *>(d_ws) + w.total_off, 8, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+    }
+    if ((long long)total > n_unpred - plan.n_anchor)
+        throw std::invalid_argument("the codes name " + std::to_string(total) + " unpredictable values but the list holds " +
+                                    std::to_string(n_unpred - plan.n_anchor) + " after the anchors");
+}
+
 template <class T>
 void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
                      unsigned long long *d_n_esc, cudaStream_t st) {
@@ -1086,7 +1100,7 @@ void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpr
         k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, d_n_esc);
         FB2_CHECK_LAUNCH();
         k_esc_scatter<T, false><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, scan, esc,
-                                                                           d_unpred, plan.n_anchor);
+                                                                           d_unpred, plan.n_anchor, ~0ull);
         FB2_CHECK_LAUNCH();
     } else if (d_n_esc) {
         FB2_CUDA(cudaMemsetAsync(d_n_esc, 0, 8, st));
@@ -1094,8 +1108,9 @@ void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpr
 }
 
 template <class T>
-void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, T *d_x, void *d_ws,
-                       cudaStream_t st) {
+void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, long long n_unpred, T *d_x,
+                       void *d_ws, cudaStream_t st) {
+    if (n_unpred < plan.n_anchor) throw std::invalid_argument("unpredictable list too short");
     const WsLayout w = ws_layout(plan, sizeof(T));
     char *ws = static_cast<char *>(d_ws);
     T *esc = reinterpret_cast<T *>(ws + w.esc_off);
@@ -1116,8 +1131,9 @@ void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *
         FB2_CHECK_LAUNCH();
         k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, total);
         FB2_CHECK_LAUNCH();
-        k_esc_scatter<T, true><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(codes, plan.n_codes, escc, scan, esc,
-                                                                          unpred, plan.n_anchor);
+        k_esc_scatter<T, true><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(
+            codes, plan.n_codes, escc, scan, esc, unpred, plan.n_anchor,
+            (unsigned long long)(n_unpred - plan.n_anchor));
         FB2_CHECK_LAUNCH();
     }
     if (plan.first_point) {
@@ -1232,10 +1248,10 @@ template void interp_compress<float>(const InterpPlan &, float *, int16_t *, flo
                                      cudaStream_t);
 template void interp_compress<double>(const InterpPlan &, double *, int16_t *, double *, void *,
                                       unsigned long long *, cudaStream_t);
-template void interp_decompress<float>(const InterpPlan &, const int16_t *, const float *, float *, void *,
-                                       cudaStream_t);
-template void interp_decompress<double>(const InterpPlan &, const int16_t *, const double *, double *, void *,
-                                        cudaStream_t);
+template void interp_decompress<float>(const InterpPlan &, const int16_t *, const float *, long long, float *,
+                                       void *, cudaStream_t);
+template void interp_decompress<double>(const InterpPlan &, const int16_t *, const double *, long long, double *,
+                                        void *, cudaStream_t);
 template void device_range<float>(const float *, long long, float *, void *, cudaStream_t);
 template void device_range<double>(const double *, long long, double *, void *, cudaStream_t);
 

@@ -70,9 +70,18 @@ template <class T>
 void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
                      unsigned long long *d_n_esc, cudaStream_t st);
 
+// d_unpred holds n_unpred values: the anchors, then one value per escape code in stream order.
+// An escape beyond the list is not read; interp_decompress_check reports it.
 template <class T>
-void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, T *d_x, void *d_ws,
-                       cudaStream_t st);
+void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *d_unpred, long long n_unpred, T *d_x,
+                       void *d_ws, cudaStream_t st);
+
+// Waits for the stream and throws std::invalid_argument when the codes of the last
+// interp_decompress on d_ws name more escapes than its unpredictable list holds after the anchors
+// (the reference's LinearQuantizer::recover would read past its list; the reconstruction is then
+// not valid).
+void interp_decompress_check(const InterpPlan &plan, int elem_size, const void *d_ws, long long n_unpred,
+                             cudaStream_t st);
 
 // Loads, on the current device, every kernel interp_decompress can launch (float and double).
 // Under lazy module loading a kernel is otherwise loaded at its first launch, which can allocate

@@ -111,6 +111,9 @@ int falcons_decompress_device(falcons_ctx *ctx, int dtype, const void *d_stream,
 int falcons_interp_compress(falcons_ctx *ctx, int dtype, const size_t *dims, int N, const falcons_interp_params *p,
                             void *d_data, int16_t *d_codes, void *d_unpred, size_t *n_codes, size_t *n_unpred,
                             void *stream);
+/* falcons_interp_decompress: d_unpred holds n_unpred values (the anchors, then one value per escape
+ * code in stream order).  Codes that name more escapes than the list holds return FALCONS_EINVAL
+ * without reading past the list.  The call waits for `stream` before it returns. */
 int falcons_interp_decompress(falcons_ctx *ctx, int dtype, const size_t *dims, int N,
                               const falcons_interp_params *p, const int16_t *d_codes, size_t n_codes,
                               const void *d_unpred, size_t n_unpred, void *d_out, void *stream);
@@ -133,11 +136,14 @@ int falcons_decode_codes(falcons_ctx *ctx, const void *d_in, size_t len, size_t 
  *   8.3 million double codes).  Larger fields are rejected with FALCONS_EINVAL and a message
  *   giving the size needed; use falcons_interp_decompress for them.
  * - Device and stream: works on the CURRENT device; `stream` is a cudaStream_t of that device
- *   (NULL: the default stream).  The call is asynchronous: d_out is complete when the stream's
- *   work is.
+ *   (NULL: the default stream).  The call returns once the stream's work up to and including it
+ *   has finished (it reads back the number of escape codes, 8 bytes, to check it against
+ *   n_unpred), so d_out is complete on return.
  * - Set-up: the first call on a device (with that device current) resolves the scratch address
  *   and loads the decompress kernels there, which reserves the region; make that first call
- *   before any stream capture begins.  Later calls allocate nothing.
+ *   before any stream capture begins.  Later calls allocate nothing.  The resolved address is kept
+ *   for the life of the process: a device reset (cudaDeviceReset) after the first call is not
+ *   supported.
  * - Nothing in the scratch has to start at zero: every word the call reads, it wrote earlier in
  *   the same call.
  * - Overlapping calls race: all calls on a device share the one region, so two calls whose work

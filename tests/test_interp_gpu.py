@@ -106,3 +106,25 @@ def test_value_range(cuda):
     x = _field((50, 60, 70), np.float32, 9)
     r = D.value_range(torch.from_numpy(x).to(cuda))
     assert r == float(np.float32(x.max()) - np.float32(x.min()))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_decompress_refuses_more_escapes_than_the_list(cuda, restatement, dtype):
+    """Codes built on the host with one escape more than the unpredictable list holds: the context
+    entry point returns EINVAL (ValueError) and reads nothing past the list."""
+    import torch
+    from falcons_b200 import device as D
+    x = _field((30, 31, 32), dtype, 7)
+    eb = 1e-3 * float(x.max() - x.min())
+    ref = restatement.compress(x, eb, 1, 0)
+    p = D.interp_params(eb, 1, 0, None, 3)
+    codes = ref.codes.copy()
+    pos = int(np.flatnonzero(codes != -p.radius)[codes.size // 3])
+    codes[pos] = -p.radius
+    dc = torch.from_numpy(codes).to(cuda)
+    du = torch.from_numpy(ref.unpred.copy()).to(cuda)
+    with pytest.raises(ValueError, match="unpredictable values"):
+        D.interp_decompress(x.shape, du.dtype, dc, du, p)
+    # a list of exactly the right length still decodes bit-exact
+    rec = D.interp_decompress(x.shape, du.dtype, torch.from_numpy(ref.codes.copy()).to(cuda), du, p)
+    np.testing.assert_array_equal(rec.cpu().numpy(), ref.recon)

@@ -114,3 +114,21 @@ def test_rejects_inconsistent_arguments():
                                                       ctypes.c_size_t(unpred.numel()),
                                                       ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(0))
     assert rc == _lib.EINVAL
+
+
+def test_rejects_codes_with_more_escapes_than_the_list():
+    """A code array naming one escape more than the unpredictable list holds (a mismatched buffer or
+    a damaged stream) is refused with FALCONS_EINVAL; the escape beyond the list is not read."""
+    shape = (40, 41, 42)
+    p, codes, unpred, ref = _case(shape, np.float32, 1, 51)
+    bad = codes.clone()
+    h = bad.cpu().numpy()
+    pos = int(np.flatnonzero(h != -p.radius)[len(h) // 2])
+    bad[pos] = -p.radius
+    out = torch.empty_like(ref)
+    assert _noalloc(shape, bad, unpred, p, out) == _lib.EINVAL
+    assert "unpredictable values" in _lib.lib().falcons_last_error().decode()
+    # the entry point is still usable and exact after the refusal
+    _lib.check(_noalloc(shape, codes, unpred, p, out), "interp_decompress_noalloc")
+    torch.cuda.synchronize()
+    assert _same_bits(out, ref)
