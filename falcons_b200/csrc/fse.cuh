@@ -1,13 +1,16 @@
-// Finite State Entropy (tANS) primitives, host+device, compatible with the FSE stream format that
-// the reference links (zstd's standalone FSE v0.9, vendored as include/Falcons/encoder/zfse, and
-// documented for zstd in RFC 8878 section 4.1):
-//   - normalized-count header ("NCount"):        zfse/fse_compress.c FSE_writeNCount, entropy_common.c FSE_readNCount
-//   - count normalization:                        zfse/fse_compress.c FSE_normalizeCount / FSE_normalizeM2
-//   - table spread, encode/decode tables:         zfse/fse_compress.c FSE_buildCTable_wksp, fse_decompress.c FSE_buildDTable
-//   - 2-state block coding:                       zfse/fse_compress.c FSE_compress_usingCTable_generic
-//   - little-endian forward bit writer, backward bit reader: zfse/bitstream.h
-// Implemented here from the published algorithm; every routine is a plain sequential function so
-// that one GPU thread (or the host) can run it.
+// Finite State Entropy (tANS) primitives, host + device, for the FSE block format the reference
+// links (zstd's standalone FSE v0.9, vendored as include/Falcons/encoder/zfse; the format is the
+// one RFC 8878 section 4.1 documents for zstd):
+//   - normalized-count header ("NCount"), RFC 8878 4.1.1: written and read here from the RFC's
+//     description, with a plain bit packer;
+//   - count normalization: this file's own rule (nearest shares, then single-cell moves by
+//     marginal coded size); any normalization is valid, since the counts travel in the header;
+//   - table spread and the encode/decode tables: the decoder must rebuild the encoder's cells, so
+//     they follow the format's spread step (zfse fse_compress.c FSE_buildCTable_wksp,
+//     fse_decompress.c FSE_buildDTable);
+//   - 2-state block coding and the little-endian forward / backward bit streams (zfse
+//     fse_compress.c FSE_compress_usingCTable_generic, bitstream.h): the stream layout.
+// Every routine is a plain sequential function so that one GPU thread (or the host) can run it.
 #pragma once
 #include <stdint.h>
 
@@ -31,298 +34,237 @@ __host__ __device__ __forceinline__ uint32_t table_step(uint32_t tableSize) {
     return (tableSize >> 1) + (tableSize >> 3) + 3;
 }
 
-// ---------------------------------------------------------------- table log choice
-__host__ __device__ inline unsigned min_table_log(size_t srcSize, unsigned maxSymbolValue) {
-    unsigned a = highbit32((uint32_t)srcSize) + 1;
-    unsigned b = highbit32(maxSymbolValue) + 2;
-    return a < b ? a : b;
+// ---------------------------------------------------------------- table size
+// About one table cell per four symbols of the block (cells beyond that cost header bits and
+// decoder memory that a short block does not earn back), but at least four cells per distinct
+// symbol present (so that rounding a share to whole cells stays a small part of it), within
+// [kMinTableLog, maxTableLog].
+__host__ __device__ inline unsigned choose_table_log(unsigned maxTableLog, size_t srcSize, unsigned nPresent) {
+    unsigned tl = 0;
+    for (size_t q = srcSize >> 2; q > 1; q >>= 1) tl++;  // floor(log2(srcSize / 4))
+    unsigned need = 2;
+    while ((1u << need) < 4u * nPresent) need++;         // 2^need >= 4 * nPresent
+    if (tl < need) tl = need;
+    if (tl < (unsigned)kMinTableLog) tl = kMinTableLog;
+    if (tl > maxTableLog) tl = maxTableLog;
+    return tl;
 }
 
-__host__ __device__ inline unsigned optimal_table_log(unsigned maxTableLog, size_t srcSize, unsigned maxSymbolValue) {
-    unsigned maxBitsSrc = highbit32((uint32_t)(srcSize - 1)) - 2;
-    unsigned tableLog = maxTableLog ? maxTableLog : kDefaultTableLog;
-    unsigned minBits = min_table_log(srcSize, maxSymbolValue);
-    if (maxBitsSrc < tableLog) tableLog = maxBitsSrc;
-    if (minBits > tableLog) tableLog = minBits;
-    if (tableLog < (unsigned)kMinTableLog) tableLog = kMinTableLog;
-    if (tableLog > (unsigned)kMaxTableLog) tableLog = kMaxTableLog;
-    return tableLog;
-}
-
-// ---------------------------------------------------------------- normalization
-// Secondary method for skewed distributions.  Returns false on failure.
-__host__ __device__ inline bool normalize_m2(int16_t *norm, uint32_t tableLog, const uint32_t *count, uint64_t total,
-                                             uint32_t maxSymbolValue) {
-    const int16_t NOT_YET = -2;
-    uint32_t distributed = 0;
-    const uint32_t lowThreshold = (uint32_t)(total >> tableLog);
-    uint32_t lowOne = (uint32_t)((total * 3) >> (tableLog + 1));
-    for (uint32_t s = 0; s <= maxSymbolValue; s++) {
-        if (count[s] == 0) { norm[s] = 0; continue; }
-        if (count[s] <= lowThreshold) { norm[s] = -1; distributed++; total -= count[s]; continue; }
-        if (count[s] <= lowOne) { norm[s] = 1; distributed++; total -= count[s]; continue; }
-        norm[s] = NOT_YET;
-    }
-    uint32_t toDistribute = (1u << tableLog) - distributed;
-    if (toDistribute == 0) return true;
-    if ((total / toDistribute) > lowOne) {
-        lowOne = (uint32_t)((total * 3) / (toDistribute * 2));
-        for (uint32_t s = 0; s <= maxSymbolValue; s++) {
-            if (norm[s] == NOT_YET && count[s] <= lowOne) {
-                norm[s] = 1;
-                distributed++;
-                total -= count[s];
-            }
-        }
-        toDistribute = (1u << tableLog) - distributed;
-    }
-    if (distributed == maxSymbolValue + 1) {
-        uint32_t maxV = 0, maxC = 0;
-        for (uint32_t s = 0; s <= maxSymbolValue; s++)
-            if (count[s] > maxC) { maxV = s; maxC = count[s]; }
-        norm[maxV] = (int16_t)(norm[maxV] + (int16_t)toDistribute);
-        return true;
-    }
-    if (total == 0) {
-        for (uint32_t s = 0; toDistribute > 0; s = (s + 1) % (maxSymbolValue + 1))
-            if (norm[s] > 0) { toDistribute--; norm[s]++; }
-        return true;
-    }
-    const uint64_t vStepLog = 62 - tableLog;
-    const uint64_t mid = (1ULL << (vStepLog - 1)) - 1;
-    const uint64_t rStep = (((1ULL << vStepLog) * toDistribute) + mid) / total;
-    uint64_t tmpTotal = mid;
-    for (uint32_t s = 0; s <= maxSymbolValue; s++) {
-        if (norm[s] == NOT_YET) {
-            const uint64_t end = tmpTotal + (count[s] * rStep);
-            const uint32_t sStart = (uint32_t)(tmpTotal >> vStepLog);
-            const uint32_t sEnd = (uint32_t)(end >> vStepLog);
-            const uint32_t weight = sEnd - sStart;
-            if (weight < 1) return false;
-            norm[s] = (int16_t)weight;
-            tmpTotal = end;
-        }
-    }
-    return true;
-}
-
-// Normalizes `count` (sum `total`) to 2^tableLog; -1 marks a low-probability symbol.
-// Returns 0 on failure, 1 for the single-symbol case (not normalized), tableLog otherwise.
+// ---------------------------------------------------------------- count normalization
+// Shares the 2^tableLog table cells among the present symbols so as to minimise the coded size,
+// sum over s of count_s * log2(2^tableLog / cells_s), with at least one cell per present symbol.
+// The saving of a symbol's n-th cell, count * log2(n / (n - 1)), is compared through
+// count / (n - 1/2) (the midpoint value of count / x on [n - 1, n]) in integer arithmetic, so that
+// host and device make the same choice.  Under that measure the best table gives every symbol
+// max(1, round(count * mu)) cells for the scale mu that fills the table, so:
+//   1. mu starts at cells / total and is refined a few times to (cells - symbols held at one
+//      cell) / (count of the others), which absorbs the one-cell floor of rare symbols;
+//   2. the few cells still missing or in excess then move one at a time: a missing cell goes to
+//      the symbol whose next cell saves most, an excess cell leaves the symbol (above one cell)
+//      whose last cell saves least.
+// The low-probability mark (-1) is never used.  Returns tableLog on success, 1 when one symbol
+// holds the whole count (the caller writes a single-symbol block instead), 0 when the table has
+// fewer cells than present symbols.
 __host__ __device__ inline unsigned normalize_count(int16_t *norm, unsigned tableLog, const uint32_t *count,
                                                     uint64_t total, unsigned maxSymbolValue) {
-    if (tableLog == 0) tableLog = kDefaultTableLog;
-    if (tableLog < (unsigned)kMinTableLog || tableLog > (unsigned)kMaxTableLog) return 0;
-    if (tableLog < min_table_log((size_t)total, maxSymbolValue)) return 0;
-    const uint32_t rtb[8] = {0, 473195, 504333, 520860, 550000, 700000, 750000, 830000};
-    const uint64_t scale = 62 - tableLog;
-    const uint64_t step = (1ULL << 62) / total;
-    const uint64_t vStep = 1ULL << (scale - 20);
-    int still = 1 << tableLog;
-    unsigned largest = 0;
-    int16_t largestP = 0;
-    const uint32_t lowThreshold = (uint32_t)(total >> tableLog);
+    if (tableLog < (unsigned)kMinTableLog || tableLog > (unsigned)kMaxTableLog || total == 0) return 0;
+    const uint64_t cells = 1ull << tableLog;
+    unsigned present = 0;
     for (unsigned s = 0; s <= maxSymbolValue; s++) {
         if (count[s] == total) return 1;
-        if (count[s] == 0) { norm[s] = 0; continue; }
-        if (count[s] <= lowThreshold) {
-            norm[s] = -1;
-            still--;
-        } else {
-            int16_t proba = (int16_t)((count[s] * step) >> scale);
-            if (proba < 8) {
-                const uint64_t restToBeat = vStep * rtb[proba];
-                proba += (count[s] * step) - ((uint64_t)proba << scale) > restToBeat;
-            }
-            if (proba > largestP) { largestP = proba; largest = s; }
-            norm[s] = proba;
-            still -= proba;
-        }
+        present += count[s] != 0;
     }
-    if (-still >= (norm[largest] >> 1)) {
-        if (!normalize_m2(norm, tableLog, count, total, maxSymbolValue)) return 0;
-    } else {
-        norm[largest] = (int16_t)(norm[largest] + still);
+    if (present > cells) return 0;
+    uint64_t A = cells, B = total;  // mu = A / B
+    int64_t left = 0;
+    for (int round = 0; round < 4; round++) {
+        uint64_t ones = 0, ones_count = 0;
+        left = (int64_t)cells;
+        for (unsigned s = 0; s <= maxSymbolValue; s++) {
+            if (count[s] == 0) {
+                norm[s] = 0;
+                continue;
+            }
+            uint64_t n = (2 * (uint64_t)count[s] * A + B) / (2 * B);  // nearest whole cell
+            if (n <= 1) {
+                n = 1;
+                ones++;
+                ones_count += count[s];
+            }
+            norm[s] = (int16_t)(n < cells ? n : cells);
+            left -= (int64_t)norm[s];
+        }
+        if (left == 0 || ones_count == total) break;
+        A = cells - ones;
+        B = total - ones_count;
+    }
+    for (; left > 0; left--) {  // hand out the missing cells
+        unsigned best = 0;
+        uint64_t bc = 0, bd = 1;  // best saving so far as the fraction bc / bd
+        for (unsigned s = 0; s <= maxSymbolValue; s++) {
+            if (!count[s]) continue;
+            const uint64_t c2 = 2 * (uint64_t)count[s], d = 2 * (uint64_t)norm[s] + 1;  // n + 1 - 1/2
+            if (c2 * bd > bc * d) {
+                best = s;
+                bc = c2;
+                bd = d;
+            }
+        }
+        norm[best]++;
+    }
+    for (; left < 0; left++) {  // take back the cells in excess
+        int best = -1;
+        uint64_t bc = 0, bd = 1;
+        for (unsigned s = 0; s <= maxSymbolValue; s++) {
+            if (norm[s] < 2) continue;
+            const uint64_t c2 = 2 * (uint64_t)count[s], d = 2 * (uint64_t)norm[s] - 1;  // n - 1/2
+            if (best < 0 || c2 * bd < bc * d) {
+                best = (int)s;
+                bc = c2;
+                bd = d;
+            }
+        }
+        if (best < 0) return 0;
+        norm[best]--;
     }
     return tableLog;
 }
 
-// ---------------------------------------------------------------- NCount header
+// ---------------------------------------------------------------- NCount header (RFC 8878 4.1.1)
+// The bit layout, least significant bit first within little-endian bytes:
+//   * 4 bits: tableLog - 5;
+//   * for symbols 0, 1, ... until all 2^tableLog cells are given out: v = normalized count + 1
+//     (0 stands for the low-probability mark -1).  With R = cells still to give out + 1, v lies in
+//     [0, R]; let B be the bit length of R and H = 2^(B-1).  The values below 2^B - 1 - R take B - 1
+//     bits; the others take B bits, the values from H upward stored plus (2^B - 1 - R);
+//   * after a zero count: the number of further zero counts, as 2-bit fields (3 = three more
+//     zeros and another field follows);
+//   * padding to a whole byte.
+
+// Upper bound of the header size: 4 bits, then per symbol at most tableLog + 1 bits for its
+// value and 2 bits of zero-run fields.
 __host__ __device__ inline size_t ncount_bound(unsigned maxSymbolValue, unsigned tableLog) {
-    return (((maxSymbolValue + 1) * tableLog) >> 3) + 3;
+    return (4 + (size_t)(maxSymbolValue + 1) * (tableLog + 3) + 7) / 8 + 1;
 }
 
-// Writes the normalized-count header; returns its size (0 on an invalid distribution).
-__host__ __device__ inline size_t write_ncount(uint8_t *out0, const int16_t *norm, unsigned maxSymbolValue,
+struct NcPacker {
+    uint8_t *out;
+    size_t bytes;
+    uint32_t acc;
+    unsigned nb;
+    __host__ __device__ void put(uint32_t v, unsigned n) {
+        acc |= v << nb;
+        nb += n;
+        while (nb >= 8) {
+            out[bytes++] = (uint8_t)acc;
+            acc >>= 8;
+            nb -= 8;
+        }
+    }
+    __host__ __device__ size_t finish() {
+        if (nb) out[bytes++] = (uint8_t)acc;
+        return bytes;
+    }
+};
+
+struct NcUnpacker {
+    const uint8_t *in;
+    size_t size;
+    size_t bit;  // bits consumed
+    __host__ __device__ uint32_t get(unsigned n) {
+        uint32_t v = 0;
+        for (unsigned i = 0; i < n; i++, bit++) {
+            const size_t byte = bit >> 3;
+            if (byte < size) v |= (uint32_t)((in[byte] >> (bit & 7)) & 1u) << i;
+        }
+        return v;
+    }
+    __host__ __device__ bool overrun() const { return bit > 8 * size; }
+};
+
+// Writes the header for `norm` (its counts must fill the 2^tableLog cells); returns its size in
+// bytes, 0 when the counts do not fill the table exactly.
+__host__ __device__ inline size_t write_ncount(uint8_t *out, const int16_t *norm, unsigned maxSymbolValue,
                                                unsigned tableLog) {
-    uint8_t *out = out0;
-    const int tableSize = 1 << tableLog;
-    int remaining = tableSize + 1;
-    int threshold = tableSize;
-    int nbBits = (int)tableLog + 1;
-    uint32_t bitStream = (tableLog - kMinTableLog);
-    int bitCount = 4;
-    unsigned symbol = 0;
-    const unsigned alphabetSize = maxSymbolValue + 1;
-    bool previousIs0 = false;
-    while (symbol < alphabetSize && remaining > 1) {
-        if (previousIs0) {
-            unsigned start = symbol;
-            while (symbol < alphabetSize && !norm[symbol]) symbol++;
-            if (symbol == alphabetSize) break;
-            while (symbol >= start + 24) {
-                start += 24;
-                bitStream += 0xFFFFu << bitCount;
-                out[0] = (uint8_t)bitStream;
-                out[1] = (uint8_t)(bitStream >> 8);
-                out += 2;
-                bitStream >>= 16;
-            }
-            while (symbol >= start + 3) {
-                start += 3;
-                bitStream += 3u << bitCount;
-                bitCount += 2;
-            }
-            bitStream += (symbol - start) << bitCount;
-            bitCount += 2;
-            if (bitCount > 16) {
-                out[0] = (uint8_t)bitStream;
-                out[1] = (uint8_t)(bitStream >> 8);
-                out += 2;
-                bitStream >>= 16;
-                bitCount -= 16;
-            }
-        }
-        {
-            int count = norm[symbol++];
-            const int max = (2 * threshold - 1) - remaining;
-            remaining -= count < 0 ? -count : count;
-            count++;
-            if (count >= threshold) count += max;
-            bitStream += (uint32_t)count << bitCount;
-            bitCount += nbBits;
-            bitCount -= (count < max);
-            previousIs0 = (count == 1);
-            if (remaining < 1) return 0;
-            while (remaining < threshold) { nbBits--; threshold >>= 1; }
-        }
-        if (bitCount > 16) {
-            out[0] = (uint8_t)bitStream;
-            out[1] = (uint8_t)(bitStream >> 8);
-            out += 2;
-            bitStream >>= 16;
-            bitCount -= 16;
+    NcPacker pk{out, 0, 0, 0};
+    pk.put(tableLog - kMinTableLog, 4);
+    int R = (1 << tableLog) + 1;
+    unsigned s = 0;
+    while (R > 1) {
+        if (s > maxSymbolValue) return 0;
+        const int n = norm[s++];
+        if (n < -1) return 0;
+        const unsigned v = (unsigned)(n + 1);
+        const unsigned B = highbit32((uint32_t)R) + 1, H = 1u << (B - 1), shortv = 2 * H - 1 - (unsigned)R;
+        if (v < shortv) pk.put(v, B - 1);
+        else pk.put(v >= H ? v + shortv : v, B);
+        R -= n < 0 ? -n : n;
+        if (R < 1) return 0;
+        if (n == 0) {
+            unsigned z = 0;
+            while (s + z <= maxSymbolValue && norm[s + z] == 0) z++;
+            if (s + z > maxSymbolValue) return 0;  // cells left but no symbol to take them
+            s += z;
+            for (; z >= 3; z -= 3) pk.put(3, 2);
+            pk.put(z, 2);
         }
     }
-    if (remaining != 1) return 0;
-    out[0] = (uint8_t)bitStream;
-    out[1] = (uint8_t)(bitStream >> 8);
-    out += (bitCount + 7) / 8;
-    return (size_t)(out - out0);
+    return pk.finish();
 }
 
-__host__ __device__ __forceinline__ uint32_t read_le32_clamped(const uint8_t *p, const uint8_t *end) {
-    uint32_t v = 0;
-    for (int i = 0; i < 4; i++) {
-        const uint8_t b = (p + i < end) ? p[i] : 0;
-        v |= (uint32_t)b << (8 * i);
-    }
-    return v;
-}
-
-// Reads a normalized-count header.  Returns the header size, 0 on corruption.
-// `*maxSV` is the alphabet bound on input and the last coded symbol on output.
+// Reads a header.  `*maxSV` is the largest symbol the caller accepts on input and the last coded
+// symbol on output.  Returns the header size in bytes, 0 when the header is malformed or runs past
+// `size` bytes.
 __host__ __device__ inline size_t read_ncount(int16_t *norm, unsigned *maxSV, unsigned *tableLogOut, const uint8_t *in,
                                               size_t size) {
     if (size < 1) return 0;
-    const uint8_t *const istart = in;
-    const uint8_t *const iend = in + size;
-    // The reference reader requires 4 readable bytes; emulate its zero padding for short headers.
-    uint8_t pad[8];
-    if (size < 4) {
-        for (int i = 0; i < 8; i++) pad[i] = i < (int)size ? in[i] : 0;
-        unsigned mx = *maxSV, tl = 0;
-        size_t r = read_ncount(norm, &mx, &tl, pad, 4);
-        if (r == 0 || r > size) return 0;
-        *maxSV = mx;
-        *tableLogOut = tl;
-        return r;
-    }
-    const uint8_t *ip = istart;
-    for (unsigned s = 0; s <= *maxSV; s++) norm[s] = 0;
-    uint32_t bitStream = read_le32_clamped(ip, iend);
-    int nbBits = (bitStream & 0xF) + kMinTableLog;
-    if (nbBits > kAbsMaxTableLog) return 0;
-    bitStream >>= 4;
-    int bitCount = 4;
-    *tableLogOut = nbBits;
-    int remaining = (1 << nbBits) + 1;
-    int threshold = 1 << nbBits;
-    nbBits++;
-    unsigned charnum = 0;
-    bool previous0 = false;
-    while ((remaining > 1) & (charnum <= *maxSV)) {
-        if (previous0) {
-            unsigned n0 = charnum;
-            while ((bitStream & 0xFFFF) == 0xFFFF) {
-                n0 += 24;
-                if (ip < iend - 5) {
-                    ip += 2;
-                    bitStream = read_le32_clamped(ip, iend) >> bitCount;
-                } else {
-                    bitStream >>= 16;
-                    bitCount += 16;
-                }
-            }
-            while ((bitStream & 3) == 3) {
-                n0 += 3;
-                bitStream >>= 2;
-                bitCount += 2;
-            }
-            n0 += bitStream & 3;
-            bitCount += 2;
-            if (n0 > *maxSV) return 0;
-            while (charnum < n0) norm[charnum++] = 0;
-            if ((ip <= iend - 7) || (ip + (bitCount >> 3) <= iend - 4)) {
-                ip += bitCount >> 3;
-                bitCount &= 7;
-                bitStream = read_le32_clamped(ip, iend) >> bitCount;
-            } else {
-                bitStream >>= 2;
-            }
+    NcUnpacker up{in, size, 0};
+    const unsigned tl = up.get(4) + kMinTableLog;
+    if (tl > (unsigned)kAbsMaxTableLog) return 0;
+    const unsigned lim = *maxSV;
+    for (unsigned s = 0; s <= lim; s++) norm[s] = 0;
+    int R = (1 << tl) + 1;
+    unsigned s = 0;
+    while (R > 1) {
+        if (s > lim || up.overrun()) return 0;
+        const unsigned B = highbit32((uint32_t)R) + 1, H = 1u << (B - 1), shortv = 2 * H - 1 - (unsigned)R;
+        unsigned v = up.get(B - 1);
+        if (v >= shortv) {
+            v |= up.get(1) << (B - 1);
+            if (v >= H) v -= shortv;
         }
-        {
-            const int max = (2 * threshold - 1) - remaining;
-            int count;
-            if ((int)(bitStream & (threshold - 1)) < max) {
-                count = bitStream & (threshold - 1);
-                bitCount += nbBits - 1;
-            } else {
-                count = bitStream & (2 * threshold - 1);
-                if (count >= threshold) count -= max;
-                bitCount += nbBits;
-            }
-            count--;
-            remaining -= count < 0 ? -count : count;
-            norm[charnum++] = (int16_t)count;
-            previous0 = !count;
-            while (remaining < threshold) { nbBits--; threshold >>= 1; }
-            if ((ip <= iend - 7) || (ip + (bitCount >> 3) <= iend - 4)) {
-                ip += bitCount >> 3;
-                bitCount &= 7;
-            } else {
-                bitCount -= (int)(8 * (iend - 4 - ip));
-                ip = iend - 4;
-            }
-            bitStream = read_le32_clamped(ip, iend) >> (bitCount & 31);
+        const int n = (int)v - 1;
+        norm[s++] = (int16_t)n;
+        R -= n < 0 ? -n : n;
+        if (n == 0) {
+            unsigned f;
+            do {
+                f = up.get(2);
+                s += f;
+            } while (f == 3 && !up.overrun());
         }
     }
-    if (remaining != 1) return 0;
-    if (bitCount > 32) return 0;
-    *maxSV = charnum - 1;
-    ip += (bitCount + 7) >> 3;
-    return (size_t)(ip - istart);
+    if (up.overrun() || s == 0 || s - 1 > lim) return 0;
+    *maxSV = s - 1;
+    *tableLogOut = tl;
+    return (up.bit + 7) / 8;
 }
 
+// Chooses how a block of n symbols with histogram `count` is coded: 0 raw, 1 a single repeated
+// symbol, 2 FSE with table log *tl and counts `norm` (largest coded symbol *maxSV).
+__host__ __device__ inline int plan_block(const uint32_t *count, size_t n, unsigned maxTableLog, int16_t *norm,
+                                          unsigned *maxSV, unsigned *tl) {
+    if (n <= 2) return 0;
+    unsigned m = 255, present = 0;
+    while (m > 0 && count[m] == 0) m--;
+    for (unsigned s = 0; s <= m; s++) {
+        present += count[s] != 0;
+        if (count[s] == n) return 1;
+    }
+    *maxSV = m;
+    *tl = choose_table_log(maxTableLog, n, present);
+    return normalize_count(norm, *tl, count, n, m) == *tl ? 2 : 0;
+}
 // ---------------------------------------------------------------- table spread (shared by both sides)
 // Fills sym[0..2^tableLog) with the spread symbol of every cell.  Returns false on an invalid table.
 __host__ __device__ inline bool spread(uint8_t *sym, const int16_t *norm, unsigned maxSymbolValue, unsigned tableLog) {
@@ -670,9 +612,9 @@ struct Writer32 {
 namespace fb2 {
 namespace fse {
 
-// One FSE block in the format of FSE_compress(src, n) with maxSymbolValue 255 and tableLog 11
-// (zfse/fse_compress.c FSE_compress_wksp).  Returns 0 when the block is not compressible, 1 when
-// it is a single repeated symbol, otherwise the number of bytes written to dst.
+// One FSE block in the format FSE_decompress reads (zfse/fse_decompress.c): NCount header, then the
+// two-state backward bit stream.  Returns 0 when the block is better stored raw, 1 when it is a
+// single repeated symbol, otherwise the number of bytes written to dst.
 // Scratch: state_table (1<<kMaxTableLog u16), sym_tt (256), spread scratch (1<<kMaxTableLog bytes).
 struct BlockScratch {
     uint16_t state_table[1 << kMaxTableLog];
@@ -685,21 +627,13 @@ struct BlockScratch {
 // Same, with w.count already holding the histogram of src.
 __host__ __device__ inline size_t compress_block_counted(uint8_t *dst, size_t cap, const uint8_t *src, size_t n,
                                                          BlockScratch &w) {
-    if (n <= 1) return 0;
-    unsigned maxSV = 255;
-    while (maxSV > 0 && w.count[maxSV] == 0) maxSV--;
-    uint32_t maxCount = 0;
-    for (unsigned s = 0; s <= maxSV; s++) maxCount = w.count[s] > maxCount ? w.count[s] : maxCount;
-    if (maxCount == n) return 1;
-    if (maxCount == 1) return 0;
-    if (maxCount < (n >> 7)) return 0;
-    const unsigned tableLog = optimal_table_log(kDefaultTableLog, n, maxSV);
-    if (normalize_count(w.norm, tableLog, w.count, n, maxSV) != tableLog) return 0;
+    unsigned maxSV = 0, tableLog = 0;
+    const int mode = plan_block(w.count, n, kDefaultTableLog, w.norm, &maxSV, &tableLog);
+    if (mode != 2) return (size_t)mode;
     if (cap < ncount_bound(maxSV, tableLog) + 16) return 0;
     const size_t hdr = write_ncount(dst, w.norm, maxSV, tableLog);
     if (hdr == 0) return 0;
     if (!build_ctable(w.state_table, w.sym_tt, w.sym, w.norm, maxSV, tableLog)) return 0;
-    if (n <= 2) return 0;
     BitWriter bw;
     bw.init(dst + hdr, cap - hdr);
     // S1 carries the even indices, S2 the odd ones; both start from the last symbol of their parity.
@@ -726,7 +660,7 @@ __host__ __device__ inline size_t compress_block_counted(uint8_t *dst, size_t ca
     // BIT_closeCStream reports overflow when the stream reaches the last 8 bytes of the buffer.
     if (bw.overflow || body + 8 > cap - hdr) return 0;
     const size_t total = hdr + body;
-    if (total >= n - 1) return 0;
+    if (total >= n - 1) return 0;  // no gain over the raw block and its smaller block header
     return total;
 }
 

@@ -365,6 +365,28 @@ class Reference:
             self._err("ref lorenzo trial")
         return out[:n.value].tobytes(), r
 
+    def fse_compress(self, raw: bytes) -> bytes:
+        """One zfse FSE_compress block: b"" when not compressible (0), b"\\x01" for a single symbol."""
+        src = np.frombuffer(raw, np.uint8)
+        out = np.empty(len(raw) + 1024, np.uint8)
+        fn = self.lib.ref_fse_compress
+        fn.restype = ctypes.c_longlong
+        n = fn(_ptr(src, ctypes.c_uint8), ctypes.c_size_t(len(raw)), _ptr(out, ctypes.c_uint8),
+               ctypes.c_size_t(out.size))
+        if n < 0:
+            self._err("ref fse compress")
+        return b"" if n == 0 else (b"\x01" if n == 1 else out[:n].tobytes())
+
+    def fse_decompress(self, block: bytes, n: int) -> bytes:
+        src = np.frombuffer(block, np.uint8)
+        out = np.empty(max(n, 1), np.uint8)
+        fn = self.lib.ref_fse_decompress
+        fn.restype = ctypes.c_longlong
+        r = fn(_ptr(src, ctypes.c_uint8), ctypes.c_size_t(len(block)), _ptr(out, ctypes.c_uint8), ctypes.c_size_t(n))
+        if r < 0:
+            self._err("ref fse decompress")
+        return out[:r].tobytes()
+
     def zstd_compress(self, raw: bytes) -> bytes:
         src = np.frombuffer(raw, np.uint8)
         cap = len(raw) + len(raw) // 128 + 1024

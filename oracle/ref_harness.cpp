@@ -13,6 +13,7 @@
 //   ref_interp_decompress_<t>   decomposition/InterpolationDecomposition.hpp:48
 //   ref_rlefse_encode/decode    encoder/RleFseEncoder.hpp:850-1079
 //   ref_zstd_compress/decompress lossless/Lossless_zstd.hpp:29-78
+//   ref_fse_compress/decompress  encoder/zfse FSE_compress / FSE_decompress (one FSE block)
 //   ref_lorenzo_payload_<t>     the pre-zstd payload of the 1-D blockwise Lorenzo path as the
 //                               tuner configures it (api/impl/FalconsAlgoInterp.hpp:229-262,
 //                               479-490; compressor/FalconsGenericCompressor.hpp:64-81), without
@@ -290,6 +291,26 @@ long long ref_rlefse_decode(const uint8_t *in, size_t n_in, size_t n_codes, int1
         g_err = e.what();
         return -1;
     }
+}
+
+// zfse FSE_compress / FSE_decompress (encoder/zfse/fse_compress.c, fse_decompress.c), the block
+// coder RleFseEncoder calls (RleFseEncoder.hpp:155,184).  Returns the size, or -1 on an error code.
+long long ref_fse_compress(const uint8_t *src, size_t n, uint8_t *dst, size_t cap) {
+    const size_t r = FSE_compress(dst, cap, src, n);
+    if (FSE_isError(r)) {
+        g_err = "FSE_compress error";
+        return -1;
+    }
+    return static_cast<long long>(r);
+}
+
+long long ref_fse_decompress(const uint8_t *src, size_t n, uint8_t *dst, size_t cap) {
+    const size_t r = FSE_decompress(dst, cap, src, n);
+    if (FSE_isError(r)) {
+        g_err = "FSE_decompress error";
+        return -1;
+    }
+    return static_cast<long long>(r);
 }
 
 long long ref_zstd_compress(const uint8_t *src, size_t n, uint8_t *dst, size_t cap) {
