@@ -178,16 +178,12 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
     if (threadIdx.x == 0) {
         int mode = 0;
         unsigned tl = 0, hdr = 0, maxSV = 255;
-        if (n > 2) {
-            while (maxSV > 0 && w.count[maxSV] == 0) maxSV--;
-            uint32_t maxCount = 0;
-            for (unsigned s2 = 0; s2 <= maxSV; s2++) maxCount = w.count[s2] > maxCount ? w.count[s2] : maxCount;
-            if (maxCount == n) {
+        {
+            const int plan = fse::plan_block(w.count, n, kFseMaxLog, w.norm, &maxSV, &tl);
+            if (plan == 1) {
                 mode = 1;
-            } else if (maxCount > 1 && maxCount >= (n >> 7)) {
-                tl = fse::optimal_table_log(fse::kDefaultTableLog, n, maxSV);
-                if (tl <= kFseMaxLog && fse::normalize_count(w.norm, tl, w.count, n, maxSV) == tl &&
-                    kBlockSlot - 5 >= fse::ncount_bound(maxSV, tl) + 16) {
+            } else if (plan == 2) {
+                if (kBlockSlot - 5 >= fse::ncount_bound(maxSV, tl) + 16) {
                     hdr = (unsigned)fse::write_ncount(out + 5, w.norm, maxSV, tl);
                     // the spread (zfse FSE_buildCTable): the low-probability (-1) symbols take the
                     // top cells; the cells of the others, in symbol order, go to the kept positions
@@ -1147,8 +1143,10 @@ struct SegInfo {
 
 // Per segment: the count of every (context, symbol) key of its chains (a chain's first code has
 // context 0) and every chain's escape count; writes every code's key (context << 8 | symbol) for
-// the chain encoder.  Codes are read 8 at a time as 16-byte vectors when q is 16-byte aligned (the
-// code before a vector comes from the lane below), runs of equal keys within a vector are counted
+// the chain encoder.  CTA (g, u) takes the u-th of gridDim.y slices of every chain of segment g
+// (slice edges on multiples of 8 codes) and adds its counts to the segment's totals, which start
+// at zero.  Codes are read 8 at a time as 16-byte vectors when q is 16-byte aligned (the
+// code before a vector comes from the lane below); runs of equal keys within a vector are counted
 // with one atomic, and the lanes of a warp spread their atomics over kHistCopies histograms.
 constexpr int kHistCopies = 4;
 constexpr size_t kHistSmem = (size_t)kHistCopies * O1_NCTX * O1_NSYM * 4;
@@ -1159,6 +1157,7 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
     __shared__ uint32_t esc[kMaxK];
     constexpr int HN = O1_NCTX * O1_NSYM;
     const SegInfo sg = segs[blockIdx.x];
+    const unsigned long long U = gridDim.y, u = blockIdx.y;
     for (int i = threadIdx.x; i < kHistCopies * HN; i += blockDim.x) hs[i] = 0;
     if (threadIdx.x < kMaxK) esc[threadIdx.x] = 0;
     __syncthreads();
@@ -1168,16 +1167,26 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
         const long long b = (long long)(sg.lo + (unsigned long long)k * sg.cs);
         const long long e = (long long)(sg.lo + min((unsigned long long)k * sg.cs + sg.cs, sg.n));
         if (e <= b) continue;
-        // codes [b, hb) and [tb, e) one per thread, whole vectors [hb, tb) one per thread
-        long long hb = e, tb = e;
+        // this CTA's slice [sb, se) of the chain [b, e)
+        const unsigned long long len = (unsigned long long)(e - b);
+        auto edge = [&](unsigned long long v) -> long long {
+            if (v == 0) return b;
+            if (v >= U) return e;
+            const long long x = (b + (long long)(len * v / U) + 7) & ~7LL;
+            return x < e ? x : e;
+        };
+        const long long sb = edge(u), se = edge(u + 1);
+        if (se <= sb) continue;
+        // codes [sb, hb) and [tb, se) one per thread, whole vectors [hb, tb) one per thread
+        long long hb = se, tb = se;
         if (vec) {
-            hb = min(e, (b + 7) & ~7LL);
-            tb = max(hb, e & ~7LL);
+            hb = min(se, (sb + 7) & ~7LL);
+            tb = max(hb, se & ~7LL);
         }
         uint32_t ne = 0;
-        const long long nh = hb - b, nt = e - tb;
+        const long long nh = hb - sb, nt = se - tb;
         for (long long j = threadIdx.x; j < nh + nt; j += blockDim.x) {
-            const long long i = j < nh ? b + j : tb + (j - nh);
+            const long long i = j < nh ? sb + j : tb + (j - nh);
             const int prev = i == b ? 0 : (int)q[i - 1];
             const int sy = o1_sym((int)q[i]);
             const uint32_t key = (uint32_t)(o1_ctx(prev) << 8) | (uint32_t)sy;
@@ -1195,7 +1204,7 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
             const uint32_t below = __shfl_up_sync(0xffffffffu, w.w >> 16, 1);
             if (!act) continue;
             int prev = 0;  // the code before this vector (context 0 at the chain's start)
-            if (vi * 8 > b) prev = lane ? (int)(int16_t)below : (int)q[vi * 8 - 1];
+            if (vi * 8 > b) prev = (lane && vi > v0) ? (int)(int16_t)below : (int)q[vi * 8 - 1];
             const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
             uint32_t kk[8];
             uint32_t rkey = ~0u, rn = 0;
@@ -1227,9 +1236,22 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
         uint32_t v = 0;
 #pragma unroll
         for (int c = 0; c < kHistCopies; c++) v += hs[c * HN + i];
-        gh[i] = v;
+        if (v) atomicAdd(gh + i, v);
     }
-    if (threadIdx.x < kMaxK) nvk[blockIdx.x * kMaxK + threadIdx.x] = esc[threadIdx.x];
+    if (threadIdx.x < kMaxK && esc[threadIdx.x]) atomicAdd(nvk + blockIdx.x * kMaxK + threadIdx.x, esc[threadIdx.x]);
+}
+
+// Keeps every m-th decode checkpoint of every chain (the m-th, 2m-th, ... of chain c's
+// src[soff[c] ..]), compacted to dst[doff[c] ..]: checkpoints m times as far apart.
+__global__ void k_ck_thin(const O1Ckpt *__restrict__ src, const unsigned long long *__restrict__ soff,
+                          const unsigned long long *__restrict__ doff, int nchains, uint32_t m,
+                          O1Ckpt *__restrict__ dst) {
+    const int c = blockIdx.y;
+    if (c >= nchains) return;
+    const unsigned long long n = doff[c + 1] - doff[c];
+    for (unsigned long long j = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (unsigned long long)gridDim.x * blockDim.x)
+        dst[doff[c] + j] = src[soff[c] + (j + 1) * m - 1];
 }
 
 // o1_normalize (RleFseEncoder.hpp:410-477) for one (segment, context) per thread.
@@ -1871,6 +1893,8 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         spec_exit = x;
         s_exit[t] = (uint16_t)x;
     }
+    // every part's speculative exit state is read by the part below it, which may be in another warp
+    __syncthreads();
     // 2. repair rounds (err[2] counts the re-run codes, err[3] the rounds, for diagnostics): a part
     //    whose entering state changed walks again from it, emitting into its repair staging, until
     //    its state meets a kept one at index m; its bits are then the repaired bits of the codes
@@ -1884,9 +1908,12 @@ __global__ void __launch_bounds__(kSpecThreads) k_o1_encode_spec(
         if (round > nparts + 2 && need) atomicExch(err, 5);
         if (t == 0) atomicMax(err + 3, round);
         const uint32_t E = need ? s_exit[t + 1] : 0u;
+        // an entering state outside the table would index outside the shared tables: refuse it
+        const bool valid = E >= (uint32_t)O1_M && E < 2u * O1_M;
+        if (need && !valid) atomicExch(err, 6);
         __syncthreads();
         bool changed = false;
-        if (need && round <= nparts + 2) {
+        if (need && valid && round <= nparts + 2) {
             Stager rg{rw};
             uint32_t x = E;
             // the kept state of the next 64th index below, loaded one kept index ahead
@@ -2519,13 +2546,11 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
     } else {
         // ---- segmentation: K chains per segment, S segments (decoder reads S and K from the stream)
         const int K = std::max(1, std::min(kMaxK, tune.o1_streams));
-        long long seg_target = tune.o1_segment;
-        if (seg_target <= 0) {
-            const char *env = getenv("FALCONS_O1_SEGMENT");
-            seg_target = env ? atoll(env) : (1LL << 18);  // 256 Ki symbols -> 16 Ki per chain
-            if (seg_target < 1024) seg_target = 1024;
-        }
-        long long S = std::max<long long>(1, (N + seg_target - 1) / seg_target);
+        // S segments as the reference sizes them, N / 8 Mi within [1, 16] (RleFseEncoder.hpp:582-587):
+        // every segment carries its own 7.5 KiB table set, so few segments keep the payload as small
+        // as the reference's; parallelism comes from the chains and their parts instead.
+        long long S = tune.o1_segment > 0 ? std::max<long long>(1, (N + tune.o1_segment - 1) / tune.o1_segment)
+                                          : std::min<long long>(16, std::max<long long>(1, N / (8LL << 20)));
         if (S > N) S = std::max<long long>(1, N);
         // every segment must be non-empty: an empty one ends after its N and K words
         while (S > 1 && (S - 1) * ((N + S - 1) / S) >= N) S--;
@@ -2567,9 +2592,16 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint32_t *hist = pool.get<uint32_t>((size_t)S * O1_NCTX * O1_NSYM);
         uint32_t *nvk = pool.get<uint32_t>((size_t)S * kMaxK);
         uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
+        FB2_CUDA(cudaMemsetAsync(hist, 0, (size_t)S * O1_NCTX * O1_NSYM * 4, st));
+        FB2_CUDA(cudaMemsetAsync(nvk, 0, (size_t)S * kMaxK * 4, st));
         enable_big_smem();
-        k_o1_hist<<<(unsigned)S, 1024, kHistSmem, st>>>(q, d_segs, hist, nvk, keys,
-                                                       (reinterpret_cast<uintptr_t>(q) & 15) == 0);
+        {
+            // about four CTAs per SM over all segments, a slice at least 64 Ki codes long
+            const long long want = (4LL * 148 + S - 1) / S;
+            const long long U = std::max<long long>(1, std::min<long long>(want, (seg + 65535) / 65536));
+            k_o1_hist<<<dim3((unsigned)S, (unsigned)U), 1024, kHistSmem, st>>>(
+                q, d_segs, hist, nvk, keys, (reinterpret_cast<uintptr_t>(q) & 15) == 0);
+        }
         FB2_CHECK_LAUNCH();
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
@@ -2662,6 +2694,40 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         std::vector<unsigned long long> h_blen = d2h(blen, (size_t)nchains, st);
         std::vector<int> h_err = d2h(d_err, 5, st);
         if (h_err[0]) throw std::runtime_error("tANS encoding failed (table construction or chain repair)");
+        // Decode checkpoints cost 12 bytes each: keep them within 1.5 % of the chains' bytes by
+        // keeping every m-th one (m a power of two; the decoder's parts become m times longer, so
+        // streams whose codes take a few bits each, where the checkpoints weigh most, decode with
+        // fewer, longer parts).
+        if (cc.n_o1) {
+            unsigned long long chain_bytes = 0;
+            for (auto b : h_blen) chain_bytes += b;
+            uint32_t m = 1;
+            while (m < (1u << 16) && 12ull * (cc.n_o1 / m) * 1000 > 15 * chain_bytes) m *= 2;
+            if (m > 1) {
+                std::vector<unsigned long long> noff(nchains_all + 1, 0);
+                const unsigned long long part2 = (unsigned long long)cc.o1_part * m;
+                for (long long g = 0; g < S; g++)
+                    for (int k = 0; k < kMaxK; k++) {
+                        unsigned long long cnt = 0;
+                        if (k < K) {
+                            const unsigned long long clo = segs[g].lo + (unsigned long long)k * segs[g].cs;
+                            const unsigned long long chi = std::min(clo + segs[g].cs, segs[g].lo + segs[g].n);
+                            if (chi > clo) cnt = (chi - clo - 1) / part2;
+                        }
+                        noff[g * kMaxK + k + 1] = noff[g * kMaxK + k] + cnt;
+                    }
+                O1Ckpt *thin = noff.back() ? pool.get<O1Ckpt>(noff.back()) : nullptr;
+                if (thin) {
+                    unsigned long long *d_noff = h2d(pool, noff, st);
+                    k_ck_thin<<<dim3(4, (unsigned)nchains_all), 256, 0, st>>>(o1ck, d_ck_off, d_noff,
+                                                                            (int)nchains_all, m, thin);
+                    FB2_CHECK_LAUNCH();
+                }
+                cc.o1 = thin;
+                cc.n_o1 = noff.back();
+                cc.o1_part = (uint32_t)part2;
+            }
+        }
         if (tr.on)
             std::fprintf(stderr, "[falcons trace] encode chain repair: %d codes re-run, %d rounds, %d far lookups; "
                          "%lld segments, %d chains each\n", h_err[2], h_err[3], h_err[4], S, K);

@@ -50,9 +50,9 @@ struct DecodeCheckpoints {
 // content and avail the content size.  Returns false when it is not a usable checkpoint frame.
 bool parse_ckpt_header(const uint8_t *h, const uint8_t *d_content, size_t avail, DecodeCheckpoints &out);
 
-// Encoder-side tunables (chosen by the autotuner; defaults give ~2% table overhead).
+// Encoder-side tunables.
 struct EntropyTuning {
-    long long o1_segment = 0;          // symbols per method-1 segment (0 = automatic)
+    long long o1_segment = 0;          // symbols per method-1 segment (0: the reference's count, N / 8 Mi in [1, 16])
     int o1_streams = 16;               // K, 1..16
     bool per_segment_tables = false;   // one table set per segment (the reference's choice)
     std::vector<long long> regions;    // code positions where the statistics change (level starts);

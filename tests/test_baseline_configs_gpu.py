@@ -1,0 +1,126 @@
+"""Parity at the full sizes of the benchmark workloads, bit-exact against the reference scalar build.
+
+Each case runs both directions through the drop-in API:
+  * the stream written on the GPU decodes with the reference's Falcons_decompress to the
+    reference's own reconstruction;
+  * the reference's stream decodes on the GPU to the same reconstruction;
+  * the field left in the caller's buffer (the in-place partial reconstruction) is the reference's;
+  * the quantization codes and the unpredictable list equal the reference's;
+  * the compressed size stays within a stated margin of the reference's.
+
+Workloads (seeded synthetic fields with the shapes and value distributions of the reference's
+datasets, which are not available offline):
+  * 512^3 float32 spectral (k^-11/3) Gaussian random field, ALGO_INTERP, EB_REL 1e-4 and 1e-2.
+    At this size the reference writes its order-1 tANS payload in 15 segments (S = N / 8 Mi codes
+    within [1, 16], encoder/RleFseEncoder.hpp:582-595) with no decode checkpoints, so the GPU
+    decodes it with the sequential chain decoder.
+  * 384^3 float64 spectral field (seed 2) + a ramp of amplitude 10 along the slowest axis + 0.5 %
+    of points set to +/-100, EB_ABS 1e-6, ALGO_INTERP_LORENZO (the tuner's choice must match).
+  * 1800 x 3600 float32 sinusoids weighted by cos(latitude) + N(0, 1e-3^2), EB_REL 1e-3,
+    ALGO_INTERP_LORENZO.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+RATIO_MARGIN = 0.02  # compressed size at most 2 % above the reference's
+
+
+def _spectral_cube(n, seed, cuda):
+    from falcons_b200 import synth
+    return synth.spectral_field_torch((n, n, n), seed=seed, device=cuda).cpu().numpy()
+
+
+def _api_conf(api, shape, algo, mode, abs_eb=0.0, rel=0.0):
+    c = api.falconsConfig(*shape)
+    c.cmprAlgo = api.falconsAlgorithm[algo]
+    c.errorBoundMode = api.falconsErrorBoundMode[mode]
+    c.absErrorBound = abs_eb
+    c.relErrorBound = rel
+    return c
+
+
+def _o1_segments(reference, stream, dtype, ndim):
+    """Number of order-1 tANS segments in a stream's RleFse payload (0 when it uses method 0)."""
+    import oracle
+    h = oracle.lossless_section(stream)
+    raw = int.from_bytes(stream[h:h + 8], "little")
+    pay = reference.zstd_decompress(stream[h:], raw)
+    off = 8 * ndim + 4 + 4 + 4 + 8 + 8 + 8 + 1 + 8 + 4
+    n_unpred = int.from_bytes(pay[off:off + 4], "little", signed=True)
+    off += 4 + n_unpred * np.dtype(dtype).itemsize + 8
+    method = pay[off] & 0x7F
+    if method != 1:
+        return 0
+    return int.from_bytes(pay[off + 5:off + 13], "little")
+
+
+def _both_directions(cuda, reference, x, api_conf, ref_conf, check_codes=True):
+    import torch
+    from falcons_b200 import api
+    from falcons_b200 import device as D
+    dtype = x.dtype
+    work = x.copy()
+    buf, _ = api.falcons.compress(work, api_conf)           # the input buffer is overwritten
+    ref_work = x.copy()
+    rs = reference.compress(ref_work, ref_conf, mutate=True)
+    np.testing.assert_array_equal(work, ref_work)            # same in-place partial reconstruction
+    del ref_work
+    hdr_gpu = api.read_config(buf)
+    hdr_ref = api.read_config(np.frombuffer(rs, np.uint8))
+    for f in ("cmprAlgo", "absErrorBound", "interpAlgo", "interpDirection", "interpAlpha", "interpBeta",
+              "interpAnchorStride", "quantbinCnt"):
+        assert getattr(hdr_gpu, f) == getattr(hdr_ref, f), f
+    y_ref = reference.decompress(rs, dtype, x.size).ravel()
+    np.testing.assert_array_equal(reference.decompress(buf.tobytes(), dtype, x.size).ravel(), y_ref)
+    y, _ = api.falcons.decompress(np.frombuffer(rs, np.uint8), dtype, x.shape)
+    np.testing.assert_array_equal(np.asarray(y).ravel(), y_ref)
+    y, _ = api.falcons.decompress(buf, dtype, x.shape)
+    np.testing.assert_array_equal(np.asarray(y).ravel(), y_ref)
+    eb = hdr_ref.absErrorBound
+    assert np.abs(y_ref.astype(np.float64) - x.ravel()).max() <= eb
+    assert len(buf) <= (1 + RATIO_MARGIN) * len(rs), (len(buf), len(rs))
+    if check_codes and int(hdr_ref.cmprAlgo) == int(api.falconsAlgorithm.INTERP):
+        ri = reference.interp_compress(x, eb, int(hdr_ref.interpAlgo), int(hdr_ref.interpDirection), -1,
+                                       float(hdr_ref.interpAlpha), float(hdr_ref.interpBeta))
+        p = D.interp_params(eb, int(hdr_ref.interpAlgo), int(hdr_ref.interpDirection), None, x.ndim,
+                            float(hdr_ref.interpAlpha), float(hdr_ref.interpBeta))
+        xd = torch.from_numpy(x.copy()).to(cuda)
+        codes, unpred = D.interp_compress(xd, p)
+        np.testing.assert_array_equal(codes.cpu().numpy(), ri.codes)
+        np.testing.assert_array_equal(unpred.cpu().numpy(), ri.unpred)
+    return buf, rs
+
+
+@pytest.mark.parametrize("rel", [1e-4, 1e-2])
+def test_single_large_field_512cube_f32(cuda, reference, rel):
+    import oracle
+    from falcons_b200 import api
+    x = _spectral_cube(512, 1, cuda)
+    buf, rs = _both_directions(cuda, reference, x, _api_conf(api, x.shape, "INTERP", "REL", rel=rel),
+                               oracle.ref_conf(algo=oracle.ALGO_INTERP, eb_mode=oracle.EB_REL, rel_eb=rel))
+    if rel == 1e-4:
+        # both streams use the multi-segment order-1 layout with the reference's segment count,
+        # N / 8 Mi codes in [1, 16] (512^3 minus the 16^3 anchors: 15); the reference's stream was
+        # decoded above without decode checkpoints
+        n_codes = x.size - 16 ** 3
+        assert _o1_segments(reference, rs, np.float32, 3) == min(16, n_codes // (8 << 20)) == 15
+        assert _o1_segments(reference, buf.tobytes(), np.float32, 3) == 15
+
+
+def test_outlier_field_384cube_f64_interp_lorenzo(cuda, reference):
+    import oracle
+    from falcons_b200 import api, synth
+    x = synth.outlier_field((384, 384, 384), seed=2)
+    assert x.dtype == np.float64
+    _both_directions(cuda, reference, x, _api_conf(api, x.shape, "INTERP_LORENZO", "ABS", abs_eb=1e-6),
+                     oracle.ref_conf(algo=oracle.ALGO_INTERP_LORENZO, abs_eb=1e-6))
+
+
+def test_latlon_field_1800x3600_f32(cuda, reference):
+    import oracle
+    from falcons_b200 import api, synth
+    x = synth.latlon_field((1800, 3600))
+    _both_directions(cuda, reference, x, _api_conf(api, x.shape, "INTERP_LORENZO", "REL", rel=1e-3),
+                     oracle.ref_conf(algo=oracle.ALGO_INTERP_LORENZO, eb_mode=oracle.EB_REL, rel_eb=1e-3))

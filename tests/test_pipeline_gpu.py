@@ -257,3 +257,36 @@ def test_decode_checkpoints_parallel_parts_and_fallback(cuda, reference, monkeyp
         monkeypatch.delenv("FALCONS_TRACE")
     # the reference decoder skips the frame, damaged or not
     np.testing.assert_array_equal(reference.decompress(damaged[0].tobytes(), np.float32, x.size).ravel(), y_ref)
+
+
+# Fields around the dispatcher's low-ratio switch (FalconsDispatcher.hpp:121-133): sinusoids
+# quantized to 1/K steps (so that zstd of the field compresses well), optionally plus noise, at
+# tiny error bounds.  (K, noise, eb relative to the range, the reference's choice).
+DISPATCH_CASES = [
+    (128, 0.0, 1e-7, "LOSSLESS"),   # lossy ratio 2.4, zstd of the field smaller
+    (8, 1e-3, 1e-7, "LOSSLESS"),    # lossy ratio 1.1
+    (512, 0.0, 1e-7, "INTERP"),     # lossy ratio 2.1, zstd of the field 7 % larger
+    (32, 0.0, 1e-6, "INTERP"),      # lossy ratio 2.5, zstd of the field 7 % larger
+    (8, 0.0, 1e-6, "INTERP"),       # lossy ratio 3.01: at the switch; zstd of the field 2 % larger
+    (32, 0.0, 1e-7, "INTERP"),      # lossy ratio 3.4 with zstd of the field 1 % smaller: no check
+]
+
+
+@pytest.mark.parametrize("K,noise,ebr,algo", DISPATCH_CASES)
+def test_low_ratio_switch_matches_reference_choice(cuda, reference, K, noise, ebr, algo):
+    """The GPU makes the reference's lossy-or-lossless choice on fields near the switch.  The
+    lossy size it compares is its own zstd section, within a fraction of a percent of the
+    reference's, so the choices can differ only for fields whose zstd size falls inside that
+    sliver; these cases keep at least 1 % away from it."""
+    import oracle
+    from falcons_b200 import api, synth
+    base = synth.sinusoid_field((48, 64, 80), seed=5, noise=0.0)
+    rng = np.random.default_rng(1)
+    x = (np.round(base * K) / K + noise * rng.standard_normal(base.shape)).astype(np.float32)
+    eb = ebr * float(x.max() - x.min())
+    rs = reference.compress(x, oracle.ref_conf(algo=oracle.ALGO_INTERP, abs_eb=eb))
+    assert api.read_config(np.frombuffer(rs, np.uint8)).cmprAlgo == api.falconsAlgorithm[algo]
+    buf, _ = api.falcons.compress(x.copy(), _conf(api, x.shape, abs_eb=eb), copy=True)
+    assert api.read_config(buf).cmprAlgo == api.falconsAlgorithm[algo]
+    y, _ = api.falcons.decompress(buf, np.float32, x.shape)
+    np.testing.assert_array_equal(y.ravel(), reference.decompress(rs, np.float32, x.size).ravel())
