@@ -1254,64 +1254,117 @@ __global__ void k_ck_thin(const O1Ckpt *__restrict__ src, const unsigned long lo
         dst[doff[c] + j] = src[soff[c] + (j + 1) * m - 1];
 }
 
-// o1_normalize (RleFseEncoder.hpp:410-477) for one (segment, context) per thread.
-__global__ void k_o1_norm(const uint32_t *__restrict__ hist, int total_tables, uint16_t *__restrict__ nf) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total_tables) return;
-    const uint32_t *cnt = hist + (size_t)t * O1_NSYM;
-    uint16_t *freq = nf + (size_t)t * O1_NSYM;
-    unsigned long long total = 0;
-    int nonzero = 0;
-    for (int s = 0; s < O1_NSYM; s++) {
-        total += cnt[s];
-        nonzero += cnt[s] != 0;
+// The order-1 tables (RleFseEncoder.hpp:410-477 normalizes each context's counts to O1_M cells):
+// one warp per (region, context) table, lanes holding 8 symbols each, with the rule of
+// fse::normalize_count: every present symbol gets its nearest share of the cells (at least one)
+// under a scale refined for the one-cell floor, then single cells move by marginal coded size
+// (count / (n - 1/2) compared in integers) until the table is full.  An empty context gets all
+// cells on symbol 0, a context with one symbol all cells on it.
+__device__ __forceinline__ void warp_best(unsigned long long &bc, unsigned long long &bd, int &bs, bool want_max) {
+    // the best fraction bc / bd over the warp (ties: the lower symbol); bs < 0 marks no candidate
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long oc = __shfl_xor_sync(0xffffffffu, bc, o);
+        const unsigned long long od = __shfl_xor_sync(0xffffffffu, bd, o);
+        const int os = __shfl_xor_sync(0xffffffffu, bs, o);
+        bool take;
+        if (os < 0) take = false;
+        else if (bs < 0) take = true;
+        else {
+            const unsigned long long l = oc * bd, r = bc * od;
+            take = want_max ? (l > r || (l == r && os < bs)) : (l < r || (l == r && os < bs));
+        }
+        if (take) {
+            bc = oc;
+            bd = od;
+            bs = os;
+        }
     }
-    if (total == 0) {
-        for (int s = 0; s < O1_NSYM; s++) freq[s] = 0;
-        freq[0] = O1_M;
+}
+
+__global__ void __launch_bounds__(256) k_o1_norm(const uint32_t *__restrict__ hist, int total_tables,
+                                                 uint16_t *__restrict__ nf) {
+    const int wt = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (wt >= total_tables) return;
+    const uint32_t *cnt = hist + (size_t)wt * O1_NSYM;
+    uint16_t *freq = nf + (size_t)wt * O1_NSYM;
+    constexpr int PER = O1_NSYM / 32;
+    uint32_t c[PER];
+    int n[PER];
+    unsigned long long total = 0;
+    int present = 0;
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+        c[i] = cnt[lane + 32 * i];
+        total += c[i];
+        present += c[i] != 0;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    present = __reduce_add_sync(0xffffffffu, (unsigned)present);
+    if (total == 0 || present == 1) {
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int sy = lane + 32 * i;
+            freq[sy] = (uint16_t)(total == 0 ? (sy == 0 ? O1_M : 0) : (c[i] ? O1_M : 0));
+        }
         return;
     }
-    if (nonzero > 1) {
-        int16_t norm[O1_NSYM];
-        if (fse::normalize_count(norm, O1_PB, cnt, total, O1_NSYM - 1) == (unsigned)O1_PB) {
-            for (int s = 0; s < O1_NSYM; s++) freq[s] = (uint16_t)norm[s];
-            return;
-        }
-    }
-    int sum = 0, maxf = 0, argmax = 0;
-    int f[O1_NSYM];
-    for (int s = 0; s < O1_NSYM; s++) {
-        if (cnt[s]) {
-            int v = (int)((unsigned long long)cnt[s] * O1_M / total);
-            if (v == 0) v = 1;
-            f[s] = v;
+    double mu = (double)O1_M / (double)total;
+    int left = 0;
+    for (int round = 0; round < 4; round++) {
+        int ones = 0, sum = 0;
+        unsigned long long ones_count = 0;
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            if (!c[i]) {
+                n[i] = 0;
+                continue;
+            }
+            const double share = floor((double)c[i] * mu + 0.5);
+            int v = share < (double)O1_M ? (int)share : O1_M;
+            if (v <= 1) {
+                v = 1;
+                ones++;
+                ones_count += c[i];
+            }
+            n[i] = v;
             sum += v;
-            if (v > maxf) { maxf = v; argmax = s; }
-        } else {
-            f[s] = 0;
         }
+        sum = (int)__reduce_add_sync(0xffffffffu, (unsigned)sum);
+        ones = (int)__reduce_add_sync(0xffffffffu, (unsigned)ones);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ones_count += __shfl_xor_sync(0xffffffffu, ones_count, o);
+        left = O1_M - sum;
+        if (left == 0 || ones_count == total) break;
+        mu = (double)(O1_M - ones) / (double)(total - ones_count);
     }
-    int e = O1_M - sum;
-    if (e > 0) {
-        f[argmax] += e;
-    } else if (e < 0) {
-        e = -e;
-        int take = (maxf - 1 < e) ? (maxf - 1) : e;
-        f[argmax] -= take;
-        e -= take;
-        while (e > 0) {
-            int mi = -1;
-            int mv = 1;
-            for (int s = 0; s < O1_NSYM; s++)
-                if (f[s] > mv) { mv = f[s]; mi = s; }
-            if (mi < 0) break;
-            take = f[mi] - 1;
-            if (take > e) take = e;
-            f[mi] -= take;
-            e -= take;
+    while (left != 0) {
+        const bool add = left > 0;
+        unsigned long long bc = 0, bd = 1;
+        int bs = -1;
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            if (!c[i] || (!add && n[i] < 2)) continue;
+            const unsigned long long c2 = 2ull * c[i], d = add ? 2ull * n[i] + 1 : 2ull * n[i] - 1;
+            if (bs < 0 || (add ? c2 * bd > bc * d : c2 * bd < bc * d)) {
+                bc = c2;
+                bd = d;
+                bs = lane + 32 * i;
+            }
         }
+        warp_best(bc, bd, bs, add);
+        if (bs < 0) break;  // nothing movable (cannot happen: fewer symbols than cells)
+        if ((bs & 31) == lane) {
+#pragma unroll
+            for (int i = 0; i < PER; i++)
+                if (lane + 32 * i == bs) n[i] += add ? 1 : -1;
+        }
+        left += add ? -1 : 1;
     }
-    for (int s = 0; s < O1_NSYM; s++) freq[s] = (uint16_t)f[s];
+#pragma unroll
+    for (int i = 0; i < PER; i++) freq[lane + 32 * i] = (uint16_t)n[i];
 }
 
 // ---- tANS tables for 15 contexts x 256 symbols, built by a whole CTA per table (zfse
@@ -2311,7 +2364,8 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_tiles(const int16_t *__res
                                                            uint32_t *__restrict__ cnt) {
     const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
     uint32_t c = 0;
-    if (base + kScanItems <= n) {  // 32-byte aligned (the code arrays are 256-byte aligned)
+    // 16-byte vectors when the code array is 16-byte aligned (tile starts are multiples of 16 codes)
+    if (base + kScanItems <= n && (reinterpret_cast<uintptr_t>(q) & 15) == 0) {
         const int4 *p4 = reinterpret_cast<const int4 *>(q + base);
         const int4 a = __ldg(p4), b = __ldg(p4 + 1);
         const int32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
@@ -2334,7 +2388,7 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_extract(const int16_t *__r
     int16_t v[kScanItems];
     uint32_t c = 0;
     static_assert(kScanItems == 16, "two 16-byte vectors per thread");
-    if (base + kScanItems <= n) {  // 32-byte aligned (the code arrays are 256-byte aligned)
+    if (base + kScanItems <= n && (reinterpret_cast<uintptr_t>(q) & 15) == 0) {
         const int4 *p4 = reinterpret_cast<const int4 *>(q + base);
         const int4 a = __ldg(p4), b = __ldg(p4 + 1);
         const int32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
@@ -2603,6 +2657,38 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
                 q, d_segs, hist, nvk, keys, (reinterpret_cast<uintptr_t>(q) & 15) == 0);
         }
         FB2_CHECK_LAUNCH();
+        // The escape side stream (escape values in index order, their gamma classes, the FSE class
+        // blocks) needs only the codes and the per-chain escape counts of the histogram pass, so
+        // with a second stream it runs next to the table builds and the chain encoder.
+        const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
+        uint32_t *tcnt = pool.get<uint32_t>(tiles + 2);
+        FB2_CUDA(cudaMemsetAsync(tcnt, 0, (tiles + 2) * 4, st));
+        const bool fork = tune.side != nullptr && tune.fork_ev != nullptr && tune.join_ev != nullptr;
+        cudaStream_t es = fork ? tune.side : st;
+        if (fork) {
+            FB2_CUDA(cudaEventRecord(tune.fork_ev, st));
+            FB2_CUDA(cudaStreamWaitEvent(es, tune.fork_ev, 0));
+        }
+        struct Join {  // the calling stream waits for the second one before anything is freed
+            bool on;
+            cudaStream_t st, es;
+            cudaEvent_t ev;
+            void operator()() {
+                if (on) {
+                    cudaEventRecord(ev, es);
+                    cudaStreamWaitEvent(st, ev, 0);
+                    on = false;
+                }
+            }
+            ~Join() { (*this)(); }
+        } join{fork, st, es, tune.join_ev};
+        Pool spool(es);  // scratch of the escape side stream, handed to `pool` once joined
+        if (N > 0) {
+            k_esc_tiles<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt);
+            FB2_CHECK_LAUNCH();
+        }
+        k_scan_small<uint32_t><<<1, 1024, 0, es>>>(tcnt, tiles);
+        FB2_CHECK_LAUNCH();
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
         std::vector<int> seg_region(S, 0), rs{0};
@@ -2632,7 +2718,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         int *d_tab = h2d(pool, seg_region, st);
         const int ntab = R * O1_NCTX;
         uint16_t *nf = pool.get<uint16_t>((size_t)ntab * O1_NSYM);
-        k_o1_norm<<<(ntab + 63) / 64, 64, 0, st>>>(rhist, ntab, nf);
+        k_o1_norm<<<(ntab + 7) / 8, 256, 0, st>>>(rhist, ntab, nf);
         FB2_CHECK_LAUNCH();
         uint16_t *stab = pool.get<uint16_t>((size_t)ntab * O1_M);
         fse::SymTT *stt = pool.get<fse::SymTT>((size_t)ntab * O1_NSYM);
@@ -2680,17 +2766,23 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             FB2_CHECK_LAUNCH();
             tr.mark("chains launched");
         }
-        // escapes in index order
-        const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
-        uint32_t *tcnt = pool.get<uint32_t>(tiles + 2);
-        FB2_CUDA(cudaMemsetAsync(tcnt, 0, (tiles + 2) * 4, st));
-        if (N > 0) {
-            k_esc_tiles<<<(unsigned)tiles, kScanThreads, 0, st>>>(q, N, tcnt);
+        // escapes in index order, on the second stream (the histogram pass has finished there)
+        std::vector<uint32_t> h_nvk = d2h(nvk, (size_t)S * kMaxK, es);
+        std::vector<unsigned long long> gstart(S + 1, 0);
+        for (long long g = 0; g < S; g++) {
+            unsigned long long e = 0;
+            for (int k = 0; k < K; k++) e += h_nvk[g * kMaxK + k];
+            gstart[g + 1] = gstart[g] + e;
+        }
+        const unsigned long long E = gstart[S];
+        uint32_t *evals = spool.get<uint32_t>(E + 1);
+        int16_t *eraw = spool.get<int16_t>(E + 1);
+        if (E > 0) {
+            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt, evals, eraw);
             FB2_CHECK_LAUNCH();
         }
-        k_scan_small<uint32_t><<<1, 1024, 0, st>>>(tcnt, tiles);
-        FB2_CHECK_LAUNCH();
-        std::vector<uint32_t> h_nvk = d2h(nvk, (size_t)S * kMaxK, st);
+        GammaOut go = gamma_encode(spool, evals, gstart, es, cc.fse_part);
+        tr.mark("escapes coded");
         std::vector<unsigned long long> h_blen = d2h(blen, (size_t)nchains, st);
         std::vector<int> h_err = d2h(d_err, 5, st);
         if (h_err[0]) throw std::runtime_error("tANS encoding failed (table construction or chain repair)");
@@ -2732,22 +2824,9 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             std::fprintf(stderr, "[falcons trace] encode chain repair: %d codes re-run, %d rounds, %d far lookups; "
                          "%lld segments, %d chains each\n", h_err[2], h_err[3], h_err[4], S, K);
         tr.mark("chains done");
-        unsigned long long E = 0;
-        std::vector<unsigned long long> gstart(S + 1, 0);
-        for (long long g = 0; g < S; g++) {
-            unsigned long long e = 0;
-            for (int k = 0; k < K; k++) e += h_nvk[g * kMaxK + k];
-            gstart[g + 1] = gstart[g] + e;
-        }
-        E = gstart[S];
-        uint32_t *evals = pool.get<uint32_t>(E + 1);
-        int16_t *eraw = pool.get<int16_t>(E + 1);
-        if (E > 0) {
-            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, st>>>(q, N, tcnt, evals, eraw);
-            FB2_CHECK_LAUNCH();
-        }
-        GammaOut go = gamma_encode(pool, evals, gstart, st, cc.fse_part);
-        tr.mark("escapes coded");
+        join();
+        pool.ptrs.insert(pool.ptrs.end(), spool.ptrs.begin(), spool.ptrs.end());
+        spool.ptrs.clear();
         for (auto b : h_blen)
             if (b == ~0ULL) throw std::runtime_error("tANS chain overflow");
         as.val<uint64_t>((uint64_t)S);

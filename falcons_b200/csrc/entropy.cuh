@@ -58,6 +58,10 @@ struct EntropyTuning {
     std::vector<long long> regions;    // code positions where the statistics change (level starts);
                                        // segments of one region share a table set
     uint32_t ckpt_part = 1024;         // symbols per decode part (power of two, 0 = no checkpoints)
+    // a second stream (and two events) on which the escape side stream runs next to the chain
+    // encoder; none: everything runs on the calling stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 };
 
 EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cudaStream_t st);

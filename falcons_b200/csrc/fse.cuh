@@ -12,6 +12,7 @@
 //     fse_compress.c FSE_compress_usingCTable_generic, bitstream.h): the stream layout.
 // Every routine is a plain sequential function so that one GPU thread (or the host) can run it.
 #pragma once
+#include <math.h>
 #include <stdint.h>
 
 namespace fb2 {
@@ -75,7 +76,7 @@ __host__ __device__ inline unsigned normalize_count(int16_t *norm, unsigned tabl
         present += count[s] != 0;
     }
     if (present > cells) return 0;
-    uint64_t A = cells, B = total;  // mu = A / B
+    double mu = (double)cells / (double)total;
     int64_t left = 0;
     for (int round = 0; round < 4; round++) {
         uint64_t ones = 0, ones_count = 0;
@@ -85,18 +86,18 @@ __host__ __device__ inline unsigned normalize_count(int16_t *norm, unsigned tabl
                 norm[s] = 0;
                 continue;
             }
-            uint64_t n = (2 * (uint64_t)count[s] * A + B) / (2 * B);  // nearest whole cell
+            const double share = floor((double)count[s] * mu + 0.5);  // nearest whole cell (built without FMA contraction)
+            uint64_t n = share < (double)cells ? (uint64_t)share : cells;
             if (n <= 1) {
                 n = 1;
                 ones++;
                 ones_count += count[s];
             }
-            norm[s] = (int16_t)(n < cells ? n : cells);
+            norm[s] = (int16_t)n;
             left -= (int64_t)norm[s];
         }
         if (left == 0 || ones_count == total) break;
-        A = cells - ones;
-        B = total - ones_count;
+        mu = (double)(cells - ones) / (double)(total - ones_count);
     }
     for (; left > 0; left--) {  // hand out the missing cells
         unsigned best = 0;

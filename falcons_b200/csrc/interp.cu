@@ -456,7 +456,8 @@ __global__ void __launch_bounds__(kTileThreads) k_esc_count(const int16_t *__res
                                                             unsigned *__restrict__ tile_count) {
     const long long base = (long long)blockIdx.x * kTile + threadIdx.x * 16;
     int cnt = 0;
-    if (base + 16 <= n) {
+    // 16-byte vectors when the code array is 16-byte aligned (tile starts are multiples of 16 codes)
+    if (base + 16 <= n && (reinterpret_cast<uintptr_t>(codes) & 15) == 0) {
         const int4 *v = reinterpret_cast<const int4 *>(codes + base);
         int4 w[2] = {__ldg(v), __ldg(v + 1)};
         const int16_t *h = reinterpret_cast<const int16_t *>(w);

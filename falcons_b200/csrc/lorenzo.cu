@@ -8,8 +8,8 @@
 // Encode (FalconsGenericCompressor.hpp:64-81 with the blockwise decomposition): one thread walks
 // the quantization; the histograms of the selection and of the codes are counted by the grid; one
 // thread per record builds the Huffman code book (the reference's heap order, canonical codes);
-// one thread per record packs the bits; the payload pieces then go through the Assembler like the
-// interpolation path's.
+// the grid packs the bits (chunk bit counts, their scan, then every thread packs 16 symbols from
+// its start bit); the payload pieces then go through the Assembler like the interpolation path's.
 #include <stdexcept>
 #include <vector>
 
@@ -124,10 +124,103 @@ __global__ void k_lz_book(const BookJob *__restrict__ jobs, int njobs, int *__re
     j.info[3] = bits;
 }
 
-__global__ void k_lz_pack(const int32_t *__restrict__ sym, unsigned long long n, uint32_t offset,
-                          const uint8_t *__restrict__ lens, const uint32_t *__restrict__ codes, uint8_t *__restrict__ out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    lz::huff_pack(sym, 0, (size_t)n, offset, lens, codes, 0, out);
+// Bit packing of one Huffman record in parallel (the layout of lz::huff_pack: code bit b of a
+// symbol at stream bit start + b, stream bits little-endian within bytes): the grid takes chunks
+// of kPackChunk symbols; each chunk's bit count, an exclusive scan of those, then every thread
+// packs 16 consecutive symbols from its start bit (a block scan of the threads' counts), OR-ing
+// each code into the one or two 32-bit words it spans.
+constexpr int kPackThreads = 256, kPackPer = 16, kPackChunk = kPackThreads * kPackPer;
+
+__global__ void __launch_bounds__(kPackThreads) k_lz_chunk_bits(const int32_t *__restrict__ sym, unsigned long long n,
+                                                                uint32_t offset, const uint8_t *__restrict__ lens,
+                                                                unsigned long long *__restrict__ chunk_bits) {
+    const unsigned long long c0 = (unsigned long long)blockIdx.x * kPackChunk;
+    const unsigned long long c1 = min(n, c0 + kPackChunk);
+    unsigned b = 0;
+    for (unsigned long long i = c0 + threadIdx.x; i < c1; i += kPackThreads) b += lens[(uint32_t)sym[i] - offset];
+    b = __reduce_add_sync(0xffffffffu, b);
+    __shared__ unsigned ws[kPackThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kPackThreads / 32; w++) t += ws[w];
+        chunk_bits[blockIdx.x] = t;
+    }
+}
+
+// In-place exclusive scan of v[0, n) (one CTA).
+__global__ void __launch_bounds__(1024) k_lz_scan(unsigned long long *__restrict__ v, unsigned long long n) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (unsigned long long base = 0; base < n; base += 1024) {
+        const unsigned long long i = base + threadIdx.x;
+        const unsigned long long x = i < n ? v[i] : 0;
+        unsigned long long s = x;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= (unsigned)o) s += y;
+        }
+        if (lane == 31) wsum[wid] = s;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned long long w = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= (unsigned)o) w += y;
+            }
+            wsum[lane] = w;
+        }
+        __syncthreads();
+        const unsigned long long excl = carry + (wid ? wsum[wid - 1] : 0) + s - x;
+        if (i < n) v[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + x;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kPackThreads) k_lz_pack_chunks(const int32_t *__restrict__ sym, unsigned long long n,
+                                                                 uint32_t offset, const uint8_t *__restrict__ lens,
+                                                                 const uint32_t *__restrict__ codes,
+                                                                 const unsigned long long *__restrict__ chunk_off,
+                                                                 uint32_t *__restrict__ out) {
+    const unsigned long long i0 = (unsigned long long)blockIdx.x * kPackChunk + threadIdx.x * kPackPer;
+    const unsigned long long i1 = min(n, i0 + kPackPer);
+    unsigned b = 0;
+    for (unsigned long long i = i0; i < i1; i++) b += lens[(uint32_t)sym[i] - offset];
+    // block exclusive scan of b
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned s = b;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= (unsigned)o) s += y;
+    }
+    __shared__ unsigned ws[kPackThreads / 32];
+    if (lane == 31) ws[wid] = s;
+    __syncthreads();
+    unsigned before = 0;
+    for (unsigned w = 0; w < wid; w++) before += ws[w];
+    unsigned long long bit = chunk_off[blockIdx.x] + before + s - b;
+    for (unsigned long long i = i0; i < i1; i++) {
+        const uint32_t k = (uint32_t)sym[i] - offset;
+        const unsigned l = lens[k];
+        const uint32_t c = codes[k];
+        // bits of the code beyond its 32-bit word are zero
+        const unsigned sh = (unsigned)(bit & 31);
+        const unsigned long long w = bit >> 5;
+        if (c) {
+            atomicOr(out + w, c << sh);
+            if (sh && (l > 32 - sh)) {
+                const uint32_t hi = c >> (32 - sh);
+                if (hi) atomicOr(out + w + 1, hi);
+            }
+        }
+        bit += l;
+    }
 }
 
 }  // namespace
@@ -213,9 +306,19 @@ std::vector<BuiltRecord> build_records(Pool &pool, const std::vector<const int32
         BuiltRecord r{jobs[k].lens, nullptr, (uint32_t)info[0], (uint32_t)info[1], (int)info[2], (info[3] + 7) / 8};
         uint8_t *packed = pool.get<uint8_t>((size_t)r.nbytes + 16);
         FB2_CUDA(cudaMemsetAsync(packed, 0, (size_t)r.nbytes + 16, st));
-        k_lz_pack<<<1, 32, 0, st>>>(syms[k], (unsigned long long)counts[k], r.lo, jobs[k].lens, jobs[k].codes,
-                                    packed);
-        FB2_CHECK_LAUNCH();
+        const unsigned long long nsym = (unsigned long long)counts[k];
+        if (nsym > 0) {
+            const unsigned long long nchunks = (nsym + kPackChunk - 1) / kPackChunk;
+            unsigned long long *coff = pool.get<unsigned long long>(nchunks + 1);
+            k_lz_chunk_bits<<<(unsigned)nchunks, kPackThreads, 0, st>>>(syms[k], nsym, r.lo, jobs[k].lens, coff);
+            FB2_CHECK_LAUNCH();
+            k_lz_scan<<<1, 1024, 0, st>>>(coff, nchunks);
+            FB2_CHECK_LAUNCH();
+            k_lz_pack_chunks<<<(unsigned)nchunks, kPackThreads, 0, st>>>(syms[k], nsym, r.lo, jobs[k].lens,
+                                                                         jobs[k].codes, coff,
+                                                                         reinterpret_cast<uint32_t *>(packed));
+            FB2_CHECK_LAUNCH();
+        }
         r.packed = packed;
         out.push_back(r);
     }

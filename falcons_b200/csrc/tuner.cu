@@ -7,6 +7,7 @@
 //   utils/Sample.hpp:234-345                sampleBlocks: strided block selection
 // The profile pass and the trial decompositions run on the GPU; the zstd ranking of the trial
 // codes (a few hundred KB) uses the runtime libzstd, as the reference does.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -78,14 +79,19 @@ double trial_ratio(Pool &pool, const T *d_blocks, long long B, long long side, i
     const long long V = plan.num;
     T *work = pool.get<T>((size_t)(B * V));
     FB2_CUDA(cudaMemcpyAsync(work, d_blocks, (size_t)(B * V) * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    int16_t *codes = pool.get<int16_t>((size_t)(B * plan.n_codes) + 16);
+    // every block's codes start on a 32-byte boundary (the escape scan reads them as vectors)
+    const long long cstride = (plan.n_codes + 15) & ~15LL;
+    int16_t *codes = pool.get<int16_t>((size_t)(B * cstride) + 16);
     T *unpred = pool.get<T>((size_t)(B * V) + 16);
     void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
     unsigned long long *nesc = pool.get<unsigned long long>((size_t)B);
     for (long long b = 0; b < B; b++)
-        interp_compress<T>(plan, work + b * V, codes + b * plan.n_codes, unpred + b * V, ws, nesc + b, st);
+        interp_compress<T>(plan, work + b * V, codes + b * cstride, unpred + b * V, ws, nesc + b, st);
     std::vector<unsigned long long> ne = d2h(nesc, (size_t)B, st);
-    std::vector<int16_t> hc = d2h(codes, (size_t)(B * plan.n_codes), st);
+    std::vector<int16_t> hs = d2h(codes, (size_t)(B * cstride), st);
+    std::vector<int16_t> hc((size_t)(B * plan.n_codes));
+    for (long long b = 0; b < B; b++)
+        std::copy(hs.begin() + b * cstride, hs.begin() + b * cstride + plan.n_codes, hc.begin() + b * plan.n_codes);
     std::vector<T> hu = d2h(unpred, (size_t)(B * V), st);
     std::vector<uint8_t> buf;
     for (long long b = 0; b < B; b++) {
