@@ -41,6 +41,13 @@ class Config(ctypes.Structure):
                 ("interpBeta", ctypes.c_double)]
 
 
+class BatchItem(ctypes.Structure):
+    """falcons_batch_item: one field of a batch call."""
+    _fields_ = [("dtype", ctypes.c_int32), ("status", ctypes.c_int32), ("conf", Config),
+                ("d_data", ctypes.c_void_p), ("d_stream", ctypes.c_void_p), ("cap", ctypes.c_size_t),
+                ("len", ctypes.c_size_t)]
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -49,7 +56,8 @@ EXPORTS = [
     "falcons_compress_size_bound", "falcons_compress", "falcons_read_config", "falcons_decompress",
     "falcons_compress_device", "falcons_decompress_device", "falcons_interp_compress",
     "falcons_interp_decompress", "falcons_device_range", "falcons_encode_codes", "falcons_decode_codes",
-    "falcons_interp_decompress_noalloc",
+    "falcons_interp_decompress_noalloc", "falcons_compress_batch", "falcons_decompress_batch",
+    "falcons_batch_workers",
 ]
 
 

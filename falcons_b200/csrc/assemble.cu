@@ -3,16 +3,19 @@
 namespace fb2 {
 
 Pool::Pool(cudaStream_t s) : st(s) {
-    static bool configured = false;
-    if (!configured) {
-        int dev = 0;
-        cudaGetDevice(&dev);
+    // once per device (one bit per device ordinal below 64): keep freed blocks of the default
+    // memory pool for reuse by the next call
+    static std::atomic<unsigned long long> configured{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(configured.load(std::memory_order_acquire) & bit)) {
         cudaMemPool_t mp;
         if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
-            uint64_t thr = ~0ULL;  // keep freed blocks for reuse by the next call
+            uint64_t thr = ~0ULL;
             cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
         }
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_acq_rel);
     }
 }
 

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../../include/falcons_b200.h"
+#include "batch.cuh"
 #include "context.cuh"
 #include "interp.cuh"
 #include "pipeline.cuh"
@@ -18,6 +19,7 @@
 
 struct falcons_ctx {
     fb2::Context c;
+    fb2::BatchPool batch;  // worker contexts of the batch entry points
 };
 
 namespace {
@@ -111,6 +113,7 @@ int falcons_ctx_create(falcons_ctx **out, int device) {
         FB2_CUDA(cudaSetDevice(device));
         auto *c = new falcons_ctx();
         c->c.device = device;
+        c->batch.device = device;
         FB2_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
         for (auto &e : c->c.ev) FB2_CUDA(cudaEventCreate(&e));
         *out = c;
@@ -289,6 +292,30 @@ int falcons_decompress_device(falcons_ctx *ctx, int dtype, const void *d_stream,
         fb2::decompress_device(ctx->c, dtype == FALCONS_DTYPE_F64 ? 8 : 4, d_stream, len, d_out, cap_elems, conf_out,
                                pick(ctx, stream));
     });
+}
+
+int falcons_compress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers) {
+    return guarded([&] {
+        check_ctx(ctx);
+        fb2::run_batch(ctx->batch, true, items, n, workers);
+    });
+}
+
+int falcons_decompress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers) {
+    return guarded([&] {
+        check_ctx(ctx);
+        fb2::run_batch(ctx->batch, false, items, n, workers);
+    });
+}
+
+int falcons_batch_workers(falcons_ctx *ctx, size_t field_bytes) {
+    int w = 0;
+    if (guarded([&] {
+            check_ctx(ctx);
+            w = fb2::batch_tuned_workers(ctx->batch, field_bytes);
+        }) != FALCONS_OK)
+        return 0;
+    return w;
 }
 
 int falcons_encode_codes(falcons_ctx *ctx, const int16_t *d_codes, size_t n, void *d_out, size_t cap, size_t *out_len,

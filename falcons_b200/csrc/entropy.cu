@@ -10,6 +10,7 @@
 //   encode_o1_ovf     :483-575   escape side stream (gamma + FSE, or raw int16)
 //   decode            :984-1070, decode_o1tans :753-843
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <stdexcept>
@@ -2320,15 +2321,19 @@ std::vector<ChainCta> chain_ctas(const std::vector<int> &chain_table, const std:
 }
 
 void enable_big_smem() {
-    static bool done = false;
-    if (done) return;
+    // once per device (a set of flags, one bit per device ordinal below 64)
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    FB2_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kDecSlots * O1_M * 4));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_decode_parts, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kDecSlots * O1_M * 4));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_encode_spec, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSpecSmem));
     FB2_CUDA(cudaFuncSetAttribute(k_o1_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHistSmem));
-    done = true;
+    done.fetch_or(bit, std::memory_order_acq_rel);
 }
 
 // Sum of the per-segment histograms of each table region (segments [rs[r], rs[r+1])).

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "interp.cuh"
 
@@ -942,6 +943,332 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
     }
 }
 
+// The level whose grid step is one element (the finest level, 7/8 of the codes) of a float field
+// whose rows are 16-byte aligned: the same passes, tiles and code positions as k_yx_fused, with
+// the tile's even and odd columns kept apart in shared memory, so that a thread takes four
+// consecutive targets at a time with 16-byte shared-memory loads and stores and one 8-byte code
+// store:
+//   tile column c <-> x = x0 - 4 + c; row r <-> y = y0 - 4 + r (72 x 72: 64 + a halo of 4)
+//   E[r * 40 + e + 2]  even column c = 2e      (own even columns: e in [2, 34))
+//   O[r * 40 + m + 2]  odd column c = 2m + 1   (own odd columns:  m in [2, 34))
+// The z and y passes take the own even columns in 8 groups of four per row (their operand rows
+// are 16-byte loads) plus the four halo columns (x0 - 4, x0 - 2, x0 + 64, x0 + 66) one by one;
+// the x pass takes the own odd columns in 8 groups of four (operands: eight consecutive even
+// columns).  Targets whose rule is not the cubic interior one, or whose columns leave the field,
+// take the rule path one by one.
+constexpr int kL1Rows = 72, kL1S = 40;
+constexpr int kL1Threads = 256;
+
+__device__ __forceinline__ float &l1_even(float *E, int r, int e) { return E[r * kL1S + e + 2]; }
+__device__ __forceinline__ float &l1_odd(float *O, int r, int m) { return O[r * kL1S + m + 2]; }
+// the value at tile column c of row r
+__device__ __forceinline__ float l1_at(float *E, float *O, int r, int c) {
+    return (c & 1) ? l1_odd(O, r, (c - 1) >> 1) : l1_even(E, r, c >> 1);
+}
+
+// Four consecutive codes at p (n of them valid): one 8-byte access when aligned.
+__device__ __forceinline__ void l1_store4(int16_t *__restrict__ codes, long long p, const int *q, int n) {
+    if (n == 4 && (p & 3) == 0) {
+        *reinterpret_cast<uint2 *>(codes + p) =
+            make_uint2((uint32_t)(q[0] & 0xFFFF) | ((uint32_t)q[1] << 16), (uint32_t)(q[2] & 0xFFFF) | ((uint32_t)q[3] << 16));
+    } else {
+        for (int k = 0; k < n; k++) codes[p + k] = (int16_t)q[k];
+    }
+}
+__device__ __forceinline__ void l1_load4(const int16_t *__restrict__ codes, long long p, int *q, int n) {
+    if (n == 4 && (p & 3) == 0) {
+        const uint2 w = *reinterpret_cast<const uint2 *>(codes + p);
+        q[0] = (int16_t)(w.x & 0xFFFF);
+        q[1] = (int16_t)(w.x >> 16);
+        q[2] = (int16_t)(w.y & 0xFFFF);
+        q[3] = (int16_t)(w.y >> 16);
+    } else {
+        for (int k = 0; k < n; k++) q[k] = codes[p + k];
+    }
+}
+
+// Quantizes (compress) or reconstructs (decompress) the n valid targets of a group of four whose
+// values are v and predictions pred, codes at p..p+3 (written when `own`); v receives the new
+// values (compress: the reconstructions unless the pass is `skip` or the value escapes).
+template <bool DECOMP>
+__device__ __forceinline__ void l1_group(float *v, const float *pred, int n, long long p, bool own, bool skip,
+                                         int16_t *__restrict__ codes, float *__restrict__ esc, const QParams &qp) {
+    int q[4];
+    if (!DECOMP) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (k >= n) break;
+            float recon;
+            q[k] = quantize<float>(v[k], pred[k], qp, recon);
+            if (q[k] == -qp.radius) {
+                if (own) esc[p + k] = v[k];
+            } else if (!skip) {
+                v[k] = recon;
+            }
+        }
+        if (own) l1_store4(codes, p, q, n);
+    } else {
+        l1_load4(codes, p, q, n);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (k >= n) break;
+            v[k] = (q[k] != -qp.radius) ? dequantize<float>(q[k], pred[k], qp) : esc[p + k];
+        }
+    }
+}
+
+// One target by itself (halo columns, partial groups).
+template <bool DECOMP>
+__device__ __forceinline__ void l1_one(float &slot, float pred, long long p, bool own, bool skip,
+                                       int16_t *__restrict__ codes, float *__restrict__ esc, const QParams &qp) {
+    if (!DECOMP) {
+        float recon;
+        const float v = slot;
+        const int q = quantize<float>(v, pred, qp, recon);
+        if (own) codes[p] = (int16_t)q;
+        if (q == -qp.radius) {
+            if (own) esc[p] = v;
+        } else if (!skip) {
+            slot = recon;
+        }
+    } else {
+        const int q = codes[p];
+        slot = (q != -qp.radius) ? dequantize<float>(q, pred, qp) : esc[p];
+    }
+}
+
+template <bool DECOMP>
+__global__ void __launch_bounds__(kL1Threads, 5) k_l1_fused(const FusedYX F, float *__restrict__ xf,
+                                                            int16_t *__restrict__ codes, float *__restrict__ esc,
+                                                            const QParams qp) {
+    __shared__ __align__(16) float E[kL1Rows * kL1S];
+    __shared__ __align__(16) float O[kL1Rows * kL1S];
+    const int ny = F.y.n, nx = F.x.n;
+    const int a = (int)blockIdx.z;
+    const int x0 = (int)blockIdx.x * kFuseW, x1 = min(nx, x0 + kFuseW);
+    const int y0 = (int)blockIdx.y * kFuseR, y1 = min(ny, y0 + kFuseR);
+    const int xo = x0 - 4, yo = y0 - 4;
+    const long long sy = F.x.sb, sz = F.x.sa;
+    float *plane = xf + (long long)a * sz;
+    const int tid = threadIdx.x;
+    // ---- stage rows [yo, yo + 72) x columns [xo, xo + 72), 16 bytes at a time
+    constexpr int NV = kL1Rows * 18;  // 16-byte groups
+    constexpr int ITER = 3;           // loads in flight per thread before their stores
+    for (int base = 0; base < NV; base += ITER * kL1Threads) {
+        float4 v[ITER];
+#pragma unroll
+        for (int k = 0; k < ITER; k++) {
+            const int idx = base + tid + k * kL1Threads;
+            const int r = idx / 18, i = idx - r * 18;
+            const int y = yo + r, x = xo + 4 * i;
+            v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (idx < NV && y >= 0 && y < ny) {
+                const float *src = plane + (long long)y * sy + x;
+                if (x >= 0 && x + 3 < nx) {
+                    v[k] = __ldg(reinterpret_cast<const float4 *>(src));
+                } else {
+                    if (x >= 0 && x < nx) v[k].x = src[0];
+                    if (x + 1 >= 0 && x + 1 < nx) v[k].y = src[1];
+                    if (x + 2 >= 0 && x + 2 < nx) v[k].z = src[2];
+                    if (x + 3 >= 0 && x + 3 < nx) v[k].w = src[3];
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < ITER; k++) {
+            const int idx = base + tid + k * kL1Threads;
+            if (idx >= NV) break;
+            const int r = idx / 18, i = idx - r * 18;
+            *reinterpret_cast<float2 *>(&l1_even(E, r, 2 * i)) = make_float2(v[k].x, v[k].z);
+            *reinterpret_cast<float2 *>(&l1_odd(O, r, 2 * i)) = make_float2(v[k].y, v[k].w);
+        }
+    }
+    __syncthreads();
+    // ---- z pass of an odd plane: even rows x even columns of the tile (halo included)
+    const bool zplane = F.has_z && (a & 1);
+    if (zplane) {
+        const int nz = F.z.n, t = a;
+        const bool zl = F.has_zlate && t == nz - 1;
+        const bool inner = t >= 3 && t <= nz - 5;
+        const Rule rz = row_rule(true, t, nz, F.z.skip);
+        for (int task = tid; task < 36 * 9; task += kL1Threads) {
+            const int rr = task / 9, g = task - rr * 9;
+            const int r = 2 * rr, y = yo + r;
+            if (y < 0 || y >= ny) continue;
+            const bool own_row = y >= y0 && y < y1;
+            const long long ay = y >> 1;
+            const long long pb = zl ? F.zlate.p_base + ay * F.zlate.C
+                                    : F.z.p_base + (ay * F.z.rows_in_group + ((t - 1) >> 1) + F.z.b_off) * F.z.C;
+            const float *col = xf + (long long)y * sy;  // col[z * sz + x] is (z, y, x)
+            auto pred_at = [&](int x) -> float {
+                const float *c1 = col + x;
+                if (inner) return cubic_pred<float>(c1[(t - 3) * sz], c1[(t - 1) * sz], c1[(t + 1) * sz], c1[(t + 3) * sz]);
+                const float o0 = c1[rz.o0 * sz];
+                const float o1 = rz.f != F_EQUAL ? c1[rz.o1 * sz] : o0;
+                const float o2 = rz.f >= F_QUAD1 ? c1[rz.o2 * sz] : o0;
+                const float o3 = rz.f == F_CUBIC ? c1[rz.o3 * sz] : o0;
+                return apply_formula<float>(rz.f, o0, o1, o2, o3);
+            };
+            if (g < 8) {
+                const int xa = x0 + 8 * g;  // targets xa, xa + 2, xa + 4, xa + 6
+                const int n = min(4, max(0, (x1 - xa + 1) / 2));
+                if (n == 0) continue;
+                float *slot = &l1_even(E, r, 2 + 4 * g);
+                float4 cur = *reinterpret_cast<const float4 *>(slot);
+                float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
+                if (inner && n == 4) {
+                    float o[4][4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const float4 *src = reinterpret_cast<const float4 *>(col + (long long)(t - 3 + 2 * j) * sz + xa);
+                        const float4 lo = __ldg(src), hi = __ldg(src + 1);
+                        o[j][0] = lo.x;
+                        o[j][1] = lo.z;
+                        o[j][2] = hi.x;
+                        o[j][3] = hi.z;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 4; k++) pred[k] = cubic_pred<float>(o[0][k], o[1][k], o[2][k], o[3][k]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) pred[k] = k < n ? pred_at(xa + 2 * k) : 0.f;
+                }
+                l1_group<DECOMP>(v, pred, n, pb + (xa >> 1), own_row, F.z.skip, codes, esc, qp);
+                *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+            } else {
+                for (int h = 0; h < 4; h++) {
+                    const int e = h < 2 ? h : 32 + h, x = xo + 2 * e;  // columns x0 - 4, x0 - 2, x0 + 64, x0 + 66
+                    if (x < 0 || x >= nx) continue;
+                    l1_one<DECOMP>(l1_even(E, r, e), pred_at(x), pb + (x >> 1), false, F.z.skip, codes, esc, qp);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // ---- y pass: odd rows of [y0, y1) x even columns of the tile (halo included)
+    {
+        const int nrows = (y1 - y0) / 2;  // odd rows y0 + 1, y0 + 3, ... below y1
+        for (int task = tid; task < nrows * 9; task += kL1Threads) {
+            const int tr = task / 9, g = task - tr * 9;
+            const int t = y0 + 1 + 2 * tr, r = t - yo;
+            const bool late = F.has_late && t == ny - 1;
+            const long long pb = late ? F.late.p_base + (long long)a * F.late.C
+                                      : F.y.p_base + ((long long)a * F.y.rows_in_group + ((t - 1) >> 1) + F.y.b_off) * F.y.C;
+            const bool inner = t >= 3 && t <= ny - 5;
+            const Rule ry = row_rule(true, t, ny, F.y.skip);
+            auto pred_at = [&](int e) -> float {  // column e, rows of the rule
+                if (inner)
+                    return cubic_pred<float>(l1_even(E, r - 3, e), l1_even(E, r - 1, e), l1_even(E, r + 1, e),
+                                             l1_even(E, r + 3, e));
+                const float o0 = l1_even(E, ry.o0 - yo, e);
+                const float o1 = ry.f != F_EQUAL ? l1_even(E, ry.o1 - yo, e) : o0;
+                const float o2 = ry.f >= F_QUAD1 ? l1_even(E, ry.o2 - yo, e) : o0;
+                const float o3 = ry.f == F_CUBIC ? l1_even(E, ry.o3 - yo, e) : o0;
+                return apply_formula<float>(ry.f, o0, o1, o2, o3);
+            };
+            if (g < 8) {
+                const int xa = x0 + 8 * g;
+                const int n = min(4, max(0, (x1 - xa + 1) / 2));
+                if (n == 0) continue;
+                float *slot = &l1_even(E, r, 2 + 4 * g);
+                float4 cur = *reinterpret_cast<const float4 *>(slot);
+                float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
+                if (inner) {
+                    const float4 u0 = *reinterpret_cast<const float4 *>(&l1_even(E, r - 3, 2 + 4 * g));
+                    const float4 u1 = *reinterpret_cast<const float4 *>(&l1_even(E, r - 1, 2 + 4 * g));
+                    const float4 u2 = *reinterpret_cast<const float4 *>(&l1_even(E, r + 1, 2 + 4 * g));
+                    const float4 u3 = *reinterpret_cast<const float4 *>(&l1_even(E, r + 3, 2 + 4 * g));
+                    pred[0] = cubic_pred<float>(u0.x, u1.x, u2.x, u3.x);
+                    pred[1] = cubic_pred<float>(u0.y, u1.y, u2.y, u3.y);
+                    pred[2] = cubic_pred<float>(u0.z, u1.z, u2.z, u3.z);
+                    pred[3] = cubic_pred<float>(u0.w, u1.w, u2.w, u3.w);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; k++) pred[k] = pred_at(2 + 4 * g + k);
+                }
+                l1_group<DECOMP>(v, pred, n, pb + (xa >> 1), true, F.y.skip, codes, esc, qp);
+                *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+            } else {
+                for (int h = 0; h < 4; h++) {
+                    const int e = h < 2 ? h : 32 + h, x = xo + 2 * e;  // columns x0 - 4, x0 - 2, x0 + 64, x0 + 66
+                    if (x < 0 || x >= nx) continue;
+                    l1_one<DECOMP>(l1_even(E, r, e), pred_at(e), pb + (x >> 1), false, F.y.skip, codes, esc, qp);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // ---- x pass: rows [y0, y1) x odd columns of [x0, x1)
+    {
+        const int nrows = y1 - y0;
+        const int odd = nx / 2, thi = 2 * odd - 5;
+        for (int task = tid; task < nrows * 8; task += kL1Threads) {
+            const int yy = task >> 3, j = task & 7;
+            const int r = yy + 4, y = y0 + yy;
+            const int ta = x0 + 1 + 8 * j;  // targets ta, ta + 2, ta + 4, ta + 6
+            const int n = min(4, max(0, (x1 - ta + 1) / 2));
+            if (n == 0) continue;
+            const long long pb = F.x.p_base + ((long long)a * F.x.B + y) * F.x.C + ((ta - 1) >> 1);
+            float *slot = &l1_odd(O, r, 2 + 4 * j);
+            const float4 cur = *reinterpret_cast<const float4 *>(slot);
+            float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
+            if (n == 4 && ta >= 3 && ta + 6 <= thi) {
+                const float e1 = l1_even(E, r, 1 + 4 * j);
+                const float4 p = *reinterpret_cast<const float4 *>(&l1_even(E, r, 2 + 4 * j));
+                const float4 q = *reinterpret_cast<const float4 *>(&l1_even(E, r, 6 + 4 * j));
+                pred[0] = cubic_pred<float>(e1, p.x, p.y, p.z);
+                pred[1] = cubic_pred<float>(p.x, p.y, p.z, p.w);
+                pred[2] = cubic_pred<float>(p.y, p.z, p.w, q.x);
+                pred[3] = cubic_pred<float>(p.z, p.w, q.x, q.y);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int t = ta + 2 * k;
+                    pred[k] = 0.f;
+                    if (k >= n) continue;
+                    if (t >= 3 && t <= thi) {
+                        pred[k] = cubic_pred<float>(l1_at(E, O, r, t - 3 - xo), l1_at(E, O, r, t - 1 - xo),
+                                                    l1_at(E, O, r, t + 1 - xo), l1_at(E, O, r, t + 3 - xo));
+                    } else {
+                        const Rule rx = line_rule(true, t, nx);
+                        const float o0 = l1_at(E, O, r, rx.o0 - xo);
+                        const float o1 = rx.f != F_EQUAL ? l1_at(E, O, r, rx.o1 - xo) : o0;
+                        const float o2 = rx.f >= F_QUAD1 ? l1_at(E, O, r, rx.o2 - xo) : o0;
+                        const float o3 = rx.f == F_CUBIC ? l1_at(E, O, r, rx.o3 - xo) : o0;
+                        pred[k] = apply_formula<float>(rx.f, o0, o1, o2, o3);
+                    }
+                }
+            }
+            l1_group<DECOMP>(v, pred, n, pb, true, F.x.skip, codes, esc, qp);
+            if (DECOMP || !F.x.skip) *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    }
+    __syncthreads();
+    // ---- write the tile back: every row, or (compress with a final x pass, no z targets in this
+    // plane) the y pass's target rows; columns [x0, x1), re-interleaved 16 bytes at a time
+    {
+        const bool odd_rows = !DECOMP && F.x.skip && !zplane;
+        const int nrows = y1 - y0;
+        for (int task = tid; task < nrows * 16; task += kL1Threads) {
+            const int yy = task >> 4, i = task & 15;
+            const int y = y0 + yy;
+            if (odd_rows && !(y & 1)) continue;
+            const int r = yy + 4, x = x0 + 4 * i;
+            if (x >= x1) continue;
+            const float2 e = *reinterpret_cast<const float2 *>(&l1_even(E, r, 2 + 2 * i));
+            const float2 o = *reinterpret_cast<const float2 *>(&l1_odd(O, r, 2 + 2 * i));
+            float *dst = plane + (long long)y * sy + x;
+            if (x + 3 < x1) {
+                *reinterpret_cast<float4 *>(dst) = make_float4(e.x, o.x, e.y, o.y);
+            } else {
+                dst[0] = e.x;
+                if (x + 1 < x1) dst[1] = o.x;
+                if (x + 2 < x1) dst[2] = e.y;
+            }
+        }
+    }
+}
+
 // Whether passes i (and i + 1, i + 2) form a fusable y + x pair; fills F.
 bool fusable_yx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedYX &F, size_t &used) {
     if (i + 1 >= ps.size()) return false;
@@ -978,6 +1305,15 @@ bool fusable_yx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedY
 template <class T, bool DECOMP>
 void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
     dim3 grid((unsigned)((F.x.n + kFuseW - 1) / kFuseW), (unsigned)((F.y.n + kFuseR - 1) / kFuseR), (unsigned)F.y.A);
+    if constexpr (std::is_same<T, float>::value) {
+        // unit grid step with 16-byte aligned rows and planes: the split-column kernel
+        const bool rows16 = F.x.sb % 4 == 0 && (F.y.A == 1 || F.x.sa % 4 == 0);
+        if (F.x.step == 1 && rows16 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+            k_l1_fused<DECOMP><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp);
+            FB2_CHECK_LAUNCH();
+            return;
+        }
+    }
     k_yx_fused<T, DECOMP><<<grid, kFuseThreads, 0, st>>>(F, x, codes, esc, qp);
     FB2_CHECK_LAUNCH();
 }
@@ -1076,19 +1412,13 @@ void interp_decompress_check(const InterpPlan &plan, int elem_size, const void *
 }
 
 template <class T>
-void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
-                     unsigned long long *d_n_esc, cudaStream_t st) {
+void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, void *d_ws, unsigned long long *d_n_esc,
+                            cudaStream_t st) {
     const WsLayout w = ws_layout(plan, sizeof(T));
     char *ws = static_cast<char *>(d_ws);
     T *esc = reinterpret_cast<T *>(ws + w.esc_off);
     unsigned *tiles = reinterpret_cast<unsigned *>(ws + w.tiles_off);
     unsigned long long *scan = reinterpret_cast<unsigned long long *>(ws + w.scan_off);
-    if (plan.n_anchor > 0) {
-        const AnchorGrid G = anchor_grid(plan);
-        const int blocks = (int)std::min<long long>((G.total + 255) / 256, 4096);
-        k_anchors<T, false><<<blocks, 256, 0, st>>>(G, d_x, d_unpred);
-        FB2_CHECK_LAUNCH();
-    }
     if (plan.first_point) {
         k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0]);
         FB2_CHECK_LAUNCH();
@@ -1100,12 +1430,37 @@ void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpr
         FB2_CHECK_LAUNCH();
         k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, d_n_esc);
         FB2_CHECK_LAUNCH();
-        k_esc_scatter<T, false><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, scan, esc,
-                                                                           d_unpred, plan.n_anchor, ~0ull);
-        FB2_CHECK_LAUNCH();
     } else if (d_n_esc) {
         FB2_CUDA(cudaMemsetAsync(d_n_esc, 0, 8, st));
     }
+}
+
+template <class T>
+void interp_compress_finish(const InterpPlan &plan, const T *d_x, const int16_t *d_codes, T *d_unpred, void *d_ws,
+                            cudaStream_t st) {
+    const WsLayout w = ws_layout(plan, sizeof(T));
+    char *ws = static_cast<char *>(d_ws);
+    T *esc = reinterpret_cast<T *>(ws + w.esc_off);
+    unsigned long long *scan = reinterpret_cast<unsigned long long *>(ws + w.scan_off);
+    if (plan.n_anchor > 0) {
+        // the anchors are never targets, so the field still holds them after the passes
+        const AnchorGrid G = anchor_grid(plan);
+        const int blocks = (int)std::min<long long>((G.total + 255) / 256, 4096);
+        k_anchors<T, false><<<blocks, 256, 0, st>>>(G, const_cast<T *>(d_x), d_unpred);
+        FB2_CHECK_LAUNCH();
+    }
+    if (w.ntiles > 0) {
+        k_esc_scatter<T, false><<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(
+            d_codes, plan.n_codes, -plan.levels[0].radius, scan, esc, d_unpred, plan.n_anchor, ~0ull);
+        FB2_CHECK_LAUNCH();
+    }
+}
+
+template <class T>
+void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
+                     unsigned long long *d_n_esc, cudaStream_t st) {
+    interp_compress_passes<T>(plan, d_x, d_codes, d_ws, d_n_esc, st);
+    interp_compress_finish<T>(plan, d_x, d_codes, d_unpred, d_ws, st);
 }
 
 template <class T>
@@ -1225,6 +1580,7 @@ cudaError_t preload_decompress_kernels() {
         reinterpret_cast<const void *>(&k_row_fast<T, true>),
         reinterpret_cast<const void *>(&k_line_smem<T, true>),
         reinterpret_cast<const void *>(&k_yx_fused<T, true>),
+        reinterpret_cast<const void *>(&k_l1_fused<true>),
     };
     for (const void *f : fns) {
         cudaFuncAttributes a;
@@ -1247,6 +1603,14 @@ cudaError_t interp_decompress_preload() {
 
 template void interp_compress<float>(const InterpPlan &, float *, int16_t *, float *, void *, unsigned long long *,
                                      cudaStream_t);
+template void interp_compress_passes<float>(const InterpPlan &, float *, int16_t *, void *, unsigned long long *,
+                                            cudaStream_t);
+template void interp_compress_passes<double>(const InterpPlan &, double *, int16_t *, void *, unsigned long long *,
+                                             cudaStream_t);
+template void interp_compress_finish<float>(const InterpPlan &, const float *, const int16_t *, float *, void *,
+                                            cudaStream_t);
+template void interp_compress_finish<double>(const InterpPlan &, const double *, const int16_t *, double *, void *,
+                                             cudaStream_t);
 template void interp_compress<double>(const InterpPlan &, double *, int16_t *, double *, void *,
                                       unsigned long long *, cudaStream_t);
 template void interp_decompress<float>(const InterpPlan &, const int16_t *, const float *, long long, float *,

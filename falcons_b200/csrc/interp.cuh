@@ -70,6 +70,16 @@ template <class T>
 void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
                      unsigned long long *d_n_esc, cudaStream_t st);
 
+// interp_compress in two steps, so that the caller can size the unpredictable list from the
+// escape count (*d_n_esc after the first step) instead of the field: the passes, the escape
+// count and its scan; then the anchors and the escape values into d_unpred (n_anchor + count).
+template <class T>
+void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, void *d_ws,
+                            unsigned long long *d_n_esc, cudaStream_t st);
+template <class T>
+void interp_compress_finish(const InterpPlan &plan, const T *d_x, const int16_t *d_codes, T *d_unpred, void *d_ws,
+                            cudaStream_t st);
+
 // d_unpred holds n_unpred values: the anchors, then one value per escape code in stream order.
 // An escape beyond the list is not read; interp_decompress_check reports it.
 template <class T>

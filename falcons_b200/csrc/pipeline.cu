@@ -145,10 +145,9 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             const InterpPlan plan = make_plan(dims, c.N, prm);
             Pool pool(st);
             int16_t *codes = pool.get<int16_t>((size_t)plan.n_codes + 16);
-            T *unpred = pool.get<T>((size_t)c.num + 16);
             void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
             unsigned long long *nesc = pool.get<unsigned long long>(2);
-            interp_compress<T>(plan, d_x, codes, unpred, ws, nesc, st);
+            interp_compress_passes<T>(plan, d_x, codes, ws, nesc, st);
             tr.mark("interpolation launched");
             const EntropyChoice ch = choose_entropy(ctx, codes, (size_t)plan.n_codes, st);  // syncs: nesc ready
             tr.mark("entropy method chosen");
@@ -157,6 +156,9 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             FB2_CUDA(cudaStreamSynchronize(st));
             const long long n_unpred = plan.n_anchor + (long long)h_nesc;
             if (n_unpred > 0x7fffffffLL) throw std::length_error("The buffer for compressed data is not large enough.");
+            // the unpredictable list, sized from the escape count (not the field)
+            T *unpred = pool.get<T>((size_t)n_unpred + 16);
+            interp_compress_finish<T>(plan, d_x, codes, unpred, ws, st);
             DecompHeader dh{};
             dh.N = c.N;
             for (int i = 0; i < c.N; i++) dh.dims[i] = c.dims[i];
@@ -200,18 +202,38 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     if (c.cmprAlgo == ALGO_LOSSLESS) {
         payload = lossless_raw_frame(d_x, raw_bytes, d_pay, pcap, st);
     } else if ((double)raw_bytes / (double)core < 3 && zstd_available()) {
-        // FalconsDispatcher.hpp:121-133: compare with zstd of the (in-place reconstructed) field.
-        // The lossy size compared is this stream's zstd section; it differs from the reference's
-        // own by the entropy coder's table and segment choices (well under 1 %), so the two choose
-        // differently only when zstd of the field falls between the two sizes.
+        // FalconsDispatcher.hpp:121-133: the reference compares zstd level 3 of the (in-place
+        // reconstructed) field with its own lossy output, which is zstd level 3 of its payload.
+        // Both sides are measured the same way here: zstd level 3 of this stream's payload content
+        // (the raw blocks' bytes), so that a payload of raw unpredictable values, which zstd
+        // shrinks, counts at the size the reference would give it.  The two choose differently
+        // only when zstd of the field falls between the two compressed payload sizes.
         std::vector<uint8_t> host(raw_bytes);
         FB2_CUDA(cudaMemcpyAsync(host.data(), d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
+        std::vector<uint8_t> framed(core);
+        FB2_CUDA(cudaMemcpyAsync(framed.data(), d_pay, core, cudaMemcpyDeviceToHost, st));
         FB2_CUDA(cudaStreamSynchronize(st));
+        size_t lossy = core;
+        size_t fb = 0, content = 0;
+        if (core > 8 && parse_raw_frame(framed.data() + 8, core - 8, fb, content)) {
+            std::vector<uint8_t> body;
+            body.reserve(content);
+            size_t p = 8 + fb;
+            while (body.size() < content && p + 3 <= core) {
+                const uint32_t bh = (uint32_t)framed[p] | ((uint32_t)framed[p + 1] << 8) | ((uint32_t)framed[p + 2] << 16);
+                const size_t bs = bh >> 3;
+                p += 3;
+                body.insert(body.end(), framed.begin() + p, framed.begin() + std::min(core, p + bs));
+                p += bs;
+            }
+            std::vector<uint8_t> zb(zstd_compress_bound(body.size()) + 16);
+            lossy = 8 + zstd_compress(body.data(), body.size(), zb.data(), zb.size(), 3);
+        }
         std::vector<uint8_t> z(8 + zstd_compress_bound(raw_bytes));
         const uint64_t L = raw_bytes;
         memcpy(z.data(), &L, 8);
         const size_t zs = 8 + zstd_compress(host.data(), raw_bytes, z.data() + 8, z.size() - 8, 3);
-        if (zs < core && zs <= pcap) {
+        if (zs < lossy && zs <= pcap) {
             c.cmprAlgo = ALGO_LOSSLESS;
             FB2_CUDA(cudaMemcpyAsync(d_pay, z.data(), zs, cudaMemcpyHostToDevice, st));
             FB2_CUDA(cudaStreamSynchronize(st));

@@ -145,3 +145,59 @@ def decompress(stream_bytes: torch.Tensor, dtype, out: torch.Tensor | None = Non
                                                     ctypes.c_void_p(out.data_ptr()), ctypes.c_size_t(out.numel()),
                                                     ctypes.byref(conf_out), _stream_ptr(stream)), "decompress_device")
     return out, conf_out
+
+
+def _batch_items(n):
+    return (_lib.BatchItem * n)()
+
+
+def compress_batch(fields, configs, outs=None, workers: int = 0, ctx=None):
+    """Falcons_compress of many device-resident fields in one call (falcons_compress_batch).
+
+    `fields` are contiguous CUDA tensors (float32 / float64), each overwritten with its partial
+    reconstruction; `configs` are falcons_b200.api.falconsConfig.  Returns a list of (uint8 stream
+    tensor on the device, stored config).  workers <= 0: the context's autotuned worker count."""
+    n = len(fields)
+    if n == 0:
+        return []
+    dev = fields[0].device
+    ctx = ctx or _lib.default_context(dev.index or 0)
+    items = _batch_items(n)
+    bufs = []
+    for i, (x, c) in enumerate(zip(fields, configs)):
+        assert x.is_cuda and x.is_contiguous()
+        if c.num_elements != x.numel():
+            c.setDims(*x.shape)
+        cap = int(_lib.lib().falcons_compress_size_bound(_dtype_code(x), ctypes.byref(c.conf)))
+        out = outs[i] if outs is not None and outs[i] is not None and outs[i].numel() >= cap else \
+            torch.empty(cap, dtype=torch.uint8, device=dev)
+        bufs.append(out)
+        it = items[i]
+        it.dtype = _dtype_code(x)
+        it.conf = c.conf
+        it.d_data = x.data_ptr()
+        it.d_stream = out.data_ptr()
+        it.cap = out.numel()
+    _lib.check(_lib.lib().falcons_compress_batch(ctx.ptr, items, ctypes.c_size_t(n), int(workers)), "compress_batch")
+    return [(bufs[i][:items[i].len], items[i].conf) for i in range(n)]
+
+
+def decompress_batch(streams, dtypes, outs, workers: int = 0, ctx=None):
+    """Falcons_decompress of many device-resident streams in one call (falcons_decompress_batch)
+    into the flat device tensors `outs` (one per stream, of the streams' field sizes)."""
+    n = len(streams)
+    if n == 0:
+        return []
+    ctx = ctx or _lib.default_context(streams[0].device.index or 0)
+    items = _batch_items(n)
+    for i, (s, out) in enumerate(zip(streams, outs)):
+        assert s.is_cuda and s.dtype == torch.uint8 and out.is_cuda and out.is_contiguous()
+        it = items[i]
+        it.dtype = _dtype_code(out)
+        it.d_data = out.data_ptr()
+        it.d_stream = s.data_ptr()
+        it.cap = out.numel()
+        it.len = s.numel()
+    _lib.check(_lib.lib().falcons_decompress_batch(ctx.ptr, items, ctypes.c_size_t(n), int(workers)),
+               "decompress_batch")
+    return [items[i].conf for i in range(n)]

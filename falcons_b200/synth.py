@@ -121,3 +121,28 @@ def spectral_field_torch(shape=(512, 512, 512), seed=1, device="cuda", dtype=Non
     x = x.double() if dtype == torch.float64 else x
     x = (x - x.mean(dtype=torch.float64)) / x.std()
     return x.to(dtype).contiguous()
+
+
+def batch_workload(n=2000, seed=4, device="cuda"):
+    """The batched mixed-size workload: n fields with per-field seeds from the spectral
+    generator.  60 % are 3-D cubes with side log-uniform in [16, 192], 30 % 2-D arrays with each
+    side log-uniform in [64, 2048], 10 % 1-D series of length log-uniform in [4 Ki, 4 Mi]; 80 %
+    float32 and 20 % float64; each with its own relative error bound, log-uniform in
+    [1e-5, 1e-2].  Returns a list of (device tensor, relative error bound)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        u = rng.random()
+        if u < 0.6:
+            s = int(round(np.exp(rng.uniform(np.log(16), np.log(192)))))
+            shape = (s, s, s)
+        elif u < 0.9:
+            shape = tuple(int(round(np.exp(rng.uniform(np.log(64), np.log(2048))))) for _ in range(2))
+        else:
+            shape = (int(round(np.exp(rng.uniform(np.log(4096), np.log(4 << 20))))),)
+        dt = torch.float64 if rng.random() < 0.2 else torch.float32
+        rel = float(np.exp(rng.uniform(np.log(1e-5), np.log(1e-2))))
+        x = spectral_field_torch(shape, seed=seed * 100003 + i, device=device, dtype=dt)
+        out.append((x, rel))
+    return out

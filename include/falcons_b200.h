@@ -122,6 +122,36 @@ int falcons_encode_codes(falcons_ctx *ctx, const int16_t *d_codes, size_t n, voi
                          size_t *out_len, void *stream);
 int falcons_decode_codes(falcons_ctx *ctx, const void *d_in, size_t len, size_t n, int16_t *d_codes, void *stream);
 
+/* ---- batches of fields (device memory) ----
+ *
+ * Many independent fields in one call: every item is one Falcons_compress or Falcons_decompress
+ * of a field in device memory (api/falcons.hpp:54,158; the reference's per-field driver is
+ * api/impl/FalconsAlgoInterp.hpp:33-69, one call per field).  The items run concurrently on
+ * worker threads of the context, each with its own stream and scratch, largest first, so the
+ * small kernels and host steps of many fields overlap on the GPU; every item's stream and
+ * reconstruction are the bits a single falcons_compress_device / falcons_decompress_device call
+ * gives.  `workers` <= 0 lets the context's autotuner choose the worker count for the batch's
+ * field-size class (tuned on the first batch of that class, kept for the next ones).
+ *
+ * Per item: compress reads conf, d_data (the field, overwritten with the partial reconstruction),
+ * d_stream and cap (its capacity in bytes) and writes len and conf (as stored in the stream);
+ * decompress reads d_stream and len and writes d_data (cap: its capacity in elements) and conf.
+ * status is FALCONS_OK or the item's own error; the call returns FALCONS_OK when every item
+ * succeeded, else the first failed item's status (its message names the item). */
+typedef struct {
+    int32_t dtype;          /* FALCONS_DTYPE_F32 or FALCONS_DTYPE_F64 */
+    int32_t status;         /* out */
+    falcons_config conf;
+    void *d_data;
+    void *d_stream;
+    size_t cap;
+    size_t len;
+} falcons_batch_item;
+int falcons_compress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers);
+int falcons_decompress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers);
+/* The worker count the autotuner chose for fields of about field_bytes bytes (0: not tuned yet). */
+int falcons_batch_workers(falcons_ctx *ctx, size_t field_bytes);
+
 /* ---- allocation-free decompress (no counterpart in the reference) ----
  *
  * falcons_interp_decompress without a context and without any device allocation: the same

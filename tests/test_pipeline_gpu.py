@@ -274,10 +274,11 @@ DISPATCH_CASES = [
 
 @pytest.mark.parametrize("K,noise,ebr,algo", DISPATCH_CASES)
 def test_low_ratio_switch_matches_reference_choice(cuda, reference, K, noise, ebr, algo):
-    """The GPU makes the reference's lossy-or-lossless choice on fields near the switch.  The
-    lossy size it compares is its own zstd section, within a fraction of a percent of the
-    reference's, so the choices can differ only for fields whose zstd size falls inside that
-    sliver; these cases keep at least 1 % away from it."""
+    """The GPU makes the reference's lossy-or-lossless choice on fields near the switch.  Like the
+    reference, it compares zstd level 3 of the field with zstd level 3 of its lossy payload,
+    whose size is within a fraction of a percent of the reference's, so the choices can differ
+    only for fields whose zstd size falls inside that sliver; these cases keep at least 1 % away
+    from it."""
     import oracle
     from falcons_b200 import api, synth
     base = synth.sinusoid_field((48, 64, 80), seed=5, noise=0.0)
