@@ -414,7 +414,7 @@ def main():
 
     # ---- live roofline of the prediction + quantization stage (interpolation kernels)
     eb_abs = args.rel * float(x0.max() - x0.min())
-    p = D.interp_params(eb_abs, 1, 0, None, 3)
+    p = D.interp_params(eb_abs, 1, 0, None, 3, max_abs=float(x0.abs().max()))
     pq = []
     pqd = []
     for it in range(4):

@@ -24,7 +24,7 @@ class FalconsError(RuntimeError):
 class InterpParams(ctypes.Structure):
     _fields_ = [("eb", ctypes.c_double), ("interp_algo", ctypes.c_int32), ("direction", ctypes.c_int32),
                 ("anchor_stride", ctypes.c_int64), ("alpha", ctypes.c_double), ("beta", ctypes.c_double),
-                ("radius", ctypes.c_int32), ("tuning", ctypes.c_int32)]
+                ("radius", ctypes.c_int32), ("tuning", ctypes.c_int32), ("max_abs", ctypes.c_double)]
 
 
 class Config(ctypes.Structure):

@@ -1,7 +1,7 @@
 // Batches of fields (batch.cuh): a worker per host thread, each with its own context, fields
-// handed out largest first; the worker count per field-size class is tuned on the first batch of
-// that class (successive slices of the batch run with 2, 4, 8 and 16 workers, and the count with
-// the highest field bytes per second is kept).
+// handed out largest first; the worker count per direction and field-size class is tuned on the
+// first batch of that class (successive slices of the batch run with 2, 4, 8 and 16 workers, and
+// the count with the highest field bytes per second is kept).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -111,7 +111,7 @@ double run_range(BatchPool &bp, bool compress, falcons_batch_item *items, const 
 
 int batch_tuned_workers(BatchPool &bp, size_t bytes) {
     std::lock_guard<std::mutex> lk(bp.mu);
-    auto it = bp.best.find(size_class(bytes));
+    auto it = bp.best.find(2 * size_class(bytes) + 1);
     return it == bp.best.end() ? 0 : it->second;
 }
 
@@ -133,31 +133,35 @@ void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n
     size_t pos = 0;
     int W = workers > 0 ? std::min(workers, kMaxWorkers) : 0;
     if (W == 0) {
-        const int cls = size_class(total / n);
-        auto found = bp.best.find(cls);
+        const int key = 2 * size_class(total / n) + (compress ? 1 : 0);  // tuned per direction
+        auto found = bp.best.find(key);
         if (found != bp.best.end()) {
             W = found->second;
         } else {
-            // tune on the batch's own fields, in their given order (a mix of sizes)
+            // tune on the batch's own fields, in their given order (a mix of sizes): per candidate
+            // count, a slice of w fields that is not timed (the workers' first calls size their
+            // scratch), then a timed slice of 3 w fields
             double best_rate = 0;
             int best_w = 0, measured = 0;
             for (int w : {2, 4, 8, 16}) {
-                const size_t take = std::min(n - pos, (size_t)(3 * w));
-                if (take < (size_t)w) break;
+                const size_t take = std::min(n - pos, (size_t)(4 * w));
+                if (take < (size_t)(4 * w)) break;
                 ensure_workers(bp, w);
-                const double s = run_range(bp, compress, items, order, pos, pos + take, w, errs);
+                run_range(bp, compress, items, order, pos, pos + w, w, errs);
+                pos += w;
+                const double s = run_range(bp, compress, items, order, pos, pos + 3 * w, w, errs);
                 size_t b = 0;
-                for (size_t k = pos; k < pos + take; k++) b += bytes[order[k]];
+                for (size_t k = pos; k < pos + 3 * w; k++) b += bytes[order[k]];
                 const double rate = s > 0 ? (double)b / s : 0;
                 if (rate > best_rate) {
                     best_rate = rate;
                     best_w = w;
                 }
                 measured++;
-                pos += take;
+                pos += 3 * w;
             }
             W = best_w ? best_w : 8;
-            if (measured >= 2) bp.best[cls] = W;
+            if (measured >= 2) bp.best[key] = W;
         }
     }
     // the rest, largest first

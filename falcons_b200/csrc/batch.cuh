@@ -18,7 +18,7 @@ struct BatchPool {
     int device = 0;
     std::mutex mu;                                  // one batch at a time per pool
     std::vector<std::unique_ptr<Context>> workers;  // created on first use, kept for reuse
-    std::map<int, int> best;                        // tuned worker count per field-size class
+    std::map<int, int> best;                        // tuned worker count per (field-size class, direction)
 };
 
 // Runs items[0, n): compress (d_data -> d_stream) or decompress (d_stream -> d_data).  `workers`
@@ -26,7 +26,8 @@ struct BatchPool {
 // the items' status; the call itself fails only on argument or set-up errors.
 void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n, int workers);
 
-// The worker count the autotuner settled on for fields of about `bytes` bytes (0: not tuned).
+// The worker count the autotuner settled on for compressing fields of about `bytes` bytes (0: not
+// tuned).
 int batch_tuned_workers(BatchPool &bp, size_t bytes);
 
 }  // namespace fb2

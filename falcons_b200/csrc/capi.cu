@@ -62,10 +62,33 @@ fb2::InterpParams to_params(const falcons_interp_params *p) {
     q.beta = p->beta;
     q.radius = p->radius;
     q.tuning = p->tuning;
+    q.max_abs = p->max_abs;
     return q;
 }
 
 cudaStream_t pick(falcons_ctx *ctx, void *s) { return s ? static_cast<cudaStream_t>(s) : ctx->c.stream; }
+
+// The largest |value| of a device field of dims[0..N) (fb2::InterpParams::max_abs).
+double measured_max_abs(falcons_ctx *ctx, int dtype, const void *d_data, const long long *dims, int N, cudaStream_t st) {
+    long long n = 1;
+    for (int i = 0; i < N && i < 4; i++) n *= std::max<long long>(dims[i], 0);
+    if (n <= 0) return 0;
+    void *ws = ctx->c.work2.get(fb2::range_workspace_bytes());
+    void *res = ctx->c.small.get(64);
+    double h[3] = {0, 0, 0};
+    if (dtype == FALCONS_DTYPE_F32) {
+        fb2::device_range<float>(static_cast<const float *>(d_data), n, static_cast<float *>(res), ws, st);
+        float f[3];
+        FB2_CUDA(cudaMemcpyAsync(f, res, sizeof f, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < 3; i++) h[i] = f[i];
+    } else {
+        fb2::device_range<double>(static_cast<const double *>(d_data), n, static_cast<double *>(res), ws, st);
+        FB2_CUDA(cudaMemcpyAsync(h, res, sizeof h, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+    }
+    return std::max(std::fabs(h[1]), std::fabs(h[2]));
+}
 
 void check_ctx(falcons_ctx *ctx) {
     if (!ctx) throw std::invalid_argument("null context");
@@ -139,11 +162,13 @@ int falcons_interp_compress(falcons_ctx *ctx, int dtype, const size_t *dims, int
         std::lock_guard<std::mutex> lk(ctx->c.mu);
         long long d[4];
         for (int i = 0; i < N && i < 4; i++) d[i] = (long long)dims[i];
-        const fb2::InterpPlan plan = fb2::make_plan(d, N, to_params(p));
+        fb2::InterpParams prm = to_params(p);
+        cudaStream_t st = pick(ctx, stream);
+        if (!(prm.max_abs >= 0)) prm.max_abs = measured_max_abs(ctx, dtype, d_data, d, N, st);
+        const fb2::InterpPlan plan = fb2::make_plan(d, N, prm);
         const int es = dtype == FALCONS_DTYPE_F32 ? 4 : 8;
         void *ws = ctx->c.work.get(fb2::interp_workspace_bytes(plan, es));
         auto *cnt = static_cast<unsigned long long *>(ctx->c.small.get(64));
-        cudaStream_t st = pick(ctx, stream);
         if (dtype == FALCONS_DTYPE_F32)
             fb2::interp_compress<float>(plan, static_cast<float *>(d_data), d_codes, static_cast<float *>(d_unpred),
                                         ws, cnt, st);

@@ -248,6 +248,7 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p) {
 
     InterpPlan P;
     P.N = N;
+    P.max_abs = p.max_abs;
     P.num = 1;
     for (int d = 0; d < N; d++) {
         if (dims[d] < 1) throw std::invalid_argument("zero-sized dimension");
@@ -313,10 +314,16 @@ constexpr int kTile = 4096;         // codes per escape-scan tile
 constexpr int kTileThreads = 256;   // 16 codes per thread
 constexpr int kPassThreads = 256;
 
+// Compress: one more escape in the tile of kTile codes holding code position p (the escape scan's
+// tile counts, gathered while the passes code).
+__device__ __forceinline__ void count_escape(unsigned *etile, long long p) {
+    if (etile) atomicAdd(etile + p / kTile, 1u);
+}
+
 template <class T, int KIND, bool DECOMP>
 __global__ void __launch_bounds__(kPassThreads) k_pass(const PassLaunch L, T *__restrict__ x,
                                                       int16_t *__restrict__ codes, T *__restrict__ esc,
-                                                      const QParams qp) {
+                                                      const QParams qp, unsigned *__restrict__ etile) {
     const long long cstride = (long long)gridDim.x * blockDim.x;
     for (long long a = blockIdx.z; a < L.A; a += gridDim.z) {
         for (long long b = blockIdx.y; b < L.B; b += gridDim.y) {
@@ -406,8 +413,12 @@ __global__ void __launch_bounds__(kPassThreads) k_pass(const PassLaunch L, T *__
                     T recon;
                     const int q = quantize<T>(v, pred, qp, recon);
                     codes[p] = (int16_t)q;
-                    if (q == -qp.radius) esc[p] = v;
-                    else if (!L.skip) *xp = recon;
+                    if (q == -qp.radius) {
+                        esc[p] = v;
+                        count_escape(etile, p);
+                    } else if (!L.skip) {
+                        *xp = recon;
+                    }
                 } else {
                     const int q = codes[p];
                     *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
@@ -418,14 +429,18 @@ __global__ void __launch_bounds__(kPassThreads) k_pass(const PassLaunch L, T *__
 }
 
 template <class T, bool DECOMP>
-__global__ void k_first_point(T *x, int16_t *codes, T *esc, const QParams qp) {
+__global__ void k_first_point(T *x, int16_t *codes, T *esc, const QParams qp, unsigned *etile) {
     if (!DECOMP) {
         T recon;
         const T v = x[0];
         const int q = quantize<T>(v, T(0), qp, recon);
         codes[0] = (int16_t)q;
-        if (q == -qp.radius) esc[0] = v;
-        else x[0] = recon;
+        if (q == -qp.radius) {
+            esc[0] = v;
+            count_escape(etile, 0);
+        } else {
+            x[0] = recon;
+        }
     } else {
         const int q = codes[0];
         x[0] = q != -qp.radius ? dequantize<T>(q, T(0), qp) : esc[0];
@@ -611,13 +626,18 @@ __device__ __forceinline__ T linear_pred(T a, T b) {
 // reconstructs (decompress) one target; p is its position in the code stream.
 template <class T, bool DECOMP>
 __device__ __forceinline__ void pass_target(T *__restrict__ xp, T v, T pred, int16_t *__restrict__ cp,
-                                            T *__restrict__ ep, const QParams &qp, bool skip) {
+                                            T *__restrict__ ep, const QParams &qp, bool skip, unsigned *etile,
+                                            long long p) {
     if (!DECOMP) {
         T recon;
         const int q = quantize<T>(v, pred, qp, recon);
         *cp = (int16_t)q;
-        if (q == -qp.radius) *ep = v;
-        else if (!skip) *xp = recon;
+        if (q == -qp.radius) {
+            *ep = v;
+            count_escape(etile, p);
+        } else if (!skip) {
+            *xp = recon;
+        }
     } else {
         const int q = *cp;
         *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : *ep;
@@ -631,7 +651,7 @@ constexpr int kRowsPerBlock = 8;
 template <class T, bool DECOMP>
 __global__ void __launch_bounds__(kPassThreads) k_row_fast(const PassLaunch L, T *__restrict__ x,
                                                           int16_t *__restrict__ codes, T *__restrict__ esc,
-                                                          const QParams qp) {
+                                                          const QParams qp, unsigned *__restrict__ etile) {
     const long long cstride = (long long)gridDim.x * blockDim.x;
     const long long st = L.step;
     for (long long a = blockIdx.z; a < L.A; a += gridDim.z) {
@@ -656,7 +676,8 @@ __global__ void __launch_bounds__(kPassThreads) k_row_fast(const PassLaunch L, T
                     pred = apply_formula<T>(r.f, o0, o1, o2, o3);
                 }
                 T *xp = xl + (long long)t * st;
-                pass_target<T, DECOMP>(xp, DECOMP ? T(0) : *xp, pred, codes + prow + c, esc + prow + c, qp, L.skip);
+                pass_target<T, DECOMP>(xp, DECOMP ? T(0) : *xp, pred, codes + prow + c, esc + prow + c, qp, L.skip, etile,
+                                       prow + c);
             }
         }
     }
@@ -671,7 +692,7 @@ constexpr int kLineMax = 4096;
 template <class T, bool DECOMP>
 __global__ void __launch_bounds__(kLineThreads) k_line_smem(const PassLaunch L, T *__restrict__ x,
                                                            int16_t *__restrict__ codes, T *__restrict__ esc,
-                                                           const QParams qp) {
+                                                           const QParams qp, unsigned *__restrict__ etile) {
     __shared__ T buf[kLineThreads / 32][kLineMax / sizeof(T)];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     T *bw = buf[wid];
@@ -706,25 +727,27 @@ __global__ void __launch_bounds__(kLineThreads) k_line_smem(const PassLaunch L, 
                 const T o3 = r.f == F_CUBIC ? bw[r.o3] : o0;
                 pred = apply_formula<T>(r.f, o0, o1, o2, o3);
             }
-            pass_target<T, DECOMP>(xl + (long long)t * st, bw[t], pred, cl + cc, el + cc, qp, L.skip);
+            pass_target<T, DECOMP>(xl + (long long)t * st, bw[t], pred, cl + cc, el + cc, qp, L.skip, etile,
+                                   L.p_base + l * L.C + cc);
         }
     }
 }
 
 template <class T, bool DECOMP>
-void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
+void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParams &qp, unsigned *etile,
+                 cudaStream_t st) {
     if (L.kind == KIND_ROW) {
         dim3 grid((unsigned)std::max<long long>(1, std::min<long long>((L.C + kPassThreads - 1) / kPassThreads, 1 << 20)),
                   (unsigned)std::min<long long>((L.B + kRowsPerBlock - 1) / kRowsPerBlock, 65535),
                   (unsigned)std::min<long long>(L.A, 65535));
-        k_row_fast<T, DECOMP><<<grid, kPassThreads, 0, st>>>(L, x, codes, esc, qp);
+        k_row_fast<T, DECOMP><<<grid, kPassThreads, 0, st>>>(L, x, codes, esc, qp, etile);
         FB2_CHECK_LAUNCH();
         return;
     }
     if (L.kind == KIND_LINE && (long long)L.n * (long long)sizeof(T) <= kLineMax) {
         const long long nlines = L.A * L.B;
         const long long blocks = std::min<long long>((nlines + kLineThreads / 32 - 1) / (kLineThreads / 32), 148LL * 64);
-        k_line_smem<T, DECOMP><<<(unsigned)std::max<long long>(blocks, 1), kLineThreads, 0, st>>>(L, x, codes, esc, qp);
+        k_line_smem<T, DECOMP><<<(unsigned)std::max<long long>(blocks, 1), kLineThreads, 0, st>>>(L, x, codes, esc, qp, etile);
         FB2_CHECK_LAUNCH();
         return;
     }
@@ -733,10 +756,10 @@ void launch_pass(const PassLaunch &L, T *x, int16_t *codes, T *esc, const QParam
     dim3 grid((unsigned)std::max<long long>(gx, 1), (unsigned)std::min<long long>(L.B, 65535),
               (unsigned)std::min<long long>(L.A, 65535));
     switch (L.kind) {
-        case KIND_ROW: k_pass<T, KIND_ROW, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
-        case KIND_LINE: k_pass<T, KIND_LINE, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
-        case KIND_GENERIC: k_pass<T, KIND_GENERIC, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
-        default: k_pass<T, KIND_LEGACY, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp); break;
+        case KIND_ROW: k_pass<T, KIND_ROW, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp, etile); break;
+        case KIND_LINE: k_pass<T, KIND_LINE, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp, etile); break;
+        case KIND_GENERIC: k_pass<T, KIND_GENERIC, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp, etile); break;
+        default: k_pass<T, KIND_LEGACY, DECOMP><<<grid, block, 0, st>>>(L, x, codes, esc, qp, etile); break;
     }
     FB2_CHECK_LAUNCH();
 }
@@ -766,7 +789,7 @@ constexpr int kFuseThreads = 256;
 template <class T, bool DECOMP>
 __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fused(const FusedYX F, T *__restrict__ xf,
                                                            int16_t *__restrict__ codes, T *__restrict__ esc,
-                                                           const QParams qp) {
+                                                           const QParams qp, unsigned *__restrict__ etile) {
     __shared__ __align__(16) T tile[kFusePR * kFusePW];
     constexpr int P = kFusePW, H = kFuseHalo;
     const int ny = F.y.n, nx = F.x.n;
@@ -836,7 +859,10 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
                 const int q = quantize<T>(v, pred, qp, recon);
                 if (own) codes[p] = (int16_t)q;
                 if (q == -qp.radius) {
-                    if (own) esc[p] = v;
+                    if (own) {
+                        esc[p] = v;
+                        count_escape(etile, p);
+                    }
                 } else if (!F.z.skip) {
                     *xp = recon;
                 }
@@ -881,7 +907,10 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
                 const int q = quantize<T>(v, pred, qp, recon);
                 if (own) codes[p] = (int16_t)q;
                 if (q == -qp.radius) {
-                    if (own) esc[p] = v;
+                    if (own) {
+                        esc[p] = v;
+                        count_escape(etile, p);
+                    }
                 } else if (!F.y.skip) {
                     *xp = recon;
                 }
@@ -920,8 +949,12 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
                 const T v = *xp;
                 const int q = quantize<T>(v, pred, qp, recon);
                 codes[p] = (int16_t)q;
-                if (q == -qp.radius) esc[p] = v;
-                else if (!F.x.skip) *xp = recon;
+                if (q == -qp.radius) {
+                    esc[p] = v;
+                    count_escape(etile, p);
+                } else if (!F.x.skip) {
+                    *xp = recon;
+                }
             } else {
                 const int q = codes[p];
                 *xp = (q != -qp.radius) ? dequantize<T>(q, pred, qp) : esc[p];
@@ -944,103 +977,91 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
 }
 
 // The level whose grid step is one element (the finest level, 7/8 of the codes) of a float field
-// whose rows are 16-byte aligned: the same passes, tiles and code positions as k_yx_fused, with
-// the tile's even and odd columns kept apart in shared memory, so that a thread takes four
-// consecutive targets at a time with 16-byte shared-memory loads and stores and one 8-byte code
-// store:
+// whose rows are 16-byte aligned: the passes, tiles and code positions of k_yx_fused, with the
+// tile's even and odd columns kept apart in shared memory so that a thread takes four consecutive
+// targets of a row at a time (16-byte shared-memory loads and stores, one 8-byte code store):
 //   tile column c <-> x = x0 - 4 + c; row r <-> y = y0 - 4 + r (72 x 72: 64 + a halo of 4)
-//   E[r * 40 + e + 2]  even column c = 2e      (own even columns: e in [2, 34))
-//   O[r * 40 + m + 2]  odd column c = 2m + 1   (own odd columns:  m in [2, 34))
-// The z and y passes take the own even columns in 8 groups of four per row (their operand rows
-// are 16-byte loads) plus the four halo columns (x0 - 4, x0 - 2, x0 + 64, x0 + 66) one by one;
-// the x pass takes the own odd columns in 8 groups of four (operands: eight consecutive even
-// columns).  Targets whose rule is not the cubic interior one, or whose columns leave the field,
-// take the rule path one by one.
-constexpr int kL1Rows = 72, kL1S = 40;
+//   E[r * 40 + e]      even column c = 2e        (e in [0, 36))
+//   O[r * 40 + m + 2]  odd column c = 2m + 1     (own odd columns: m in [2, 34))
+// Every pass covers whole groups of four, the halo included, so that the lanes of a warp run the
+// same code: the z pass (odd planes) the even rows y0 - 2 .. y0 + 66 x the 36 even columns
+// x0 - 4 .. x0 + 66, the y pass the odd rows of the tile x the same columns, the x pass the rows
+// of the tile x its 32 odd columns.  Targets outside the tile (the halo; their codes belong to the
+// neighbouring tiles, but the y and x passes read their values) are recomputed and not stored,
+// and targets outside the field are computed from don't-care values and not stored either.
+// A plane's z rule is the same for the whole CTA; the y and x rules leave the interior cubic one
+// only in the tiles at the field's edges.
+constexpr int kL1Rows = 72, kL1S = 40, kL1Groups = 9;
 constexpr int kL1Threads = 256;
 
-__device__ __forceinline__ float &l1_even(float *E, int r, int e) { return E[r * kL1S + e + 2]; }
-__device__ __forceinline__ float &l1_odd(float *O, int r, int m) { return O[r * kL1S + m + 2]; }
+__device__ __forceinline__ float *l1_e(float *E, int r, int e) { return E + r * kL1S + e; }
+__device__ __forceinline__ float *l1_o(float *O, int r, int m) { return O + r * kL1S + m + 2; }
 // the value at tile column c of row r
 __device__ __forceinline__ float l1_at(float *E, float *O, int r, int c) {
-    return (c & 1) ? l1_odd(O, r, (c - 1) >> 1) : l1_even(E, r, c >> 1);
+    return (c & 1) ? *l1_o(O, r, (c - 1) >> 1) : *l1_e(E, r, c >> 1);
 }
 
-// Four consecutive codes at p (n of them valid): one 8-byte access when aligned.
-__device__ __forceinline__ void l1_store4(int16_t *__restrict__ codes, long long p, const int *q, int n) {
-    if (n == 4 && (p & 3) == 0) {
-        *reinterpret_cast<uint2 *>(codes + p) =
-            make_uint2((uint32_t)(q[0] & 0xFFFF) | ((uint32_t)q[1] << 16), (uint32_t)(q[2] & 0xFFFF) | ((uint32_t)q[3] << 16));
-    } else {
-        for (int k = 0; k < n; k++) codes[p + k] = (int16_t)q[k];
-    }
-}
-__device__ __forceinline__ void l1_load4(const int16_t *__restrict__ codes, long long p, int *q, int n) {
-    if (n == 4 && (p & 3) == 0) {
-        const uint2 w = *reinterpret_cast<const uint2 *>(codes + p);
-        q[0] = (int16_t)(w.x & 0xFFFF);
-        q[1] = (int16_t)(w.x >> 16);
-        q[2] = (int16_t)(w.y & 0xFFFF);
-        q[3] = (int16_t)(w.y >> 16);
-    } else {
-        for (int k = 0; k < n; k++) q[k] = codes[p + k];
-    }
-}
-
-// Quantizes (compress) or reconstructs (decompress) the n valid targets of a group of four whose
-// values are v and predictions pred, codes at p..p+3 (written when `own`); v receives the new
-// values (compress: the reconstructions unless the pass is `skip` or the value escapes).
+// Quantizes (compress) or reconstructs (decompress) four targets at consecutive code positions
+// p .. p + 3, of values v and predictions pred.  `valid` (bit k: target k lies in the field) and
+// `own` (bit k: its code belongs to this tile) select the code and escape slots read
+// (decompress) and written (compress); compress leaves the reconstructions in v when `keep` (the
+// reference overwrites in every pass but the last of level 1).
 template <bool DECOMP>
-__device__ __forceinline__ void l1_group(float *v, const float *pred, int n, long long p, bool own, bool skip,
-                                         int16_t *__restrict__ codes, float *__restrict__ esc, const QParams &qp) {
+__device__ __forceinline__ void l1_quad(float (&v)[4], const float (&pred)[4], int16_t *__restrict__ codes,
+                                        float *__restrict__ esc, long long p, unsigned valid, unsigned own, bool keep,
+                                        const QParams &qp, unsigned *__restrict__ etile) {
+    int16_t *cp = codes + p;
+    const bool vec = (reinterpret_cast<uintptr_t>(cp) & 7u) == 0;
     int q[4];
     if (!DECOMP) {
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            if (k >= n) break;
             float recon;
             q[k] = quantize<float>(v[k], pred[k], qp, recon);
-            if (q[k] == -qp.radius) {
-                if (own) esc[p + k] = v[k];
-            } else if (!skip) {
-                v[k] = recon;
+            if (q[k] == -qp.radius && ((own >> k) & 1u)) {
+                esc[p + k] = v[k];
+                count_escape(etile, p + k);
             }
+            if (keep) v[k] = recon;  // the value itself when it escaped
         }
-        if (own) l1_store4(codes, p, q, n);
-    } else {
-        l1_load4(codes, p, q, n);
+        if (own == 0xFu && vec) {
+            *reinterpret_cast<uint2 *>(cp) = make_uint2((uint32_t)(q[0] & 0xFFFF) | ((uint32_t)q[1] << 16),
+                                                        (uint32_t)(q[2] & 0xFFFF) | ((uint32_t)q[3] << 16));
+        } else {
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (k >= n) break;
-            v[k] = (q[k] != -qp.radius) ? dequantize<float>(q[k], pred[k], qp) : esc[p + k];
-        }
-    }
-}
-
-// One target by itself (halo columns, partial groups).
-template <bool DECOMP>
-__device__ __forceinline__ void l1_one(float &slot, float pred, long long p, bool own, bool skip,
-                                       int16_t *__restrict__ codes, float *__restrict__ esc, const QParams &qp) {
-    if (!DECOMP) {
-        float recon;
-        const float v = slot;
-        const int q = quantize<float>(v, pred, qp, recon);
-        if (own) codes[p] = (int16_t)q;
-        if (q == -qp.radius) {
-            if (own) esc[p] = v;
-        } else if (!skip) {
-            slot = recon;
+            for (int k = 0; k < 4; k++)
+                if ((own >> k) & 1u) cp[k] = (int16_t)q[k];
         }
     } else {
-        const int q = codes[p];
-        slot = (q != -qp.radius) ? dequantize<float>(q, pred, qp) : esc[p];
+        if (valid == 0xFu && vec) {
+            const uint2 w = *reinterpret_cast<const uint2 *>(cp);
+            q[0] = (int16_t)(w.x & 0xFFFF);
+            q[1] = (int16_t)(w.x >> 16);
+            q[2] = (int16_t)(w.y & 0xFFFF);
+            q[3] = (int16_t)(w.y >> 16);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) q[k] = ((valid >> k) & 1u) ? (int)cp[k] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            v[k] = (q[k] != -qp.radius) ? dequantize<float>(q[k], pred[k], qp) : ((valid >> k) & 1u) ? esc[p + k] : 0.f;
     }
 }
 
+// bit k set when a + 2 k lies in [lo, hi)
+__device__ __forceinline__ unsigned l1_mask(int a, int lo, int hi) {
+    if (a >= lo && a + 6 < hi) return 0xFu;
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) m |= (a + 2 * k >= lo && a + 2 * k < hi) ? (1u << k) : 0u;
+    return m;
+}
+
 template <bool DECOMP>
-__global__ void __launch_bounds__(kL1Threads, 5) k_l1_fused(const FusedYX F, float *__restrict__ xf,
+__global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, float *__restrict__ xf,
                                                             int16_t *__restrict__ codes, float *__restrict__ esc,
-                                                            const QParams qp) {
+                                                            const QParams qp, unsigned *__restrict__ etile) {
     __shared__ __align__(16) float E[kL1Rows * kL1S];
     __shared__ __align__(16) float O[kL1Rows * kL1S];
     const int ny = F.y.n, nx = F.x.n;
@@ -1079,153 +1100,132 @@ __global__ void __launch_bounds__(kL1Threads, 5) k_l1_fused(const FusedYX F, flo
             const int idx = base + tid + k * kL1Threads;
             if (idx >= NV) break;
             const int r = idx / 18, i = idx - r * 18;
-            *reinterpret_cast<float2 *>(&l1_even(E, r, 2 * i)) = make_float2(v[k].x, v[k].z);
-            *reinterpret_cast<float2 *>(&l1_odd(O, r, 2 * i)) = make_float2(v[k].y, v[k].w);
+            *reinterpret_cast<float2 *>(l1_e(E, r, 2 * i)) = make_float2(v[k].x, v[k].z);
+            *reinterpret_cast<float2 *>(l1_o(O, r, 2 * i)) = make_float2(v[k].y, v[k].w);
         }
     }
     __syncthreads();
-    // ---- z pass of an odd plane: even rows x even columns of the tile (halo included)
+    // ---- z pass of an odd plane t = a: even rows x even columns, operands in the even planes
+    // around it (points of coarser levels, which this level never writes)
     const bool zplane = F.has_z && (a & 1);
     if (zplane) {
         const int nz = F.z.n, t = a;
         const bool zl = F.has_zlate && t == nz - 1;
+        const long long zb = zl ? F.zlate.p_base : F.z.p_base + ((long long)((t - 1) >> 1) + F.z.b_off) * F.z.C;
+        const long long zr = zl ? F.zlate.C : F.z.rows_in_group * F.z.C;
         const bool inner = t >= 3 && t <= nz - 5;
         const Rule rz = row_rule(true, t, nz, F.z.skip);
-        for (int task = tid; task < 36 * 9; task += kL1Threads) {
-            const int rr = task / 9, g = task - rr * 9;
-            const int r = 2 * rr, y = yo + r;
+        const float *q0 = xf + (long long)rz.o0 * sz;
+        const float *q1 = xf + (long long)(rz.f != F_EQUAL ? rz.o1 : rz.o0) * sz;
+        const float *q2 = xf + (long long)(rz.f >= F_QUAD1 ? rz.o2 : rz.o0) * sz;
+        const float *q3 = xf + (long long)(rz.f == F_CUBIC ? rz.o3 : rz.o0) * sz;
+        for (int i = tid; i < 35 * kL1Groups; i += kL1Threads) {
+            const int rr = i / kL1Groups, g = i - kL1Groups * rr;
+            const int r = 2 + 2 * rr, y = yo + r;
             if (y < 0 || y >= ny) continue;
-            const bool own_row = y >= y0 && y < y1;
-            const long long ay = y >> 1;
-            const long long pb = zl ? F.zlate.p_base + ay * F.zlate.C
-                                    : F.z.p_base + (ay * F.z.rows_in_group + ((t - 1) >> 1) + F.z.b_off) * F.z.C;
-            const float *col = xf + (long long)y * sy;  // col[z * sz + x] is (z, y, x)
-            auto pred_at = [&](int x) -> float {
-                const float *c1 = col + x;
-                if (inner) return cubic_pred<float>(c1[(t - 3) * sz], c1[(t - 1) * sz], c1[(t + 1) * sz], c1[(t + 3) * sz]);
-                const float o0 = c1[rz.o0 * sz];
-                const float o1 = rz.f != F_EQUAL ? c1[rz.o1 * sz] : o0;
-                const float o2 = rz.f >= F_QUAD1 ? c1[rz.o2 * sz] : o0;
-                const float o3 = rz.f == F_CUBIC ? c1[rz.o3 * sz] : o0;
-                return apply_formula<float>(rz.f, o0, o1, o2, o3);
-            };
-            if (g < 8) {
-                const int xa = x0 + 8 * g;  // targets xa, xa + 2, xa + 4, xa + 6
-                const int n = min(4, max(0, (x1 - xa + 1) / 2));
-                if (n == 0) continue;
-                float *slot = &l1_even(E, r, 2 + 4 * g);
-                float4 cur = *reinterpret_cast<const float4 *>(slot);
-                float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
-                if (inner && n == 4) {
-                    float o[4][4];
+            const int xg = xo + 8 * g;  // targets xg, xg + 2, xg + 4, xg + 6
+            const unsigned valid = l1_mask(xg, 0, nx);
+            const unsigned own = (y >= y0 && y < y1) ? l1_mask(xg, x0, x1) : 0u;
+            float *slot = l1_e(E, r, 4 * g);
+            const float4 cur = *reinterpret_cast<const float4 *>(slot);
+            float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
+            const long long off = (long long)y * sy + xg;
+            if (xg >= 0 && xg + 7 < nx) {
+                float o[4][4];
+                const float *qs[4] = {q0, q1, q2, q3};
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const float4 *src = reinterpret_cast<const float4 *>(col + (long long)(t - 3 + 2 * j) * sz + xa);
-                        const float4 lo = __ldg(src), hi = __ldg(src + 1);
-                        o[j][0] = lo.x;
-                        o[j][1] = lo.z;
-                        o[j][2] = hi.x;
-                        o[j][3] = hi.z;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 4; k++) pred[k] = cubic_pred<float>(o[0][k], o[1][k], o[2][k], o[3][k]);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; k++) pred[k] = k < n ? pred_at(xa + 2 * k) : 0.f;
+                for (int j = 0; j < 4; j++) {
+                    const float4 *src = reinterpret_cast<const float4 *>(qs[j] + off);
+                    const float4 lo = __ldg(src), hi = __ldg(src + 1);
+                    o[j][0] = lo.x;
+                    o[j][1] = lo.z;
+                    o[j][2] = hi.x;
+                    o[j][3] = hi.z;
                 }
-                l1_group<DECOMP>(v, pred, n, pb + (xa >> 1), own_row, F.z.skip, codes, esc, qp);
-                *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    pred[k] = inner ? cubic_pred<float>(o[0][k], o[1][k], o[2][k], o[3][k])
+                                    : apply_formula<float>(rz.f, o[0][k], o[1][k], o[2][k], o[3][k]);
             } else {
-                for (int h = 0; h < 4; h++) {
-                    const int e = h < 2 ? h : 32 + h, x = xo + 2 * e;  // columns x0 - 4, x0 - 2, x0 + 64, x0 + 66
-                    if (x < 0 || x >= nx) continue;
-                    l1_one<DECOMP>(l1_even(E, r, e), pred_at(x), pb + (x >> 1), false, F.z.skip, codes, esc, qp);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    pred[k] = 0.f;
+                    if (!((valid >> k) & 1u)) continue;
+                    const long long ok = off + 2 * k;
+                    pred[k] = apply_formula<float>(rz.f, __ldg(q0 + ok), __ldg(q1 + ok), __ldg(q2 + ok), __ldg(q3 + ok));
                 }
             }
+            l1_quad<DECOMP>(v, pred, codes, esc, zb + (long long)(y >> 1) * zr + (xg >> 1), valid, own, !F.z.skip, qp, etile);
+            *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
         }
         __syncthreads();
     }
-    // ---- y pass: odd rows of [y0, y1) x even columns of the tile (halo included)
+    // ---- y pass: odd rows of [y0, y1) x even columns (halo included)
     {
-        const int nrows = (y1 - y0) / 2;  // odd rows y0 + 1, y0 + 3, ... below y1
-        for (int task = tid; task < nrows * 9; task += kL1Threads) {
-            const int tr = task / 9, g = task - tr * 9;
-            const int t = y0 + 1 + 2 * tr, r = t - yo;
+        const int nyr = (y1 - y0) >> 1;  // odd rows y0 + 1, y0 + 3, ... below y1
+        const long long ya = (long long)a * F.y.rows_in_group + F.y.b_off;
+        for (int i = tid; i < nyr * kL1Groups; i += kL1Threads) {
+            const int k2 = i / kL1Groups, g = i - kL1Groups * k2;
+            const int t = y0 + 1 + 2 * k2, r = t - yo;
+            const int xg = xo + 8 * g;
+            const unsigned valid = l1_mask(xg, 0, nx);
+            const unsigned own = l1_mask(xg, x0, x1);
             const bool late = F.has_late && t == ny - 1;
-            const long long pb = late ? F.late.p_base + (long long)a * F.late.C
-                                      : F.y.p_base + ((long long)a * F.y.rows_in_group + ((t - 1) >> 1) + F.y.b_off) * F.y.C;
-            const bool inner = t >= 3 && t <= ny - 5;
-            const Rule ry = row_rule(true, t, ny, F.y.skip);
-            auto pred_at = [&](int e) -> float {  // column e, rows of the rule
-                if (inner)
-                    return cubic_pred<float>(l1_even(E, r - 3, e), l1_even(E, r - 1, e), l1_even(E, r + 1, e),
-                                             l1_even(E, r + 3, e));
-                const float o0 = l1_even(E, ry.o0 - yo, e);
-                const float o1 = ry.f != F_EQUAL ? l1_even(E, ry.o1 - yo, e) : o0;
-                const float o2 = ry.f >= F_QUAD1 ? l1_even(E, ry.o2 - yo, e) : o0;
-                const float o3 = ry.f == F_CUBIC ? l1_even(E, ry.o3 - yo, e) : o0;
-                return apply_formula<float>(ry.f, o0, o1, o2, o3);
-            };
-            if (g < 8) {
-                const int xa = x0 + 8 * g;
-                const int n = min(4, max(0, (x1 - xa + 1) / 2));
-                if (n == 0) continue;
-                float *slot = &l1_even(E, r, 2 + 4 * g);
-                float4 cur = *reinterpret_cast<const float4 *>(slot);
-                float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
-                if (inner) {
-                    const float4 u0 = *reinterpret_cast<const float4 *>(&l1_even(E, r - 3, 2 + 4 * g));
-                    const float4 u1 = *reinterpret_cast<const float4 *>(&l1_even(E, r - 1, 2 + 4 * g));
-                    const float4 u2 = *reinterpret_cast<const float4 *>(&l1_even(E, r + 1, 2 + 4 * g));
-                    const float4 u3 = *reinterpret_cast<const float4 *>(&l1_even(E, r + 3, 2 + 4 * g));
-                    pred[0] = cubic_pred<float>(u0.x, u1.x, u2.x, u3.x);
-                    pred[1] = cubic_pred<float>(u0.y, u1.y, u2.y, u3.y);
-                    pred[2] = cubic_pred<float>(u0.z, u1.z, u2.z, u3.z);
-                    pred[3] = cubic_pred<float>(u0.w, u1.w, u2.w, u3.w);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 4; k++) pred[k] = pred_at(2 + 4 * g + k);
-                }
-                l1_group<DECOMP>(v, pred, n, pb + (xa >> 1), true, F.y.skip, codes, esc, qp);
-                *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
+            const long long p =
+                (late ? F.late.p_base + (long long)a * F.late.C : F.y.p_base + (ya + ((t - 1) >> 1)) * F.y.C) + (xg >> 1);
+            float *slot = l1_e(E, r, 4 * g);
+            const float4 cur = *reinterpret_cast<const float4 *>(slot);
+            float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
+            if (t >= 3 && t <= ny - 5) {
+                const float4 u0 = *reinterpret_cast<const float4 *>(l1_e(E, r - 3, 4 * g));
+                const float4 u1 = *reinterpret_cast<const float4 *>(l1_e(E, r - 1, 4 * g));
+                const float4 u2 = *reinterpret_cast<const float4 *>(l1_e(E, r + 1, 4 * g));
+                const float4 u3 = *reinterpret_cast<const float4 *>(l1_e(E, r + 3, 4 * g));
+                pred[0] = cubic_pred<float>(u0.x, u1.x, u2.x, u3.x);
+                pred[1] = cubic_pred<float>(u0.y, u1.y, u2.y, u3.y);
+                pred[2] = cubic_pred<float>(u0.z, u1.z, u2.z, u3.z);
+                pred[3] = cubic_pred<float>(u0.w, u1.w, u2.w, u3.w);
             } else {
-                for (int h = 0; h < 4; h++) {
-                    const int e = h < 2 ? h : 32 + h, x = xo + 2 * e;  // columns x0 - 4, x0 - 2, x0 + 64, x0 + 66
-                    if (x < 0 || x >= nx) continue;
-                    l1_one<DECOMP>(l1_even(E, r, e), pred_at(e), pb + (x >> 1), false, F.y.skip, codes, esc, qp);
-                }
+                const Rule ry = row_rule(true, t, ny, F.y.skip);
+                const int r0 = ry.o0 - yo, r1 = (ry.f != F_EQUAL ? ry.o1 : ry.o0) - yo;
+                const int r2 = (ry.f >= F_QUAD1 ? ry.o2 : ry.o0) - yo, r3 = (ry.f == F_CUBIC ? ry.o3 : ry.o0) - yo;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    pred[k] = apply_formula<float>(ry.f, *l1_e(E, r0, 4 * g + k), *l1_e(E, r1, 4 * g + k),
+                                                   *l1_e(E, r2, 4 * g + k), *l1_e(E, r3, 4 * g + k));
             }
+            l1_quad<DECOMP>(v, pred, codes, esc, p, valid, own, !F.y.skip, qp, etile);
+            *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
         }
     }
     __syncthreads();
-    // ---- x pass: rows [y0, y1) x odd columns of [x0, x1)
+    // ---- x pass: rows [y0, y1) x odd columns of [x0, x1), eight groups of four per row
     {
         const int nrows = y1 - y0;
-        const int odd = nx / 2, thi = 2 * odd - 5;
-        for (int task = tid; task < nrows * 8; task += kL1Threads) {
-            const int yy = task >> 3, j = task & 7;
-            const int r = yy + 4, y = y0 + yy;
-            const int ta = x0 + 1 + 8 * j;  // targets ta, ta + 2, ta + 4, ta + 6
-            const int n = min(4, max(0, (x1 - ta + 1) / 2));
-            if (n == 0) continue;
-            const long long pb = F.x.p_base + ((long long)a * F.x.B + y) * F.x.C + ((ta - 1) >> 1);
-            float *slot = &l1_odd(O, r, 2 + 4 * j);
+        const int thi = 2 * (nx / 2) - 5;  // odd columns up to here take the interior cubic rule
+        const long long xb = F.x.p_base + (long long)a * F.x.B * F.x.C + (x0 >> 1);
+        for (int i = tid; i < nrows * 8; i += kL1Threads) {
+            const int yy = i >> 3, g = i & 7;
+            const int r = yy + 4;
+            const int ta = x0 + 1 + 8 * g;  // targets ta, ta + 2, ta + 4, ta + 6
+            const unsigned valid = l1_mask(ta, 0, x1);
+            if (!valid) continue;
+            float *slot = l1_o(O, r, 4 * g + 2);
             const float4 cur = *reinterpret_cast<const float4 *>(slot);
             float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
-            if (n == 4 && ta >= 3 && ta + 6 <= thi) {
-                const float e1 = l1_even(E, r, 1 + 4 * j);
-                const float4 p = *reinterpret_cast<const float4 *>(&l1_even(E, r, 2 + 4 * j));
-                const float4 q = *reinterpret_cast<const float4 *>(&l1_even(E, r, 6 + 4 * j));
-                pred[0] = cubic_pred<float>(e1, p.x, p.y, p.z);
-                pred[1] = cubic_pred<float>(p.x, p.y, p.z, p.w);
-                pred[2] = cubic_pred<float>(p.y, p.z, p.w, q.x);
-                pred[3] = cubic_pred<float>(p.z, p.w, q.x, q.y);
+            if (ta >= 3 && ta + 6 <= thi) {
+                const float4 A = *reinterpret_cast<const float4 *>(l1_e(E, r, 4 * g));
+                const float4 B = *reinterpret_cast<const float4 *>(l1_e(E, r, 4 * g + 4));
+                pred[0] = cubic_pred<float>(A.y, A.z, A.w, B.x);
+                pred[1] = cubic_pred<float>(A.z, A.w, B.x, B.y);
+                pred[2] = cubic_pred<float>(A.w, B.x, B.y, B.z);
+                pred[3] = cubic_pred<float>(B.x, B.y, B.z, B.w);
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int t = ta + 2 * k;
                     pred[k] = 0.f;
-                    if (k >= n) continue;
+                    if (!((valid >> k) & 1u)) continue;
                     if (t >= 3 && t <= thi) {
                         pred[k] = cubic_pred<float>(l1_at(E, O, r, t - 3 - xo), l1_at(E, O, r, t - 1 - xo),
                                                     l1_at(E, O, r, t + 1 - xo), l1_at(E, O, r, t + 3 - xo));
@@ -1239,7 +1239,7 @@ __global__ void __launch_bounds__(kL1Threads, 5) k_l1_fused(const FusedYX F, flo
                     }
                 }
             }
-            l1_group<DECOMP>(v, pred, n, pb, true, F.x.skip, codes, esc, qp);
+            l1_quad<DECOMP>(v, pred, codes, esc, xb + (long long)(y0 + yy) * F.x.C + 4 * g, valid, valid, !F.x.skip, qp, etile);
             if (DECOMP || !F.x.skip) *reinterpret_cast<float4 *>(slot) = make_float4(v[0], v[1], v[2], v[3]);
         }
     }
@@ -1255,8 +1255,8 @@ __global__ void __launch_bounds__(kL1Threads, 5) k_l1_fused(const FusedYX F, flo
             if (odd_rows && !(y & 1)) continue;
             const int r = yy + 4, x = x0 + 4 * i;
             if (x >= x1) continue;
-            const float2 e = *reinterpret_cast<const float2 *>(&l1_even(E, r, 2 + 2 * i));
-            const float2 o = *reinterpret_cast<const float2 *>(&l1_odd(O, r, 2 + 2 * i));
+            const float2 e = *reinterpret_cast<const float2 *>(l1_e(E, r, 2 + 2 * i));
+            const float2 o = *reinterpret_cast<const float2 *>(l1_o(O, r, 2 + 2 * i));
             float *dst = plane + (long long)y * sy + x;
             if (x + 3 < x1) {
                 *reinterpret_cast<float4 *>(dst) = make_float4(e.x, o.x, e.y, o.y);
@@ -1303,18 +1303,19 @@ bool fusable_yx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, FusedY
 }
 
 template <class T, bool DECOMP>
-void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QParams &qp, cudaStream_t st) {
+void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QParams &qp, unsigned *etile,
+                     cudaStream_t st) {
     dim3 grid((unsigned)((F.x.n + kFuseW - 1) / kFuseW), (unsigned)((F.y.n + kFuseR - 1) / kFuseR), (unsigned)F.y.A);
     if constexpr (std::is_same<T, float>::value) {
         // unit grid step with 16-byte aligned rows and planes: the split-column kernel
         const bool rows16 = F.x.sb % 4 == 0 && (F.y.A == 1 || F.x.sa % 4 == 0);
         if (F.x.step == 1 && rows16 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
-            k_l1_fused<DECOMP><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp);
+            k_l1_fused<DECOMP><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp, etile);
             FB2_CHECK_LAUNCH();
             return;
         }
     }
-    k_yx_fused<T, DECOMP><<<grid, kFuseThreads, 0, st>>>(F, x, codes, esc, qp);
+    k_yx_fused<T, DECOMP><<<grid, kFuseThreads, 0, st>>>(F, x, codes, esc, qp, etile);
     FB2_CHECK_LAUNCH();
 }
 
@@ -1349,18 +1350,36 @@ bool fusable_zyx(const std::vector<PassLaunch> &ps, size_t i, size_t elem, Fused
     return true;
 }
 
+// Whether quantizing a reconstruction again gives it back, for every field value of magnitude up
+// to max_abs at error bound eb.  The fused kernels need this when they compress: a CTA recomputes
+// the targets in its halo from the values it stages, and the CTA owning those targets may already
+// have written their reconstructions back, so the value staged there is the original or the
+// reconstruction r = fl(q 2eb + pred).  Re-quantizing r gives q again when
+// |fl(r - pred) / 2eb - q| < 1/2.  With u the unit roundoff of T (2^-24 float, 2^-53 double),
+// |q| < 2^15 and |pred| <= 7 (max_abs + eb) (the largest weight sum of the interpolation
+// formulas), that error is at most u (2 |q| + |pred| / 2eb) + (double-rounding terms)
+// <= u 2^16 + 3.5 u (max_abs / eb + 1), below 1/4 when eb >= 2^-20 max_abs (float) or
+// 2^-49 max_abs (double).  Below that bound (error bounds near the type's precision) the plan
+// runs its passes one kernel each, which recompute nothing.
+template <class T>
+bool requant_exact(double eb, double max_abs) {
+    const double tol = sizeof(T) == 4 ? 0x1p-20 : 0x1p-49;
+    return max_abs >= 0 && std::isfinite(max_abs) && eb >= tol * max_abs;
+}
+
 // Runs the plan's passes in order, the fusable z + y + x and y + x passes as one kernel.
 template <class T, bool DECOMP>
-void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, cudaStream_t st) {
+void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, unsigned *etile, cudaStream_t st) {
     const std::vector<PassLaunch> &ps = plan.passes;
     for (size_t i = 0; i < ps.size();) {
         FusedYX F{};
         size_t used = 0;
-        if (fusable_zyx(ps, i, sizeof(T), F, used) || fusable_yx(ps, i, sizeof(T), F, used)) {
-            launch_fused_yx<T, DECOMP>(F, x, codes, esc, plan.levels[F.y.level], st);
+        if ((fusable_zyx(ps, i, sizeof(T), F, used) || fusable_yx(ps, i, sizeof(T), F, used)) &&
+            (DECOMP || requant_exact<T>(plan.levels[F.y.level].eb, plan.max_abs))) {
+            launch_fused_yx<T, DECOMP>(F, x, codes, esc, plan.levels[F.y.level], etile, st);
             i += used;
         } else {
-            launch_pass<T, DECOMP>(ps[i], x, codes, esc, plan.levels[ps[i].level], st);
+            launch_pass<T, DECOMP>(ps[i], x, codes, esc, plan.levels[ps[i].level], etile, st);
             i++;
         }
     }
@@ -1419,15 +1438,15 @@ void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, vo
     T *esc = reinterpret_cast<T *>(ws + w.esc_off);
     unsigned *tiles = reinterpret_cast<unsigned *>(ws + w.tiles_off);
     unsigned long long *scan = reinterpret_cast<unsigned long long *>(ws + w.scan_off);
+    // the passes count their escapes per tile of kTile codes as they code them
+    if (w.ntiles > 0) FB2_CUDA(cudaMemsetAsync(tiles, 0, (size_t)w.ntiles * sizeof(unsigned), st));
+    unsigned *etile = w.ntiles > 0 ? tiles : nullptr;
     if (plan.first_point) {
-        k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0]);
+        k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0], etile);
         FB2_CHECK_LAUNCH();
     }
-    run_passes<T, false>(plan, d_x, d_codes, esc, st);
-    const int escc = -plan.levels[0].radius;
+    run_passes<T, false>(plan, d_x, d_codes, esc, etile, st);
     if (w.ntiles > 0) {
-        k_esc_count<<<(unsigned)w.ntiles, kTileThreads, 0, st>>>(d_codes, plan.n_codes, escc, tiles);
-        FB2_CHECK_LAUNCH();
         k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, d_n_esc);
         FB2_CHECK_LAUNCH();
     } else if (d_n_esc) {
@@ -1493,10 +1512,10 @@ void interp_decompress(const InterpPlan &plan, const int16_t *d_codes, const T *
         FB2_CHECK_LAUNCH();
     }
     if (plan.first_point) {
-        k_first_point<T, true><<<1, 1, 0, st>>>(d_x, codes, esc, plan.levels[0]);
+        k_first_point<T, true><<<1, 1, 0, st>>>(d_x, codes, esc, plan.levels[0], nullptr);
         FB2_CHECK_LAUNCH();
     }
-    run_passes<T, true>(plan, d_x, codes, esc, st);
+    run_passes<T, true>(plan, d_x, codes, esc, nullptr, st);
 }
 
 // ------------------------------------------------------------------------------------------ range

@@ -44,6 +44,7 @@ struct InterpParams {
     double alpha, beta;    // interpAlpha / interpBeta
     int radius;            // quantbinCnt / 2
     int tuning;            // 1: the auto-tuner's trial path (TUNING::ENABLED)
+    double max_abs = -1;   // largest |value| of the field (compress); negative: not known
 };
 
 struct InterpPlan {
@@ -58,6 +59,7 @@ struct InterpPlan {
     std::vector<QParams> levels;      // index 0: first point (constructor reciprocal), then one per level
     std::vector<PassLaunch> passes;   // in stream order
     std::vector<long long> level_starts;  // first code position of every level (statistics change there)
+    double max_abs = -1;    // InterpParams::max_abs
 };
 
 // Builds the pass plan; throws std::invalid_argument for unsupported parameters.

@@ -41,21 +41,32 @@ double psnr_to_abs(double psnr, double threshold, double range) {
     return range * v3;
 }
 
+// max - min and the largest |value| of a device field (one read of the field, one small D2H).
+struct FieldStats {
+    double range, max_abs;
+};
 template <class T>
-double field_range(Context &ctx, const T *d_x, long long n, cudaStream_t st) {
+FieldStats field_stats(Context &ctx, const T *d_x, long long n, cudaStream_t st) {
+    (void)ctx;
     Pool pool(st);
     void *ws = pool.get<uint8_t>(range_workspace_bytes());
     T *res = pool.get<T>(4);
     device_range<T>(d_x, n, res, ws, st);
     std::vector<T> h = d2h(res, 3, st);
-    return (double)h[0];
+    return {(double)h[0], std::max(std::fabs((double)h[1]), std::fabs((double)h[2]))};
 }
 
-// calAbsErrorBound (utils/Statistic.hpp:216-240)
+// calAbsErrorBound (utils/Statistic.hpp:216-240).  *max_abs receives the field's largest
+// |value| when the range had to be measured (negative otherwise).
 template <class T>
-void resolve_error_bound(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st) {
+void resolve_error_bound(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st, double *max_abs) {
+    *max_abs = -1;
     if (c.errorBoundMode == EB_ABS) return;
-    auto range = [&]() { return field_range<T>(ctx, d_x, (long long)c.num, st); };
+    auto range = [&]() {
+        const FieldStats fs = field_stats<T>(ctx, d_x, (long long)c.num, st);
+        *max_abs = fs.max_abs;
+        return fs.range;
+    };
     switch (c.errorBoundMode) {
         case EB_REL: c.absErrorBound = c.relErrorBound * range(); break;
         case EB_PSNR: c.absErrorBound = psnr_to_abs(c.psnrErrorBound, 0.99, range()); break;
@@ -104,8 +115,15 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     normalize_dims(c);
     c.openmp = 0;  // serial stream format
     if (c.quantbinCnt <= 0 || c.quantbinCnt > 65536) throw std::invalid_argument("QuantizationBinTotal must be in [2, 65536]");
-    resolve_error_bound<T>(ctx, c, d_x, st);
+    double max_abs = -1;
+    resolve_error_bound<T>(ctx, c, d_x, st, &max_abs);
     tr.mark("error bound resolved");
+    // the interpolation kernels' choice of fused passes depends on the field's largest |value|
+    // (requant_exact in interp.cu); measured here when the error bound did not need the range
+    auto need_max_abs = [&]() {
+        if (max_abs < 0) max_abs = field_stats<T>(ctx, d_x, (long long)c.num, st).max_abs;
+        return max_abs;
+    };
     if (c.absErrorBound == 0) c.cmprAlgo = ALGO_LOSSLESS;
     if (c.cmprAlgo == ALGO_NOPRED) throw std::invalid_argument("unsupported on GPU build: ALGO_NOPRED is not implemented");
     if (c.cmprAlgo == ALGO_LORENZO_REG && !lorenzo_stream_supported(c))
@@ -124,7 +142,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
         if (c.interpAnchorStride < 0) c.interpAnchorStride = (int)default_anchor(c.N);
         // sets interpAlgo/direction/alpha/beta and cmprAlgo = ALGO_INTERP, or (1-D fields) the
         // Lorenzo path's Config with cmprAlgo = ALGO_LORENZO_REG
-        tune_interp<T>(ctx, c, d_x, st);
+        tune_interp<T>(ctx, c, d_x, st, need_max_abs());
     }
     if (c.cmprAlgo == ALGO_LORENZO_REG) {
         try {
@@ -141,7 +159,8 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
                 throw std::invalid_argument("unsupported on GPU build: the tuner chose a non-interpolation algorithm");
             long long dims[4];
             for (int i = 0; i < c.N; i++) dims[i] = (long long)c.dims[i];
-            const InterpParams prm = interp_params_of(c);
+            InterpParams prm = interp_params_of(c);
+            prm.max_abs = need_max_abs();
             const InterpPlan plan = make_plan(dims, c.N, prm);
             Pool pool(st);
             int16_t *codes = pool.get<int16_t>((size_t)plan.n_codes + 16);
@@ -208,36 +227,43 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
         // (the raw blocks' bytes), so that a payload of raw unpredictable values, which zstd
         // shrinks, counts at the size the reference would give it.  The two choose differently
         // only when zstd of the field falls between the two compressed payload sizes.
-        std::vector<uint8_t> host(raw_bytes);
-        FB2_CUDA(cudaMemcpyAsync(host.data(), d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
-        std::vector<uint8_t> framed(core);
-        FB2_CUDA(cudaMemcpyAsync(framed.data(), d_pay, core, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaStreamSynchronize(st));
+        // The ratio test itself is taken on that size too, so a payload whose raw blocks put it
+        // under 3 while the reference's compressed one is above takes no check, as there.  The
+        // payload and the field come back in one pinned buffer, the field's copy running while
+        // the payload is compressed; the field's zstd stops early once it is clearly larger.
+        uint8_t *hb = static_cast<uint8_t *>(ctx.host_big.get(core + raw_bytes));
+        FB2_CUDA(cudaMemcpyAsync(hb, d_pay, core, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaEventRecord(ctx.ev[7], st));  // every context creates its events
+        FB2_CUDA(cudaMemcpyAsync(hb + core, d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaEventSynchronize(ctx.ev[7]));
         size_t lossy = core;
         size_t fb = 0, content = 0;
-        if (core > 8 && parse_raw_frame(framed.data() + 8, core - 8, fb, content)) {
+        if (core > 8 && parse_raw_frame(hb + 8, core - 8, fb, content)) {
             std::vector<uint8_t> body;
             body.reserve(content);
             size_t p = 8 + fb;
             while (body.size() < content && p + 3 <= core) {
-                const uint32_t bh = (uint32_t)framed[p] | ((uint32_t)framed[p + 1] << 8) | ((uint32_t)framed[p + 2] << 16);
+                const uint32_t bh = (uint32_t)hb[p] | ((uint32_t)hb[p + 1] << 8) | ((uint32_t)hb[p + 2] << 16);
                 const size_t bs = bh >> 3;
                 p += 3;
-                body.insert(body.end(), framed.begin() + p, framed.begin() + std::min(core, p + bs));
+                body.insert(body.end(), hb + p, hb + std::min(core, p + bs));
                 p += bs;
             }
             std::vector<uint8_t> zb(zstd_compress_bound(body.size()) + 16);
             lossy = 8 + zstd_compress(body.data(), body.size(), zb.data(), zb.size(), 3);
         }
-        std::vector<uint8_t> z(8 + zstd_compress_bound(raw_bytes));
-        const uint64_t L = raw_bytes;
-        memcpy(z.data(), &L, 8);
-        const size_t zs = 8 + zstd_compress(host.data(), raw_bytes, z.data() + 8, z.size() - 8, 3);
-        if (zs < lossy && zs <= pcap) {
+        FB2_CUDA(cudaStreamSynchronize(st));  // the field is on the host
+        std::vector<uint8_t> z;
+        if ((double)raw_bytes / (double)lossy < 3 && zstd_compress_if_below(hb + core, raw_bytes, 3, lossy - 8, z) &&
+            8 + z.size() <= pcap) {
             c.cmprAlgo = ALGO_LOSSLESS;
-            FB2_CUDA(cudaMemcpyAsync(d_pay, z.data(), zs, cudaMemcpyHostToDevice, st));
+            const uint64_t L = raw_bytes;
+            uint8_t *out = hb;  // reuse the pinned buffer: [u64 L][frame]
+            memcpy(out, &L, 8);
+            memcpy(out + 8, z.data(), z.size());
+            FB2_CUDA(cudaMemcpyAsync(d_pay, out, 8 + z.size(), cudaMemcpyHostToDevice, st));
             FB2_CUDA(cudaStreamSynchronize(st));
-            payload = zs;
+            payload = 8 + z.size();
         }
     }
     std::vector<uint8_t> h(512);

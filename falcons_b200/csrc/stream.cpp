@@ -196,6 +196,16 @@ void decomp_header_write(const DecompHeader &h, std::vector<uint8_t> &out) {
 
 // ------------------------------------------------------------------ libzstd (runtime-loaded)
 namespace {
+// The streaming entry points of the stable zstd API (zstd.h, 1.4.0 on): ZSTD_inBuffer /
+// ZSTD_outBuffer, ZSTD_c_compressionLevel = 100, ZSTD_e_continue = 0, ZSTD_e_end = 2.
+struct ZInBuf {
+    const void *src;
+    size_t size, pos;
+};
+struct ZOutBuf {
+    void *dst;
+    size_t size, pos;
+};
 struct Zstd {
     void *h = nullptr;
     size_t (*compress)(void *, size_t, const void *, size_t, int) = nullptr;
@@ -203,6 +213,12 @@ struct Zstd {
     size_t (*bound)(size_t) = nullptr;
     unsigned (*is_error)(size_t) = nullptr;
     unsigned long long (*fcs)(const void *, size_t) = nullptr;
+    // optional (streaming)
+    void *(*create_cctx)() = nullptr;
+    size_t (*free_cctx)(void *) = nullptr;
+    size_t (*set_param)(void *, int, int) = nullptr;
+    size_t (*set_pledged)(void *, unsigned long long) = nullptr;
+    size_t (*stream2)(void *, ZOutBuf *, ZInBuf *, int) = nullptr;
     Zstd() {
         const char *names[] = {"libzstd.so.1", "libzstd.so"};
         for (const char *n : names) {
@@ -216,7 +232,14 @@ struct Zstd {
         is_error = (decltype(is_error))dlsym(h, "ZSTD_isError");
         fcs = (decltype(fcs))dlsym(h, "ZSTD_getFrameContentSize");
         if (!compress || !decompress || !bound || !is_error || !fcs) h = nullptr;
+        if (!h) return;
+        create_cctx = (decltype(create_cctx))dlsym(h, "ZSTD_createCCtx");
+        free_cctx = (decltype(free_cctx))dlsym(h, "ZSTD_freeCCtx");
+        set_param = (decltype(set_param))dlsym(h, "ZSTD_CCtx_setParameter");
+        set_pledged = (decltype(set_pledged))dlsym(h, "ZSTD_CCtx_setPledgedSrcSize");
+        stream2 = (decltype(stream2))dlsym(h, "ZSTD_compressStream2");
     }
+    bool streaming() const { return create_cctx && free_cctx && set_param && set_pledged && stream2; }
 };
 Zstd &zs() {
     static Zstd z;
@@ -236,6 +259,43 @@ size_t zstd_compress(const void *src, size_t n, void *dst, size_t cap, int level
     const size_t r = zs().compress(dst, cap, src, n, level);
     if (zs().is_error(r)) throw std::runtime_error("Zstd compression failed");
     return r;
+}
+
+bool zstd_compress_if_below(const void *src, size_t n, int level, size_t limit, std::vector<uint8_t> &out) {
+    if (!zstd_available()) throw std::runtime_error("libzstd is not available");
+    Zstd &z = zs();
+    const size_t stop = limit + limit / 50 + 4096;
+    if (z.streaming()) {
+        void *cc = z.create_cctx();
+        if (!cc) throw std::bad_alloc();
+        bool past = false;
+        try {
+            if (z.is_error(z.set_param(cc, 100 /* ZSTD_c_compressionLevel */, level)) ||
+                z.is_error(z.set_pledged(cc, (unsigned long long)n)))
+                throw std::runtime_error("Zstd compression failed");
+            std::vector<uint8_t> buf(1 << 18);
+            size_t produced = 0;
+            constexpr size_t kChunk = 1 << 20;
+            for (size_t at = 0; at < n && !past; at += kChunk) {
+                ZInBuf in{static_cast<const uint8_t *>(src) + at, std::min(kChunk, n - at), 0};
+                while (in.pos < in.size) {
+                    ZOutBuf o{buf.data(), buf.size(), 0};
+                    const size_t r = z.stream2(cc, &o, &in, 0 /* ZSTD_e_continue */);
+                    if (z.is_error(r)) throw std::runtime_error("Zstd compression failed");
+                    produced += o.pos;
+                }
+                past = produced >= stop;
+            }
+        } catch (...) {
+            z.free_cctx(cc);
+            throw;
+        }
+        z.free_cctx(cc);
+        if (past) return false;
+    }
+    out.resize(zstd_compress_bound(n) + 16);
+    out.resize(zstd_compress(src, n, out.data(), out.size(), level));
+    return out.size() < limit;
 }
 
 size_t zstd_decompress(const void *src, size_t n, void *dst, size_t cap) {

@@ -50,6 +50,12 @@ void decomp_header_write(const DecompHeader &h, std::vector<uint8_t> &out);
 bool zstd_available();
 size_t zstd_compress_bound(size_t n);
 size_t zstd_compress(const void *src, size_t n, void *dst, size_t cap, int level);
+// ZSTD_compress of src[0, n) at `level` into `out` when its size is below `limit` (returns true);
+// false when it is not.  Fields whose frame is far larger than `limit` stop early: the streaming
+// API codes the input a chunk at a time and the call gives up once its frame so far exceeds
+// limit by 2 % + 4 KiB (the streaming frame's size can differ from ZSTD_compress's by a few bytes,
+// never by that much); otherwise the answer is ZSTD_compress's own frame.
+bool zstd_compress_if_below(const void *src, size_t n, int level, size_t limit, std::vector<uint8_t> &out);
 size_t zstd_decompress(const void *src, size_t n, void *dst, size_t cap);
 unsigned long long zstd_frame_content_size(const void *src, size_t n);
 

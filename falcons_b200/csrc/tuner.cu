@@ -109,7 +109,7 @@ double trial_ratio(Pool &pool, const T *d_blocks, long long B, long long side, i
 }  // namespace
 
 template <class T>
-void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st) {
+void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st, double max_abs) {
     (void)ctx;
     const int N = c.N;
     const double num = (double)c.num;
@@ -233,6 +233,7 @@ void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st)
     base.anchor = c.interpAnchorStride;
     base.radius = c.quantbinCnt / 2;
     base.tuning = 1;
+    base.max_abs = max_abs;  // the blocks' values are the field's
     int fact = 1;
     for (int i = 2; i <= N; i++) fact *= i;
     const int reverse = fact - 1;
@@ -315,7 +316,7 @@ void tune_interp(Context &ctx, falcons_config &c, const T *d_x, cudaStream_t st)
     c.cmprAlgo = ALGO_INTERP;
 }
 
-template void tune_interp<float>(Context &, falcons_config &, const float *, cudaStream_t);
-template void tune_interp<double>(Context &, falcons_config &, const double *, cudaStream_t);
+template void tune_interp<float>(Context &, falcons_config &, const float *, cudaStream_t, double);
+template void tune_interp<double>(Context &, falcons_config &, const double *, cudaStream_t, double);
 
 }  // namespace fb2

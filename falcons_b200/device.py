@@ -27,11 +27,13 @@ def _stream_ptr(stream) -> ctypes.c_void_p:
 
 
 def interp_params(eb, interp_algo=1, direction=0, anchor_stride=None, ndim=3, alpha=1.25, beta=2.0,
-                  radius=32768, tuning=False) -> _lib.InterpParams:
+                  radius=32768, tuning=False, max_abs=-1.0) -> _lib.InterpParams:
+    """falcons_interp_params.  max_abs: the field's largest |value| if known (compress measures it
+    otherwise)."""
     if anchor_stride is None or anchor_stride < 0:
         anchor_stride = {1: 4096, 2: 128, 3: 32, 4: 16}[ndim]
     return _lib.InterpParams(float(eb), int(interp_algo), int(direction), int(anchor_stride), float(alpha),
-                             float(beta), int(radius), int(tuning))
+                             float(beta), int(radius), int(tuning), float(max_abs))
 
 
 def value_range(x: torch.Tensor, ctx=None, stream=None) -> float:

@@ -17,8 +17,8 @@ The loop's own work is host-side bookkeeping; every byte of compression runs in 
 kernels of libfalcons_b200.so (there is no CPU path)."""
 from __future__ import annotations
 
+import collections
 import ctypes
-import queue
 import threading
 import time
 from concurrent.futures import Future
@@ -50,22 +50,24 @@ class _Req:
 
 
 class Server:
-    """Continuous-batching request loop: `workers` slots, a device-memory budget, FIFO admission
-    (a request waits while the head of the queue does not fit)."""
+    """Continuous-batching request loop: `workers` slots, each a host thread with its own library
+    context and CUDA stream for the server's lifetime; a free slot takes the head of the FIFO queue
+    as soon as its device-memory estimate fits the budget (a request waits while the head of the
+    queue does not fit)."""
 
     def __init__(self, workers: int = 8, budget_bytes: int = 120 << 30, device: int = 0):
         self.device = device
         self.budget = int(budget_bytes)
         self.in_use = 0
         self._cv = threading.Condition()
-        self._queue: list[_Req] = []
+        self._queue: collections.deque[_Req] = collections.deque()
         self._seq = 0
         self._stop = False
         self._ctxs = [_lib.Context(device) for _ in range(workers)]
-        self._free = list(range(workers))
         self.completed: list[_Req] = []
-        self._sched = threading.Thread(target=self._schedule, daemon=True)
-        self._sched.start()
+        self._threads = [threading.Thread(target=self._worker, args=(w,), daemon=True) for w in range(workers)]
+        for t in self._threads:
+            t.start()
 
     # ---- submission
     def submit_compress(self, x: torch.Tensor, config, arrival: float | None = None) -> Future:
@@ -87,63 +89,59 @@ class Server:
             fut.set_exception(ValueError(f"request needs {need} bytes, more than the {self.budget}-byte budget"))
             return fut
         with self._cv:
+            if self._stop:
+                fut.set_exception(RuntimeError("server closed"))
+                return fut
             self._seq += 1
             r = _Req(time.perf_counter() if arrival is None else arrival, self._seq, kind, nbytes, args, fut)
             self._queue.append(r)
             self._cv.notify_all()
         return fut
 
-    # ---- scheduling: admit the head of the queue when a slot is free and it fits the budget
-    def _schedule(self):
-        while True:
-            with self._cv:
-                while not self._stop and not (self._queue and self._free and
-                                              self.in_use + request_bytes(self._queue[0].kind,
-                                                                          self._queue[0].nbytes) <= self.budget):
-                    self._cv.wait()
-                if self._stop and not self._queue:
-                    return
-                if self._stop and not self._free:
-                    self._cv.wait()
-                    continue
-                r = self._queue.pop(0)
-                w = self._free.pop()
-                self.in_use += request_bytes(r.kind, r.nbytes)
-            threading.Thread(target=self._run, args=(r, w), daemon=True).start()
+    # ---- a worker slot: take the head of the queue when it fits the budget, run it, repeat
+    def _admissible(self) -> bool:
+        return bool(self._queue) and self.in_use + request_bytes(self._queue[0].kind, self._queue[0].nbytes) <= self.budget
 
-    def _run(self, r: _Req, w: int):
+    def _worker(self, w: int):
         ctx = self._ctxs[w]
         torch.cuda.set_device(self.device)
         stream = torch.cuda.Stream(device=self.device)
-        r.start = time.perf_counter()
-        try:
-            with torch.cuda.stream(stream):
-                if r.kind == "compress":
-                    x, config = r.args
-                    s, conf = D.compress(x, config, ctx=ctx, stream=stream)
-                    result = (s, conf)
-                else:
-                    s, dtype, num = r.args
-                    out = torch.empty(num, dtype=dtype, device=s.device)
-                    y, conf = D.decompress(s, dtype, out=out, ctx=ctx, stream=stream)
-                    result = (y, conf)
-            stream.synchronize()
-            r.done = time.perf_counter()
-            r.fut.set_result(result)
-        except Exception as e:  # the request fails alone; the loop goes on
-            r.done = time.perf_counter()
-            r.fut.set_exception(e)
-        with self._cv:
-            self.in_use -= request_bytes(r.kind, r.nbytes)
-            self._free.append(w)
-            self.completed.append(r)
-            self._cv.notify_all()
+        while True:
+            with self._cv:
+                while not self._admissible() and not (self._stop and not self._queue):
+                    self._cv.wait()
+                if not self._queue:
+                    return
+                r = self._queue.popleft()
+                need = request_bytes(r.kind, r.nbytes)
+                self.in_use += need
+            r.start = time.perf_counter()
+            try:
+                with torch.cuda.stream(stream):
+                    if r.kind == "compress":
+                        x, config = r.args
+                        result = D.compress(x, config, ctx=ctx, stream=stream)
+                    else:
+                        s, dtype, num = r.args
+                        out = torch.empty(num, dtype=dtype, device=s.device)
+                        result = D.decompress(s, dtype, out=out, ctx=ctx, stream=stream)
+                stream.synchronize()
+                r.done = time.perf_counter()
+                r.fut.set_result(result)
+            except Exception as e:  # the request fails alone; the loop goes on
+                r.done = time.perf_counter()
+                r.fut.set_exception(e)
+            with self._cv:
+                self.in_use -= need
+                self.completed.append(r)
+                self._cv.notify_all()
 
     def close(self):
         with self._cv:
             self._stop = True
             self._cv.notify_all()
-        self._sched.join(timeout=60)
+        for t in self._threads:
+            t.join(timeout=60)
         for c in self._ctxs:
             c.close()
 

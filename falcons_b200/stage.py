@@ -31,7 +31,7 @@ def main(argv=None):
     shape = (a.size,) * 3
     x0 = synth.spectral_field_torch(shape, seed=1)
     eb = a.rel * float(x0.max() - x0.min())
-    p = D.interp_params(eb, 1, 0, None, 3)
+    p = D.interp_params(eb, 1, 0, None, 3, max_abs=float(x0.abs().max()))
     ctx = _lib.default_context(0)
     x = x0.clone()
     rec = torch.empty_like(x0)

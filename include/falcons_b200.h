@@ -56,6 +56,10 @@ typedef struct {
     double beta;             /* Config::interpBeta */
     int32_t radius;          /* Config::quantbinCnt / 2 */
     int32_t tuning;          /* 1: the auto-tuner's trial sweeps (TUNING::ENABLED), N >= 3 */
+    double max_abs;          /* compress: the field's largest |value| when the caller knows it (>= 0);
+                                negative or NaN: falcons_interp_compress measures it (one read of the
+                                field).  It selects the fused kernels; the output does not depend on it.
+                                Ignored by decompress. */
 } falcons_interp_params;
 
 /* The fields of Falcons::Config (utils/Config.hpp:482-511) that the path reads or writes. */
@@ -149,7 +153,8 @@ typedef struct {
 } falcons_batch_item;
 int falcons_compress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers);
 int falcons_decompress_batch(falcons_ctx *ctx, falcons_batch_item *items, size_t n, int workers);
-/* The worker count the autotuner chose for fields of about field_bytes bytes (0: not tuned yet). */
+/* The worker count the autotuner chose for compressing fields of about field_bytes bytes (0: not
+ * tuned yet).  Compress and decompress are tuned apart. */
 int falcons_batch_workers(falcons_ctx *ctx, size_t field_bytes);
 
 /* ---- allocation-free decompress (no counterpart in the reference) ----

@@ -67,6 +67,44 @@ def test_fused_level_passes(cuda, restatement, shape, dtype):
             _run(cuda, restatement, _field(shape, dtype, 11), algo, direction)
 
 
+@pytest.mark.parametrize("shape", [(9, 100, 132), (10, 130, 68), (6, 67, 72), (7, 129, 260), (4, 64, 4),
+                                   (131, 196), (64, 4), (70, 8)])
+def test_unit_step_level_kernel(cuda, restatement, shape):
+    # the finest level of a float field whose rows are 16-byte aligned runs the split-column
+    # kernel: tiles cut short in x and in y, odd and even plane counts (the last plane's own z
+    # pass), an even row count (the last row's own y pass), rows of 4 and 8 values
+    for x in (_field(shape, np.float32, 13), _field(shape, np.float32, 14) * 1e-3):
+        _run(cuda, restatement, x, 1, 0)
+
+
+def test_fused_kernels_only_where_requantization_is_exact(cuda, restatement):
+    """A float field far from zero (values near 1e4, range about 53) at an error bound of 1e-4 of
+    its range: the bound is below 2^-20 of the largest |value|, where quantizing a reconstruction
+    again may not give it back, so compress runs the level passes one kernel each instead of the
+    fused kernels (which re-quantize the halo targets that a neighbouring tile may already have
+    overwritten).  Codes and reconstruction stay bit-exact, and that compress launches more
+    kernels than the same field near zero."""
+    import torch
+    from falcons_b200 import _lib
+    from falcons_b200 import device as D
+    x = _field((12, 70, 136), np.float32, 3)
+    counts = []
+    for field in (x, (x + np.float32(1e4)).astype(np.float32)):
+        eb = 1e-4 * float(field.max() - field.min())
+        assert (eb < 2.0 ** -20 * float(np.abs(field).max())) == (field is not x)
+        _run(cuda, restatement, field, 1, 0)  # 1e-3 of the range: fused for both fields
+        ref = restatement.compress(field, eb, 1, 0)
+        xd = torch.from_numpy(field.copy()).to(cuda)
+        torch.cuda.synchronize()
+        l0 = _lib.lib().falcons_kernel_launches()
+        codes, unpred = D.interp_compress(xd, D.interp_params(eb, 1, 0, None, 3))
+        counts.append(_lib.lib().falcons_kernel_launches() - l0)
+        np.testing.assert_array_equal(codes.cpu().numpy(), ref.codes)
+        np.testing.assert_array_equal(unpred.cpu().numpy(), ref.unpred)
+        np.testing.assert_array_equal(xd.cpu().numpy(), ref.mutated)
+    assert counts[1] > counts[0]
+
+
 @pytest.mark.parametrize("shape", [(33, 40, 17), (20, 21, 22), (5, 6, 7, 8), (17, 3, 9, 4)])
 def test_generic_and_tuning_sweeps(cuda, restatement, shape):
     for algo in (0, 1):

@@ -106,7 +106,8 @@ def test_rejects_inconsistent_arguments():
     out = torch.empty_like(ref)
     assert _noalloc(shape, codes[:-1], unpred, p, out) == _lib.EINVAL
     assert "code count" in _lib.lib().falcons_last_error().decode()
-    bad = _lib.InterpParams(p.eb, p.interp_algo, p.direction, p.anchor_stride, p.alpha, p.beta, p.radius, p.tuning)
+    bad = _lib.InterpParams(p.eb, p.interp_algo, p.direction, p.anchor_stride, p.alpha, p.beta, p.radius, p.tuning,
+                            p.max_abs)
     dims = (ctypes.c_size_t * 3)(*shape)
     rc = _lib.lib().falcons_interp_decompress_noalloc(7, dims, 3, ctypes.byref(bad), ctypes.c_void_p(codes.data_ptr()),
                                                       ctypes.c_size_t(codes.numel()),
