@@ -140,25 +140,24 @@ void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n
         } else {
             // tune on the batch's own fields, in their given order (a mix of sizes): per candidate
             // count, a slice of w fields that is not timed (the workers' first calls size their
-            // scratch), then a timed slice of 3 w fields
+            // scratch), then a timed slice of 6 w fields
             double best_rate = 0;
             int best_w = 0, measured = 0;
             for (int w : {2, 4, 8, 16}) {
-                const size_t take = std::min(n - pos, (size_t)(4 * w));
-                if (take < (size_t)(4 * w)) break;
+                if (n - pos < (size_t)(7 * w)) break;
                 ensure_workers(bp, w);
                 run_range(bp, compress, items, order, pos, pos + w, w, errs);
                 pos += w;
-                const double s = run_range(bp, compress, items, order, pos, pos + 3 * w, w, errs);
+                const double s = run_range(bp, compress, items, order, pos, pos + 6 * w, w, errs);
                 size_t b = 0;
-                for (size_t k = pos; k < pos + 3 * w; k++) b += bytes[order[k]];
+                for (size_t k = pos; k < pos + 6 * w; k++) b += bytes[order[k]];
                 const double rate = s > 0 ? (double)b / s : 0;
                 if (rate > best_rate) {
                     best_rate = rate;
                     best_w = w;
                 }
                 measured++;
-                pos += 3 * w;
+                pos += 6 * w;
             }
             W = best_w ? best_w : 8;
             if (measured >= 2) bp.best[key] = W;

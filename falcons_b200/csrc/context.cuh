@@ -57,7 +57,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     std::mutex mu;                 // one call at a time per context
     DevBuf field, codes, unpred, work, work2, out, small;
-    PinnedBuf host_small, host_big;
+    PinnedBuf host_small;
     cudaEvent_t ev[8] = {};
     // a second stream for work that overlaps the calling stream, with its fork/join events
     // (created on first use by side_stream())
@@ -72,7 +72,6 @@ struct Context {
         out.release();
         small.release();
         host_small.release();
-        host_big.release();
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         for (auto &e : side_ev)

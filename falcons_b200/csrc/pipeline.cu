@@ -229,13 +229,12 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
         // only when zstd of the field falls between the two compressed payload sizes.
         // The ratio test itself is taken on that size too, so a payload whose raw blocks put it
         // under 3 while the reference's compressed one is above takes no check, as there.  The
-        // payload and the field come back in one pinned buffer, the field's copy running while
-        // the payload is compressed; the field's zstd stops early once it is clearly larger.
-        uint8_t *hb = static_cast<uint8_t *>(ctx.host_big.get(core + raw_bytes));
-        FB2_CUDA(cudaMemcpyAsync(hb, d_pay, core, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaEventRecord(ctx.ev[7], st));  // every context creates its events
-        FB2_CUDA(cudaMemcpyAsync(hb + core, d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaEventSynchronize(ctx.ev[7]));
+        // field's zstd stops early once it is clearly larger.  (Pageable host copies: growing a
+        // pinned buffer would synchronize the whole device, stalling concurrent calls.)
+        std::vector<uint8_t> hpay(core);
+        FB2_CUDA(cudaMemcpyAsync(hpay.data(), d_pay, core, cudaMemcpyDeviceToHost, st));
+        FB2_CUDA(cudaStreamSynchronize(st));
+        const uint8_t *hb = hpay.data();
         size_t lossy = core;
         size_t fb = 0, content = 0;
         if (core > 8 && parse_raw_frame(hb + 8, core - 8, fb, content)) {
@@ -252,18 +251,19 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             std::vector<uint8_t> zb(zstd_compress_bound(body.size()) + 16);
             lossy = 8 + zstd_compress(body.data(), body.size(), zb.data(), zb.size(), 3);
         }
-        FB2_CUDA(cudaStreamSynchronize(st));  // the field is on the host
         std::vector<uint8_t> z;
-        if ((double)raw_bytes / (double)lossy < 3 && zstd_compress_if_below(hb + core, raw_bytes, 3, lossy - 8, z) &&
-            8 + z.size() <= pcap) {
-            c.cmprAlgo = ALGO_LOSSLESS;
-            const uint64_t L = raw_bytes;
-            uint8_t *out = hb;  // reuse the pinned buffer: [u64 L][frame]
-            memcpy(out, &L, 8);
-            memcpy(out + 8, z.data(), z.size());
-            FB2_CUDA(cudaMemcpyAsync(d_pay, out, 8 + z.size(), cudaMemcpyHostToDevice, st));
+        if ((double)raw_bytes / (double)lossy < 3) {
+            std::vector<uint8_t> field(raw_bytes);
+            FB2_CUDA(cudaMemcpyAsync(field.data(), d_x, raw_bytes, cudaMemcpyDeviceToHost, st));
             FB2_CUDA(cudaStreamSynchronize(st));
-            payload = 8 + z.size();
+            if (zstd_compress_if_below(field.data(), raw_bytes, 3, lossy - 8, z) && 8 + z.size() <= pcap) {
+                c.cmprAlgo = ALGO_LOSSLESS;
+                const uint64_t L = raw_bytes;
+                z.insert(z.begin(), reinterpret_cast<const uint8_t *>(&L), reinterpret_cast<const uint8_t *>(&L) + 8);
+                FB2_CUDA(cudaMemcpyAsync(d_pay, z.data(), z.size(), cudaMemcpyHostToDevice, st));
+                FB2_CUDA(cudaStreamSynchronize(st));
+                payload = z.size();
+            }
         }
     }
     std::vector<uint8_t> h(512);

@@ -45,7 +45,7 @@ def test_batch_matches_single_field_path(cuda):
     import torch
     from falcons_b200 import _lib, api
     from falcons_b200 import device as D
-    fields = _mixed(30, 1, cuda)
+    fields = _mixed(48, 1, cuda)  # enough for the autotuner's first two candidates (7 x 2 + 7 x 4 fields)
     single, mutated = [], []
     for x, rel in fields:
         w = x.clone()
