@@ -42,9 +42,11 @@ def parse():
     ap.add_argument("--rel", type=float, default=1e-4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve"],
+    ap.add_argument("--workload", default="single", choices=["single", "batch", "serve", "lorenzo1d"],
                     help="single: the 512^3 field (the headline line); batch: the mixed-size batch against "
-                         "one call per field; serve: the open-loop serving sweep")
+                         "one call per field; serve: the open-loop serving sweep; lorenzo1d: a long 1-D "
+                         "field through the blockwise Lorenzo path (its sequential quantization on record)")
+    ap.add_argument("--points", type=int, default=64 << 20, help="lorenzo1d: points of the 1-D field")
     ap.add_argument("--fields", type=int, default=2000, help="batch: number of fields")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests per rate")
     ap.add_argument("--rates", default="200,1000,5000", help="serve: arrival rates per second")
@@ -339,8 +341,54 @@ def run_serve_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def run_lorenzo1d_workload(args):
+    """A long 1-D float32 field (the spectral generator, --points points, EB_REL --rel) compressed
+    and decompressed on the device with ALGO_LORENZO_REG (1-D blockwise Lorenzo, order 1, Huffman),
+    and with ALGO_INTERP_LORENZO (the tuner's choice between interpolation and Lorenzo).  The
+    Lorenzo quantization is one sequential chain (every prediction reads the reconstruction before
+    it), so this line puts its cost on record; wall time per call, field and stream in HBM."""
+    import torch
+    from falcons_b200 import api, synth
+    from falcons_b200 import device as D
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    x = synth.spectral_field_torch((args.points,), seed=11, device=dev)
+    nbytes = x.numel() * x.element_size()
+    out = {}
+    for name, algo in (("lorenzo_reg", api.falconsAlgorithm.LORENZO_REG),
+                       ("interp_lorenzo", api.falconsAlgorithm.INTERP_LORENZO)):
+        c = api.falconsConfig(args.points)
+        c.cmprAlgo = algo
+        c.errorBoundMode = api.falconsErrorBoundMode.REL
+        c.relErrorBound = args.rel
+        c.conf.lorenzo, c.conf.lorenzo2, c.conf.regression, c.conf.regression2 = 1, 0, 0, 0
+        w = x.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s, conf = D.compress(w, c)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        y, _ = D.decompress(s, torch.float32)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        eb = args.rel * float(x.max() - x.min())
+        err = float((y.double() - x.double()).abs().max())
+        out[name] = {"stored_algo": api.falconsAlgorithm(int(conf.cmprAlgo)).name, "compress_s": round(t1 - t0, 3),
+                     "decompress_s": round(t2 - t1, 3), "compress_GBps": round(nbytes / (t1 - t0) / 1e9, 3),
+                     "decompress_GBps": round(nbytes / (t2 - t1) / 1e9, 3), "ratio": round(nbytes / s.numel(), 3),
+                     "max_error_over_bound": round(err / eb, 6)}
+    line = {"metric": "1-D blockwise Lorenzo path: compress / decompress wall time on the device", "value":
+            out["lorenzo_reg"]["compress_s"] + out["lorenzo_reg"]["decompress_s"], "unit": "s", "n_gpus": 1,
+            "higher_is_better": False, "dtype": "f32", "data": "synthetic (seeded spectral 1-D field, on the device)",
+            "config": {"workload": f"1-D float32 field of {args.points} points, EB_REL {args.rel}", **out}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "lorenzo1d" and args.impl != "reference":
+        run_lorenzo1d_workload(args)
+        return
     if args.workload == "batch" and args.impl != "reference":
         run_batch_workload(args)
         return
