@@ -976,10 +976,11 @@ __global__ void __launch_bounds__(kFuseThreads, sizeof(T) == 4 ? 8 : 6) k_yx_fus
     }
 }
 
-// The level whose grid step is one element (the finest level, 7/8 of the codes) of a float field
-// whose rows are 16-byte aligned: the passes, tiles and code positions of k_yx_fused, with the
-// tile's even and odd columns kept apart in shared memory so that a thread takes four consecutive
-// targets of a row at a time (16-byte shared-memory loads and stores, one 8-byte code store):
+// The levels whose grid step is one element (the finest level, 7/8 of the codes) or two (the next,
+// 7/64) of a float field whose rows are 16-byte aligned: the passes, tiles and code positions of
+// k_yx_fused, with the tile's even and odd grid columns kept apart in shared memory so that a
+// thread takes four consecutive targets of a row at a time (16-byte shared-memory loads and
+// stores, one 8-byte code store).  Grid coordinates below; a grid column is STEP elements:
 //   tile column c <-> x = x0 - 4 + c; row r <-> y = y0 - 4 + r (72 x 72: 64 + a halo of 4)
 //   E[r * 40 + e]      even column c = 2e        (e in [0, 36))
 //   O[r * 40 + m + 2]  odd column c = 2m + 1     (own odd columns: m in [2, 34))
@@ -1058,7 +1059,7 @@ __device__ __forceinline__ unsigned l1_mask(int a, int lo, int hi) {
     return m;
 }
 
-template <bool DECOMP>
+template <bool DECOMP, int STEP>
 __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, float *__restrict__ xf,
                                                             int16_t *__restrict__ codes, float *__restrict__ esc,
                                                             const QParams qp, unsigned *__restrict__ etile) {
@@ -1072,26 +1073,31 @@ __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, flo
     const long long sy = F.x.sb, sz = F.x.sa;
     float *plane = xf + (long long)a * sz;
     const int tid = threadIdx.x;
-    // ---- stage rows [yo, yo + 72) x columns [xo, xo + 72), 16 bytes at a time
-    constexpr int NV = kL1Rows * 18;  // 16-byte groups
-    constexpr int ITER = 3;           // loads in flight per thread before their stores
+    // ---- stage rows [yo, yo + 72) x grid columns [xo, xo + 72), 16 bytes at a time: four grid
+    // columns per vector at a grid step of one element, two (at element offsets 0 and 2) at two
+    constexpr int VPR = 72 / (4 / STEP);  // vectors per row
+    constexpr int NV = kL1Rows * VPR;
+    constexpr int ITER = 3;               // loads in flight per thread before their stores
     for (int base = 0; base < NV; base += ITER * kL1Threads) {
         float4 v[ITER];
 #pragma unroll
         for (int k = 0; k < ITER; k++) {
             const int idx = base + tid + k * kL1Threads;
-            const int r = idx / 18, i = idx - r * 18;
-            const int y = yo + r, x = xo + 4 * i;
+            const int r = idx / VPR, i = idx - r * VPR;
+            const int y = yo + r, x = xo + (4 / STEP) * i;  // the vector's first grid column
             v[k] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (idx < NV && y >= 0 && y < ny) {
-                const float *src = plane + (long long)y * sy + x;
-                if (x >= 0 && x + 3 < nx) {
+                const float *src = plane + (long long)y * sy + (long long)x * STEP;
+                if (STEP == 1 ? (x >= 0 && x + 3 < nx) : (x >= 0 && x + 2 < nx)) {
                     v[k] = __ldg(reinterpret_cast<const float4 *>(src));
-                } else {
+                } else if (STEP == 1) {
                     if (x >= 0 && x < nx) v[k].x = src[0];
                     if (x + 1 >= 0 && x + 1 < nx) v[k].y = src[1];
                     if (x + 2 >= 0 && x + 2 < nx) v[k].z = src[2];
                     if (x + 3 >= 0 && x + 3 < nx) v[k].w = src[3];
+                } else {
+                    if (x >= 0 && x < nx) v[k].x = src[0];
+                    if (x + 1 >= 0 && x + 1 < nx) v[k].z = src[2];
                 }
             }
         }
@@ -1099,9 +1105,14 @@ __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, flo
         for (int k = 0; k < ITER; k++) {
             const int idx = base + tid + k * kL1Threads;
             if (idx >= NV) break;
-            const int r = idx / 18, i = idx - r * 18;
-            *reinterpret_cast<float2 *>(l1_e(E, r, 2 * i)) = make_float2(v[k].x, v[k].z);
-            *reinterpret_cast<float2 *>(l1_o(O, r, 2 * i)) = make_float2(v[k].y, v[k].w);
+            const int r = idx / VPR, i = idx - r * VPR;
+            if (STEP == 1) {
+                *reinterpret_cast<float2 *>(l1_e(E, r, 2 * i)) = make_float2(v[k].x, v[k].z);
+                *reinterpret_cast<float2 *>(l1_o(O, r, 2 * i)) = make_float2(v[k].y, v[k].w);
+            } else {
+                *l1_e(E, r, i) = v[k].x;
+                *l1_o(O, r, i) = v[k].z;
+            }
         }
     }
     __syncthreads();
@@ -1129,18 +1140,23 @@ __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, flo
             float *slot = l1_e(E, r, 4 * g);
             const float4 cur = *reinterpret_cast<const float4 *>(slot);
             float v[4] = {cur.x, cur.y, cur.z, cur.w}, pred[4];
-            const long long off = (long long)y * sy + xg;
+            const long long off = (long long)y * sy + (long long)xg * STEP;
             if (xg >= 0 && xg + 7 < nx) {
                 float o[4][4];
                 const float *qs[4] = {q0, q1, q2, q3};
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    const float4 *src = reinterpret_cast<const float4 *>(qs[j] + off);
-                    const float4 lo = __ldg(src), hi = __ldg(src + 1);
-                    o[j][0] = lo.x;
-                    o[j][1] = lo.z;
-                    o[j][2] = hi.x;
-                    o[j][3] = hi.z;
+                    if (STEP == 1) {
+                        const float4 *src = reinterpret_cast<const float4 *>(qs[j] + off);
+                        const float4 lo = __ldg(src), hi = __ldg(src + 1);
+                        o[j][0] = lo.x;
+                        o[j][1] = lo.z;
+                        o[j][2] = hi.x;
+                        o[j][3] = hi.z;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++) o[j][k] = __ldg(qs[j] + off + 4 * k);
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < 4; k++)
@@ -1151,7 +1167,7 @@ __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, flo
                 for (int k = 0; k < 4; k++) {
                     pred[k] = 0.f;
                     if (!((valid >> k) & 1u)) continue;
-                    const long long ok = off + 2 * k;
+                    const long long ok = off + 2 * k * STEP;
                     pred[k] = apply_formula<float>(rz.f, __ldg(q0 + ok), __ldg(q1 + ok), __ldg(q2 + ok), __ldg(q3 + ok));
                 }
             }
@@ -1257,13 +1273,14 @@ __global__ void __launch_bounds__(kL1Threads, 6) k_l1_fused(const FusedYX F, flo
             if (x >= x1) continue;
             const float2 e = *reinterpret_cast<const float2 *>(l1_e(E, r, 2 + 2 * i));
             const float2 o = *reinterpret_cast<const float2 *>(l1_o(O, r, 2 + 2 * i));
-            float *dst = plane + (long long)y * sy + x;
-            if (x + 3 < x1) {
+            float *dst = plane + (long long)y * sy + (long long)x * STEP;
+            if (STEP == 1 && x + 3 < x1) {
                 *reinterpret_cast<float4 *>(dst) = make_float4(e.x, o.x, e.y, o.y);
-            } else {
+            } else {  // at a step of two the finer level's points lie between: one value at a time
                 dst[0] = e.x;
-                if (x + 1 < x1) dst[1] = o.x;
-                if (x + 2 < x1) dst[2] = e.y;
+                if (x + 1 < x1) dst[STEP] = o.x;
+                if (x + 2 < x1) dst[2 * STEP] = e.y;
+                if (x + 3 < x1) dst[3 * STEP] = o.y;
             }
         }
     }
@@ -1307,10 +1324,12 @@ void launch_fused_yx(const FusedYX &F, T *x, int16_t *codes, T *esc, const QPara
                      cudaStream_t st) {
     dim3 grid((unsigned)((F.x.n + kFuseW - 1) / kFuseW), (unsigned)((F.y.n + kFuseR - 1) / kFuseR), (unsigned)F.y.A);
     if constexpr (std::is_same<T, float>::value) {
-        // unit grid step with 16-byte aligned rows and planes: the split-column kernel
+        // a grid step of one or two elements with 16-byte aligned rows and planes: the
+        // split-column kernel
         const bool rows16 = F.x.sb % 4 == 0 && (F.y.A == 1 || F.x.sa % 4 == 0);
-        if (F.x.step == 1 && rows16 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
-            k_l1_fused<DECOMP><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp, etile);
+        if ((F.x.step == 1 || F.x.step == 2) && rows16 && (reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+            if (F.x.step == 1) k_l1_fused<DECOMP, 1><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp, etile);
+            else k_l1_fused<DECOMP, 2><<<grid, kL1Threads, 0, st>>>(F, x, codes, esc, qp, etile);
             FB2_CHECK_LAUNCH();
             return;
         }
@@ -1599,7 +1618,8 @@ cudaError_t preload_decompress_kernels() {
         reinterpret_cast<const void *>(&k_row_fast<T, true>),
         reinterpret_cast<const void *>(&k_line_smem<T, true>),
         reinterpret_cast<const void *>(&k_yx_fused<T, true>),
-        reinterpret_cast<const void *>(&k_l1_fused<true>),
+        reinterpret_cast<const void *>(&k_l1_fused<true, 1>),
+        reinterpret_cast<const void *>(&k_l1_fused<true, 2>),
     };
     for (const void *f : fns) {
         cudaFuncAttributes a;
