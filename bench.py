@@ -293,27 +293,36 @@ def run_serve_workload(args):
     made = []  # (stream, dtype) of compress results, for the decompress requests
     rows = []
     try:
-        for x, rel in pool[:8]:  # streams for the first decompress requests
-            s, _ = srv.submit_compress(x.clone(), conf(x, rel)).result()
-            made.append((s, x.dtype))
+        # warm-up: every field of the pool compressed and decompressed once through the server (its
+        # workers' scratch and the kernels come up here, not in the first measured requests); the
+        # streams serve the first decompress requests
+        warm = [(srv.submit_compress(x.clone(), conf(x, rel)), x.dtype) for x, rel in pool]
+        for f, dt in warm:
+            made.append((f.result()[0], dt))
+        for f in [srv.submit_decompress(s, dt) for s, dt in made]:
+            f.result()
         for rate in [float(r) for r in args.rates.split(",")]:
             srv.completed.clear()
+            # the requests' inputs are made before the arrivals start (a compress overwrites its
+            # input, so each gets a copy of its field), so that the arrival loop only submits
             reqs, nbytes = [], 0
             for k in range(args.requests):
                 if rng.random() < 0.7:
                     x, rel = pool[int(rng.integers(len(pool)))]
                     nbytes += x.numel() * x.element_size()
 
-                    def mk(t, x=x, rel=rel):
-                        f = srv.submit_compress(x.clone(), conf(x, rel), arrival=t)
-                        f.add_done_callback(lambda ff, dt=x.dtype: made.append((ff.result()[0], dt))
+                    def mk(t, xc=x.clone(), c=conf(x, rel)):
+                        f = srv.submit_compress(xc, c, arrival=t)
+                        f.add_done_callback(lambda ff, dt=xc.dtype: made.append((ff.result()[0], dt))
                                             if not ff.exception() else None)
                         return f
                     reqs.append(mk)
                 else:
                     s, dt = made[int(rng.integers(len(made)))]
-                    nbytes += int(api.read_config(s[:256].cpu().numpy()).num_elements) * (8 if dt == torch.float64 else 4)
-                    reqs.append(lambda t, s=s, dt=dt: srv.submit_decompress(s, dt, arrival=t))
+                    num = int(api.read_config(s[:256].cpu().numpy()).num_elements)
+                    nbytes += num * (8 if dt == torch.float64 else 4)
+                    reqs.append(lambda t, s=s, dt=dt, num=num: srv.submit_decompress(s, dt, arrival=t, num=num))
+            torch.cuda.synchronize()
             futs, wall = serve.open_loop(srv, reqs, rate, seed=int(rate))
             st = serve.latency_stats(srv.completed)
             small = [r for r in srv.completed if r.nbytes <= (16 << 20)]

@@ -45,6 +45,7 @@ class _Req:
     nbytes: int = field(compare=False)
     args: tuple = field(compare=False)
     fut: Future = field(compare=False)
+    ready: object = field(default=None, compare=False)  # CUDA event: the caller's work on the input is done
     start: float = field(default=0.0, compare=False)
     done: float = field(default=0.0, compare=False)
 
@@ -73,14 +74,19 @@ class Server:
     def submit_compress(self, x: torch.Tensor, config, arrival: float | None = None) -> Future:
         return self._submit("compress", x.numel() * x.element_size(), (x, config), arrival)
 
-    def submit_decompress(self, stream: torch.Tensor, dtype, arrival: float | None = None) -> Future:
-        head = stream[:256].cpu().numpy().tobytes()
-        c = _lib.Config()
-        buf = bytearray(head)
-        _lib.check(_lib.lib().falcons_read_config((ctypes.c_char * len(buf)).from_buffer(buf),
-                                                  ctypes.c_size_t(len(buf)), ctypes.byref(c)), "read_config")
-        nbytes = int(c.num) * torch.empty((), dtype=dtype).element_size()
-        return self._submit("decompress", nbytes, (stream, dtype, int(c.num)), arrival)
+    def submit_decompress(self, stream: torch.Tensor, dtype, arrival: float | None = None,
+                          num: int | None = None) -> Future:
+        """`num`: the field's element count when the caller knows it (from the stream's header,
+        `api.read_config`); otherwise it is read here, one small device-to-host copy."""
+        if num is None:
+            head = stream[:256].cpu().numpy().tobytes()
+            c = _lib.Config()
+            buf = bytearray(head)
+            _lib.check(_lib.lib().falcons_read_config((ctypes.c_char * len(buf)).from_buffer(buf),
+                                                      ctypes.c_size_t(len(buf)), ctypes.byref(c)), "read_config")
+            num = int(c.num)
+        nbytes = int(num) * torch.empty((), dtype=dtype).element_size()
+        return self._submit("decompress", nbytes, (stream, dtype, int(num)), arrival)
 
     def _submit(self, kind, nbytes, args, arrival):
         fut = Future()
@@ -88,12 +94,15 @@ class Server:
         if need > self.budget:
             fut.set_exception(ValueError(f"request needs {need} bytes, more than the {self.budget}-byte budget"))
             return fut
+        # the input was written on the caller's stream; the worker's stream waits for it
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(self.device))
         with self._cv:
             if self._stop:
                 fut.set_exception(RuntimeError("server closed"))
                 return fut
             self._seq += 1
-            r = _Req(time.perf_counter() if arrival is None else arrival, self._seq, kind, nbytes, args, fut)
+            r = _Req(time.perf_counter() if arrival is None else arrival, self._seq, kind, nbytes, args, fut, ready)
             self._queue.append(r)
             self._cv.notify_all()
         return fut
@@ -117,6 +126,7 @@ class Server:
                 self.in_use += need
             r.start = time.perf_counter()
             try:
+                stream.wait_event(r.ready)
                 with torch.cuda.stream(stream):
                     if r.kind == "compress":
                         x, config = r.args
