@@ -1147,9 +1147,8 @@ struct SegInfo {
 // the chain encoder.  CTA (g, u) takes the u-th of gridDim.y slices of every chain of segment g
 // (slice edges on multiples of 8 codes) and adds its counts to the segment's totals, which start
 // at zero.  Codes are read 8 at a time as 16-byte vectors when q is 16-byte aligned (the
-// code before a vector comes from the lane below); the lanes of a warp holding the same key at the
-// same place in their vectors count it with one atomic, and the warps spread their atomics over
-// kHistCopies histograms.
+// code before a vector comes from the lane below); runs of equal keys within a vector are counted
+// with one atomic, and the lanes of a warp spread their atomics over kHistCopies histograms.
 constexpr int kHistCopies = 4;
 constexpr size_t kHistSmem = (size_t)kHistCopies * O1_NCTX * O1_NSYM * 4;
 __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__ q, const SegInfo *__restrict__ segs,
@@ -1164,8 +1163,7 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
     if (threadIdx.x < kMaxK) esc[threadIdx.x] = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31u;
-    uint32_t *h = hs + (lane % kHistCopies) * HN;              // the scalar loops: a copy per lane class
-    uint32_t *hw = hs + ((threadIdx.x >> 5) % kHistCopies) * HN;  // the vector loop: a copy per warp class
+    uint32_t *h = hs + (lane % kHistCopies) * HN;
     for (int k = 0; k < sg.K; k++) {
         const long long b = (long long)(sg.lo + (unsigned long long)k * sg.cs);
         const long long e = (long long)(sg.lo + min((unsigned long long)k * sg.cs + sg.cs, sg.n));
@@ -1205,27 +1203,29 @@ __global__ void __launch_bounds__(1024, 2) k_o1_hist(const int16_t *__restrict__
             const bool act = vi < v1;
             const uint4 w = act ? __ldg(q4 + vi) : make_uint4(0, 0, 0, 0);
             const uint32_t below = __shfl_up_sync(0xffffffffu, w.w >> 16, 1);
-            const unsigned amask = __ballot_sync(0xffffffffu, act);
             if (!act) continue;
             int prev = 0;  // the code before this vector (context 0 at the chain's start)
             if (vi * 8 > b) prev = (lane && vi > v0) ? (int)(int16_t)below : (int)q[vi * 8 - 1];
             const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
             uint32_t kk[8];
+            uint32_t rkey = ~0u, rn = 0;
 #pragma unroll
             for (int m = 0; m < 8; m++) {
                 const int code = (int)(int16_t)(ww[m >> 1] >> (16 * (m & 1)));
                 const int sy = o1_sym(code);
-                kk[m] = (uint32_t)(o1_ctx(prev) << 8) | (uint32_t)sy;
+                const uint32_t key = (uint32_t)(o1_ctx(prev) << 8) | (uint32_t)sy;
+                kk[m] = key;
                 ne += sy == O1_NSYM - 1;
+                if (key == rkey) {
+                    rn++;
+                } else {
+                    if (rn) atomicAdd(&h[rkey], rn);
+                    rkey = key;
+                    rn = 1;
+                }
                 prev = code;
             }
-            // the lanes holding the same key at the same place count it with one atomic (the keys
-            // of a smooth field's codes concentrate on a few contexts and symbols)
-#pragma unroll
-            for (int m = 0; m < 8; m++) {
-                const unsigned peers = __match_any_sync(amask, kk[m]);
-                if (lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&hw[kk[m]], (uint32_t)__popc(peers));
-            }
+            atomicAdd(&h[rkey], rn);
             k4[vi] = make_uint4(kk[0] | (kk[1] << 16), kk[2] | (kk[3] << 16), kk[4] | (kk[5] << 16), kk[6] | (kk[7] << 16));
         }
         ne = __reduce_add_sync(0xffffffffu, ne);
