@@ -8,7 +8,7 @@
 
 namespace fb2 {
 
-// Whether a stream's Config selects the Lorenzo path this build decodes: a 1-D field, Lorenzo
+// Whether a stream's Config selects the Lorenzo path decoded here: a 1-D field, Lorenzo
 // order 1 and / or 2 (composed per block when both are on), no regression predictor.
 bool lorenzo_stream_supported(const falcons_config &c);
 

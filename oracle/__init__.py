@@ -1,6 +1,6 @@
 """ORACLE — test infrastructure, never product code.
 
-Python access to the two CPU checkers of the CUDA path:
+Python access to the two CPU restatements the tests compare the CUDA path with:
 
 * ``Restatement`` wraps ``oracle/liboracle.so``, the plain-C restatements of the reference's
   interpolation decomposition (oracle/interp_oracle.c) and of its 1-D blockwise Lorenzo +

@@ -3,7 +3,7 @@
  *
  * A plain-C restatement of the reference's serial interpolation decomposition
  * (prediction + linear quantization) for float and double fields, used only by the
- * tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker
+ * tests, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the reference
  * of the CUDA path.  Nothing in falcons_b200/ links or calls it.
  *
  * What it restates (reference = JLiu-1/Falcons, include/Falcons/...):

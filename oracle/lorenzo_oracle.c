@@ -5,7 +5,7 @@
  * interpolation tuner configures it for 1-D fields (Lorenzo order 1 and order 2 composed per
  * block, block size 5, no regression), up to the payload that the reference hands to its
  * trailing zstd stage, and the matching decoder.  Used only by tests/ and
- * tests/golden/make_golden.py as the checker of that path; nothing in falcons_b200/ links it.
+ * tests/golden/make_golden.py as the reference restatement of that path; nothing in falcons_b200/ links it.
  *
  * What it restates (reference = JLiu-1/Falcons, include/Falcons/...):
  *   - the blockwise decomposition    decomposition/BlockwiseDecomposition.hpp:28-72: blocks of

@@ -3,7 +3,7 @@
 // oracle/Makefile compiles this file against the reference's own include tree and its
 // vendored FSE sources, producing oracle/_ref/libfalcons_ref.so.  Only the tests, the
 // fixture generator under tests/golden/ and bench.py's reference arm load it, and only
-// as a checker or a timed CPU baseline.  Nothing in the product links it.
+// as a reference for the tests or a timed CPU baseline.  Nothing in the product links it.
 //
 // Entry points (all extern "C", plain pointers):
 //   ref_compress_<t>            include/Falcons/api/falcons.hpp:54       (Falcons_compress into a buffer)

@@ -8,7 +8,7 @@ Each case runs both directions through the drop-in API:
   * the quantization codes and the unpredictable list equal the reference's;
   * the compressed size stays within a stated margin of the reference's: 2 %, except where the
     payload is mostly raw unpredictable values, which the reference's trailing zstd level-3
-    stage shrinks and this build's frame of raw zstd blocks stores as they are (the 384^3 float64
+    stage shrinks and the library's frame of raw zstd blocks stores as they are (the 384^3 float64
     case: 85 % of its payload is float64 unpredictable values, which zstd shrinks by about 5 %).
 
 Workloads (seeded synthetic fields with the shapes and value distributions of the reference's

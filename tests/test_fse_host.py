@@ -4,7 +4,7 @@ FSE_decompress (include/Falcons/encoder/zfse).
 
 * Every block written here decodes with the reference's FSE_decompress; every block the reference
   writes decodes here (including its low-probability -1 counts).
-* The normalization is this build's own (nearest shares, then single-cell moves by marginal coded
+* The normalization is the library's own (nearest shares, then single-cell moves by marginal coded
   size), so the bytes differ from FSE_compress's; the total size stays within 0.5 % of it.
 * The NCount header round-trips, and the reader refuses truncated or malformed headers.
 """

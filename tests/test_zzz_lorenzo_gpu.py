@@ -66,7 +66,7 @@ def lorenzo_config(api, n, eb, l1=1, l2=1):
 
 
 def stream_payload(buf):
-    """The payload of one of this build's streams ([Config][u64 L][zstd raw-block frame])."""
+    """The payload of one of the library's streams ([Config][u64 L][zstd raw-block frame])."""
     import pyarrow as pa
     import oracle
     s = buf.tobytes()
@@ -99,7 +99,7 @@ def test_lorenzo_compress_matches_oracle(cuda, restatement, kind, n, dtype, eb, 
 
 @pytest.mark.gpu
 def test_lorenzo_compress_of_golden_inputs(cuda):
-    """The golden inputs compressed here: where this build's stream keeps the Lorenzo path its
+    """The golden inputs compressed here: where the library's stream keeps the Lorenzo path its
     payload is the reference's (golden) one; a stream the dispatcher stores losslessly decodes to
     the input itself."""
     from falcons_b200 import api
