@@ -119,6 +119,27 @@ void Trace::mark(const char *label) {
         std::fprintf(stderr, "[falcons trace] %s %-28s +%8.3f ms  launches %llu\n", what, label, now_ms() - t0,
                      g_launches.load() - l0);
 }
+void Trace::gpu(const char *label, cudaStream_t s) {
+    if (!on) return;
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, s);
+    events.emplace_back(label, e);
+}
+void Trace::gpu_dump() {
+    if (!on || events.empty()) return;
+    for (auto &p : events) cudaEventSynchronize(p.second);
+    for (auto &p : events) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, events.front().second, p.second);
+        std::fprintf(stderr, "[falcons trace] %s device: %-26s +%8.3f ms\n", what, p.first, ms);
+    }
+    for (auto &p : events) cudaEventDestroy(p.second);
+    events.clear();
+}
+Trace::~Trace() {
+    for (auto &p : events) cudaEventDestroy(p.second);
+}
 }  // namespace fb2
 
 extern "C" {

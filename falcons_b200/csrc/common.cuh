@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace fb2 {
 
@@ -36,13 +38,21 @@ unsigned long long count_launch();
 // Host-side phase trace, on when the environment variable FALCONS_TRACE is set: each mark()
 // prints to stderr the host time since the traced call began and the kernel launches so far.
 // A long gap between two marks with few launches is host work the GPU waited for.
+// gpu() records a CUDA event on a stream; gpu_dump() waits for them and prints each one's device
+// time since the first, which shows what ran when across the streams of one call.
 struct Trace {
     const char *what;
     double t0;
     unsigned long long l0;
     bool on;
+    std::vector<std::pair<const char *, cudaEvent_t>> events;
     explicit Trace(const char *w);
+    Trace(const Trace &) = delete;
+    Trace &operator=(const Trace &) = delete;
+    ~Trace();
     void mark(const char *label);
+    void gpu(const char *label, cudaStream_t s);
+    void gpu_dump();
 };
 #define FB2_CHECK_LAUNCH()      \
     do {                        \

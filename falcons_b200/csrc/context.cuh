@@ -62,7 +62,7 @@ struct Context {
     // a second stream for work that overlaps the calling stream, with its fork/join events
     // (created on first use by side_stream())
     cudaStream_t side = nullptr;
-    cudaEvent_t side_ev[2] = {};
+    cudaEvent_t side_ev[3] = {};
     ~Context() {
         field.release();
         codes.release();
@@ -81,9 +81,15 @@ struct Context {
     }
 };
 
-// The context's second stream (non-blocking), created on first use on the current device.
+// The context's second stream (non-blocking), created on first use on the current device, at the
+// device's highest priority: it carries the escape coders, whose CTAs are long sequential chains,
+// and those must take their SMs before the chain encoder's CTAs queued beside them.
 inline cudaStream_t side_stream(Context &ctx) {
-    if (!ctx.side) FB2_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
+    if (!ctx.side) {
+        int least = 0, greatest = 0;
+        FB2_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        FB2_CUDA(cudaStreamCreateWithPriority(&ctx.side, cudaStreamNonBlocking, greatest));
+    }
     for (auto &e : ctx.side_ev)
         if (!e) FB2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return ctx.side;

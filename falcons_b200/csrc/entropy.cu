@@ -88,16 +88,16 @@ __host__ __device__ __forceinline__ uint32_t fse_ckpt_count(uint32_t n, uint32_t
     return n >= 3 ? (n - 3) / part : 0;
 }
 
-// FSE class block encoder (zfse/fse_compress.c FSE_compress), one CTA per 64 Ki-symbol block,
-// the largest blocks first.  The CTA counts the block; thread 0 normalizes and writes the table
-// header; the CTA builds the coding tables in shared memory (the state table with warp match
-// ranks, the symbol transforms per symbol, and, where it fits, the next-state table); two warps
-// then code the two state chains (symbols n-3 .. 0, each coded by the state of its index parity)
-// side by side, recording for every symbol only the state before it (the emitted bits are its low
-// bits, their count follows from the state and the symbol); the CTA then packs in parallel: a
-// block scan of the bit counts gives every symbol its bit position, each thread writes the bits of
-// one run of symbols (words shared with a neighbour merged with atomicOr), and thread 0 appends
-// the two final states and the end mark.  (The
+// FSE class block encoder (zfse/fse_compress.c FSE_compress), one group of 256 threads per 64
+// Ki-symbol block (four groups per CTA, below), the largest blocks first.  The group counts the
+// block; its thread 0 normalizes and writes the table header; the group builds the coding tables
+// in shared memory (the state table with warp match ranks, the symbol transforms per symbol, and,
+// where it fits, the next-state table); two warps then code the two state chains (symbols n-3 .. 0,
+// each coded by the state of its index parity) side by side, recording for every symbol only the
+// state before it (the emitted bits are its low bits, their count follows from the state and the
+// symbol); the group then packs in parallel: a scan of the bit counts gives every symbol its bit
+// position, each thread writes the bits of one run of symbols (words shared with a neighbour
+// merged with atomicOr), and thread 0 appends the two final states and the end mark.  (The
 // chains of these skewed class streams converge too slowly for a speculative split.)  Writes the
 // complete fse_enc record ([1][u32 len][data] | [0][raw] | [2][sym]) to the block's slot; the
 // record flag goes into bits 56-63 of `sizes`.  `recs` is scratch of kFseRecWords words per block
@@ -112,6 +112,14 @@ constexpr size_t kFseNxtBytes = 40 * 1024;
 // chain's lead (the steps that its first 16-byte symbol word holds above the chain's start).
 constexpr unsigned kFseChainRec = FBLK / 2 + 32;
 constexpr unsigned kFseRecWords = kFseChainRec;  // both chains, 2 records per word
+// The packer's chunk of emission positions and its word buffer (the chunk's bits, at most
+// kFseMaxLog per position, plus the partial word in front and one behind), staged with its records,
+// symbols and slice offsets in the next-state table's space.
+constexpr unsigned kPackChunk = 8192;
+constexpr unsigned kPackWords = kPackChunk * kFseMaxLog / 32 + 2;
+static_assert(kPackChunk * 3 + (kPackWords + kPackChunk / 32 + 1) * 4 <= kFseNxtBytes,
+              "the packer's staging fits the next-state table's space");
+static_assert(kPackChunk % 1024 == 0, "one warp scans the chunk's slices, a whole number per lane");
 static_assert(kFseChainRec % 8 == 0, "records of whole symbol words are stored as 16-byte vectors");
 struct FseSmem {
     uint32_t count[256];
@@ -122,21 +130,63 @@ struct FseSmem {
     uint16_t state_table[1 << kFseMaxLog];
     uint8_t sym[1 << kFseMaxLog];
 };
+// A CTA codes kFseGroups blocks side by side, one group of kFseGroupThreads threads each, with
+// its own shared memory and its own named barrier: the CTA fills an SM (registers), so the blocks
+// of one launch sit on a quarter as many SMs as one CTA per block would spread over, and the chain
+// encoder launched beside them keeps the other SMs.
+constexpr unsigned kFseGroups = 4, kFseGroupThreads = 256;
+struct FseGroupSmem {
+    FseSmem w;
+    int mode;
+    unsigned tl, hdr, s0, s1, maxsv, i0, i1, minsv, fast, high;
+    unsigned lead[2];
+    uint32_t sh[32];
+};
 
-__global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__restrict__ cls,
-                                                          const BlockJob *__restrict__ jobs,
-                                                          uint8_t *__restrict__ slots,
-                                                          unsigned long long *__restrict__ sizes,
-                                                          uint8_t *__restrict__ scratch, uint32_t part,
-                                                          FseCkpt *__restrict__ cks, uint32_t *__restrict__ recs,
-                                                          const uint32_t *__restrict__ order) {
-    __shared__ FseSmem w;
-    extern __shared__ uint4 s_nxt4[];  // next-state table (kFseNxtBytes)
-    __shared__ int s_mode;  // 0 raw, 1 RLE, 2 FSE
-    __shared__ unsigned s_tl, s_hdr, s_s0, s_s1, s_maxsv, s_i0, s_i1, s_minsv, s_fast;
-    __shared__ unsigned s_lead[2], s_high;
-    __shared__ uint32_t s_sh[32];
-    const unsigned b = order[blockIdx.x];  // the largest blocks first
+__device__ __forceinline__ void group_sync(unsigned bar) {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(kFseGroupThreads) : "memory");
+}
+
+// Exclusive scan over a group's threads (tid = index in the group), total of the group in `total`.
+__device__ __forceinline__ uint32_t group_excl_scan(uint32_t v, uint32_t *sh, uint32_t &total, unsigned tid,
+                                                    unsigned bar) {
+    constexpr unsigned nw = kFseGroupThreads / 32;
+    const unsigned lane = tid & 31u, wid = tid >> 5;
+    const uint32_t incl = warp_incl_scan(v);
+    if (lane == 31) sh[wid] = incl;
+    group_sync(bar);
+    if (wid == 0) {
+        uint32_t x = lane < nw ? sh[lane] : 0u;
+        x = warp_incl_scan(x);
+        sh[lane] = x;
+    }
+    group_sync(bar);
+    const uint32_t before = wid ? sh[wid - 1] : 0u;
+    total = sh[nw - 1];
+    group_sync(bar);
+    return before + incl - v;
+}
+
+__global__ void __launch_bounds__(kFseGroups * kFseGroupThreads, 4 / kFseGroups)
+    k_fse_encode_blocks(const uint8_t *__restrict__ cls, const BlockJob *__restrict__ jobs, unsigned njobs,
+                        uint8_t *__restrict__ slots, unsigned long long *__restrict__ sizes,
+                        uint8_t *__restrict__ scratch, uint32_t part, FseCkpt *__restrict__ cks,
+                        uint32_t *__restrict__ recs, const uint32_t *__restrict__ order) {
+    __shared__ FseGroupSmem groups[kFseGroups];
+    extern __shared__ uint4 s_nxt_all[];  // the groups' next-state tables (kFseNxtBytes each)
+    const unsigned grp = threadIdx.x / kFseGroupThreads, tid = threadIdx.x % kFseGroupThreads;
+    const unsigned slot = blockIdx.x * kFseGroups + grp;
+    if (slot >= njobs) return;  // the other groups synchronise on barriers of their own
+    const unsigned bar = 1 + grp;  // named barrier of this group (0 is the CTA's)
+    FseGroupSmem &gm = groups[grp];
+    FseSmem &w = gm.w;
+    uint4 *s_nxt4 = s_nxt_all + (size_t)grp * (kFseNxtBytes / 16);
+    int &s_mode = gm.mode;  // 0 raw, 1 RLE, 2 FSE
+    unsigned &s_tl = gm.tl, &s_hdr = gm.hdr, &s_s0 = gm.s0, &s_s1 = gm.s1, &s_maxsv = gm.maxsv, &s_i0 = gm.i0,
+             &s_i1 = gm.i1, &s_minsv = gm.minsv, &s_fast = gm.fast, &s_high = gm.high;
+    unsigned *s_lead = gm.lead;
+    uint32_t *s_sh = gm.sh;
+    const unsigned b = order[slot];  // the largest blocks first
     const BlockJob jb = jobs[b];
     const uint8_t *src = cls + jb.src;
     uint8_t *out = slots + (size_t)b * kBlockSlot;
@@ -144,16 +194,16 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
     uint32_t *rec = recs + (size_t)b * kFseRecWords;
     FseCkpt *ck = cks ? cks + (size_t)b * (FBLK / part) : nullptr;
     const unsigned n = jb.n;
-    for (int s = threadIdx.x; s < 256; s += blockDim.x) w.count[s] = 0;
-    __syncthreads();
+    for (int s = tid; s < 256; s += kFseGroupThreads) w.count[s] = 0;
+    group_sync(bar);
     // Count the symbols: every thread reads a contiguous run of aligned 16-byte words (the pool's
     // allocations are 16-byte aligned with slack behind them) and adds runs of equal symbols with
     // one atomic (the class streams are dominated by a few symbols).
     {
         const unsigned lead = (unsigned)(jb.src & 15u);
         const uint4 *g4 = reinterpret_cast<const uint4 *>(src - lead);
-        const unsigned nw = (lead + n + 15) / 16, per = (nw + blockDim.x - 1) / blockDim.x;
-        const unsigned w0 = min(nw, threadIdx.x * per), cnt = min(nw, w0 + per) - w0;
+        const unsigned nw = (lead + n + 15) / 16, per = (nw + kFseGroupThreads - 1) / kFseGroupThreads;
+        const unsigned w0 = min(nw, tid * per), cnt = min(nw, w0 + per) - w0;
         unsigned cur = 256, run = 0;
         for (unsigned j = 0; j < cnt; j++) {
             const unsigned wi = w0 + j;
@@ -175,8 +225,8 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
         }
         if (run) atomicAdd(&w.count[cur], run);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
+    group_sync(bar);
+    if (tid == 0) {
         int mode = 0;
         unsigned tl = 0, hdr = 0, maxSV = 255;
         {
@@ -213,18 +263,18 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
         s_hdr = hdr;
         s_maxsv = maxSV;
     }
-    __syncthreads();
+    group_sync(bar);
     if (s_mode == 2) {
         const unsigned tl = s_tl, L = 1u << tl, maxSV = s_maxsv;
         {
             // parallel spread: thread t ranks the kept positions of j in [t * per, (t + 1) * per)
             const uint32_t step = fse::table_step(L), mask = L - 1, high = s_high;
-            const unsigned per = (L + blockDim.x - 1) / blockDim.x;
-            const unsigned j0 = min(L, threadIdx.x * per), j1 = min(L, j0 + per);
+            const unsigned per = (L + kFseGroupThreads - 1) / kFseGroupThreads;
+            const unsigned j0 = min(L, tid * per), j1 = min(L, j0 + per);
             uint32_t cnt = 0;
             for (unsigned j = j0; j < j1; j++) cnt += ((j * step) & mask) <= high;
             uint32_t tot;
-            uint32_t kc = block_excl_scan<uint32_t>(cnt, s_sh, tot);
+            uint32_t kc = group_excl_scan(cnt, s_sh, tot, tid, bar);
             unsigned sy = 0;  // the symbol of cell kc: the last one whose first cell is <= kc
             for (unsigned lo = 0, hi = maxSV + 1; hi - lo > 1;) {
                 const unsigned mid = (lo + hi) >> 1;
@@ -239,11 +289,11 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
                 w.sym[pos] = (uint8_t)sy;
                 kc++;
             }
-            __syncthreads();
+            group_sync(bar);
         }
         // state table: the cells of every symbol in increasing order (match ranks within a warp)
-        if (threadIdx.x < 32) {
-            const unsigned lane = threadIdx.x;
+        if (tid < 32) {
+            const unsigned lane = tid;
             for (unsigned u0 = 0; u0 < L; u0 += 32) {
                 const unsigned u = u0 + lane;
                 const unsigned sy = u < L ? w.sym[u] : 256u + lane;
@@ -255,7 +305,7 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
                 __syncwarp();
             }
         }
-        for (unsigned sy = threadIdx.x; sy <= maxSV; sy += blockDim.x) {
+        for (unsigned sy = tid; sy <= maxSV; sy += kFseGroupThreads) {
             const int nn = w.norm[sy];
             uint32_t total = 0;  // cells of the symbols before sy
             for (unsigned s2 = 0; s2 < sy; s2++) total += w.norm[s2] == -1 ? 1u : (uint32_t)max(0, (int)w.norm[s2]);
@@ -272,34 +322,34 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
                 w.sym_tt[sy].deltaFindState = (int32_t)total - nn;
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
+        group_sync(bar);
+        if (tid == 0) {
             unsigned lo = 0;
             while (lo < maxSV && w.count[lo] == 0) lo++;
             s_minsv = lo;
             s_fast = (size_t)(maxSV - lo + 1) * L * 2 <= kFseNxtBytes;
         }
-        __syncthreads();
+        group_sync(bar);
         uint16_t *nxt = reinterpret_cast<uint16_t *>(s_nxt4);
         const unsigned minSV = s_minsv;
         const bool fast = s_fast != 0;
         if (fast) {
-            for (unsigned e = threadIdx.x; e < (maxSV - minSV + 1) * L; e += blockDim.x) {
+            for (unsigned e = tid; e < (maxSV - minSV + 1) * L; e += kFseGroupThreads) {
                 const unsigned sy = minSV + (e >> tl), x = L + (e & (L - 1));
                 if (!w.count[sy]) continue;
                 const fse::SymTT t = w.sym_tt[sy];
                 const uint32_t nb = (x + t.deltaNbBits) >> 16;
                 nxt[e] = (uint16_t)((w.state_table[(int32_t)(x >> nb) + t.deltaFindState] - L) << 1);
             }
-            __syncthreads();
+            group_sync(bar);
         }
-        if ((threadIdx.x & 31u) == 0 && threadIdx.x < 64) {
+        if ((tid & 31u) == 0 && tid < 64) {
             // The two state chains, one per warp: chain k codes the symbols i <= n - 3 of parity k
             // from the top down (step j codes symbol top - 2 j), starting from the state that
             // symbol n-1 or n-2 (of parity k) initialised.  Each step records twice the state
             // before it minus L (16 bits, table log <= 11): its low bits are the emitted ones, and
             // the record of the chain's next step holds the state after it.
-            const unsigned k = threadIdx.x >> 5;
+            const unsigned k = tid >> 5;
             uint32_t v;  // the state minus L
             {
                 const unsigned i0 = ((n - 1) % 2 == k) ? n - 1 : n - 2;
@@ -410,14 +460,12 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
             else s_s1 = v + L;
         }
     }
-    __syncthreads();
+    group_sync(bar);
     int mode = s_mode;
     size_t body = 0;
     if (mode == 2) {
         const unsigned tl = s_tl;
-        // symbols n-3 .. 0 in emission order; thread t owns emission positions [t*per, (t+1)*per)
-        const unsigned ns = n - 2, per = (ns + blockDim.x - 1) / blockDim.x;
-        const unsigned e0 = min(ns, threadIdx.x * per), e1 = min(ns, e0 + per);
+        const unsigned ns = n - 2;  // emission position e codes symbol n - 3 - e
         // the record of emission position e: even positions belong to the chain of n-3's parity
         const unsigned ka = (n - 3) & 1u;
         const unsigned offA = ka * kFseChainRec + s_lead[ka], offB = (ka ^ 1u) * kFseChainRec + s_lead[ka ^ 1u];
@@ -427,95 +475,120 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
         // the number of bits that state v + L emits for symbol sy
         const uint32_t Lb = 1u << tl;
         auto NB = [&](uint32_t v, unsigned sy) -> uint32_t { return (v + Lb + w.sym_tt[sy].deltaNbBits) >> 16; };
-        // records and symbols are read kPackBatch at a time, all loads of a batch before its uses
-        constexpr unsigned kPackBatch = 8;
-        uint32_t cnt = 0;
-        for (unsigned e = e0; e < e1; e += kPackBatch) {
-            uint32_t vv[kPackBatch], sy[kPackBatch];
-#pragma unroll
-            for (unsigned u = 0; u < kPackBatch; u++) {
-                const unsigned ee = min(e + u, e1 - 1);
-                vv[u] = V(ee);
-                sy[u] = src[n - 3 - ee];
-            }
-#pragma unroll
-            for (unsigned u = 0; u < kPackBatch; u++)
-                if (e + u < e1) cnt += NB(vv[u], sy[u]);
+        // The bits leave in chunks of kPackChunk emission positions.  A chunk's records and symbols
+        // are staged in shared memory (the next-state table's space, free once the chains are
+        // done); lane l of a warp takes position 32 s + l of the chunk's slice s; the slices' bit
+        // totals, scanned, and a warp scan within the slice give every position its bit offset; the
+        // bits are merged into a shared word buffer, whose words then leave as whole-word stores
+        // (the chunk's two edge words, shared with the neighbouring chunks, by atomicOr into the
+        // zeroed scratch).  Words past the block's slot are dropped: such a block is stored raw.
+        uint16_t *sv = reinterpret_cast<uint16_t *>(s_nxt4);
+        uint8_t *ss = reinterpret_cast<uint8_t *>(sv + kPackChunk);
+        uint32_t *sw = reinterpret_cast<uint32_t *>(ss + kPackChunk);
+        uint32_t *slice = sw + kPackWords;  // kPackChunk / 32 slice offsets, then the chunk's total
+        const unsigned lane = tid & 31u, wid = tid >> 5;
+        constexpr unsigned kCap = (unsigned)(kBlockSlot / 4);
+        {
+            const unsigned long long most = (unsigned long long)ns * tl + 2 * tl + 1;
+            const unsigned zw = (unsigned)((most + 31) / 32 + 1 < kCap ? (most + 31) / 32 + 1 : kCap);
+            for (unsigned z = tid; z < zw; z += kFseGroupThreads) bw[z] = 0u;
         }
-        uint32_t sym_bits;  // bits of all symbols
-        const uint32_t off = block_excl_scan<uint32_t>(cnt, s_sh, sym_bits);
+        uint32_t base = 0;  // bits of the chunks before
+        for (unsigned c0 = 0; c0 < ns; c0 += kPackChunk) {
+            const unsigned cn = min(kPackChunk, ns - c0), nsl = (cn + 31) / 32;
+            group_sync(bar);  // the previous chunk's words are out (the first time: the scratch is zero)
+            for (unsigned j = tid; j < cn; j += kFseGroupThreads) {
+                const unsigned e = c0 + j;
+                sv[j] = rec16[((e & 1u) ? offB : offA) + (e >> 1)];
+                ss[j] = src[n - 3 - e];
+            }
+            for (unsigned z = tid; z < kPackWords; z += kFseGroupThreads) sw[z] = 0u;
+            group_sync(bar);
+            for (unsigned sl = wid; sl < nsl; sl += kFseGroupThreads / 32) {
+                const unsigned j = sl * 32 + lane;
+                const uint32_t nb = j < cn ? NB(sv[j] >> 1, ss[j]) : 0u;
+                const uint32_t t = __reduce_add_sync(0xffffffffu, nb);
+                if (lane == 0) slice[sl] = t;
+            }
+            group_sync(bar);
+            if (wid == 0) {  // exclusive scan of the slice totals; the chunk's total after them
+                constexpr unsigned kPer = kPackChunk / 32 / 32;
+                uint32_t a[kPer], sum = 0;
+#pragma unroll
+                for (unsigned q = 0; q < kPer; q++) {
+                    const unsigned sl = lane * kPer + q;
+                    a[q] = sl < nsl ? slice[sl] : 0u;
+                    sum += a[q];
+                }
+                const uint32_t incl = warp_incl_scan(sum);
+                uint32_t run = incl - sum;
+#pragma unroll
+                for (unsigned q = 0; q < kPer; q++) {
+                    const unsigned sl = lane * kPer + q;
+                    if (sl < nsl) slice[sl] = run;
+                    run += a[q];
+                }
+                if (lane == 31) slice[kPackChunk / 32] = incl;
+            }
+            group_sync(bar);
+            const uint32_t ctot = slice[kPackChunk / 32], b0 = base & 31u;
+            for (unsigned sl = wid; sl < nsl; sl += kFseGroupThreads / 32) {
+                const unsigned j = sl * 32 + lane;
+                uint32_t v = 0, nb = 0;
+                if (j < cn) {
+                    v = sv[j] >> 1;
+                    nb = NB(v, ss[j]);
+                }
+                const uint32_t incl = warp_incl_scan(nb);
+                const uint32_t p = b0 + slice[sl] + incl - nb;  // bit offset in the chunk's words
+                if (nb) {
+                    const uint32_t bits = v & ((1u << nb) - 1u), w0 = p >> 5, sh = p & 31u;
+                    atomicOr(sw + w0, bits << sh);
+                    if (sh + nb > 32) atomicOr(sw + w0 + 1, bits >> (32 - sh));
+                }
+                if (ck && j < cn) {
+                    const unsigned e = c0 + j, i = n - 3 - e;
+                    if (i > 0 && (i & (part - 1)) == 0) {
+                        // decoder states before symbol i: the states after symbol i (the state
+                        // before symbol i - 2 of its chain) and after symbol i + 1 (before i - 1)
+                        const uint32_t odd = i + 1 <= n - 3 ? V(e + 1) : ((n - 2) & 1 ? s_i1 : s_i0);
+                        ck[i / part - 1] = FseCkpt{base + slice[sl] + incl, (uint16_t)V(e + 2), (uint16_t)odd};
+                    }
+                }
+            }
+            group_sync(bar);
+            const unsigned wfirst = base >> 5, nw = (b0 + ctot + 31) >> 5;
+            for (unsigned z = tid; z < nw; z += kFseGroupThreads) {
+                const unsigned gw = wfirst + z;
+                if (gw >= kCap) continue;
+                if (z == 0 || z == nw - 1) atomicOr(bw + gw, sw[z]);
+                else bw[gw] = sw[z];
+            }
+            base += ctot;
+        }
+        const uint32_t sym_bits = base;  // bits of all symbols
         const uint32_t total = sym_bits + 2 * tl + 1;
         body = (total + 7) / 8;
         if (body + 8 > kBlockSlot - 5 - s_hdr || s_hdr + body >= n - 1) mode = 0;  // not worth coding: raw
-        if (mode == 2) {
-            if (e1 > e0) bw[off >> 5] = 0u;
-            if (threadIdx.x == 0) bw[sym_bits >> 5] = 0u;
-        }
-        __syncthreads();
-        if (mode == 2) {
-            const unsigned lastw = (off + cnt) >> 5;
-            uint32_t wi = off >> 5, accn = off & 31u;
-            uint64_t acc = 0;
-            bool first = true;
-            auto flush_word = [&](uint32_t v) {
-                if (first || wi == lastw) atomicOr(bw + wi, v);
-                else bw[wi] = v;
-                first = false;
+        group_sync(bar);
+        if (mode == 2 && tid == 0) {  // final states (odd, then even) and the end mark
+            uint32_t p2 = sym_bits;
+            auto put = [&](uint32_t v, uint32_t nb) {
+                for (uint32_t b = 0; b < nb; b++, p2++)
+                    if ((v >> b) & 1u) atomicOr(bw + (p2 >> 5), 1u << (p2 & 31u));
             };
-            uint32_t pos = off;
-            for (unsigned e = e0; e < e1; e += kPackBatch) {
-                uint32_t vv[kPackBatch], sy[kPackBatch];
-#pragma unroll
-                for (unsigned u = 0; u < kPackBatch; u++) {
-                    const unsigned ee = min(e + u, e1 - 1);
-                    vv[u] = V(ee);
-                    sy[u] = src[n - 3 - ee];
-                }
-#pragma unroll
-                for (unsigned u = 0; u < kPackBatch; u++) {
-                    if (e + u >= e1) break;
-                    const unsigned i = n - 3 - (e + u);
-                    const uint32_t v = vv[u], nb = NB(v, sy[u]);
-                    acc |= (uint64_t)(v & ((1u << nb) - 1u)) << accn;
-                    accn += nb;
-                    pos += nb;
-                    if (ck && i > 0 && (i & (part - 1)) == 0) {
-                        // decoder states before symbol i: the states after symbol i (the state
-                        // before symbol i - 2 of its chain) and after symbol i + 1 (before i - 1)
-                        const uint32_t odd = i + 1 <= n - 3 ? V(e + u + 1) : ((n - 2) & 1 ? s_i1 : s_i0);
-                        ck[i / part - 1] = FseCkpt{pos, (uint16_t)V(e + u + 2), (uint16_t)odd};
-                    }
-                    if (accn >= 32) {
-                        flush_word((uint32_t)acc);
-                        wi++;
-                        acc >>= 32;
-                        accn -= 32;
-                    }
-                }
-            }
-            if (e1 > e0 && accn > 0) atomicOr(bw + wi, (uint32_t)acc);
-            __syncthreads();
-            if (threadIdx.x == 0) {  // final states (odd, then even) and the end mark
-                uint32_t p2 = sym_bits;
-                auto put = [&](uint32_t v, uint32_t nb) {
-                    for (uint32_t b = 0; b < nb; b++, p2++)
-                        if ((v >> b) & 1u) atomicOr(bw + (p2 >> 5), 1u << (p2 & 31u));
-                };
-                if ((sym_bits & 31u) == 0) bw[sym_bits >> 5] = 0u;
-                for (uint32_t z = (sym_bits >> 5) + 1; z <= (total - 1) >> 5; z++) bw[z] = 0u;
-                put(s_s1 & ((1u << tl) - 1), tl);
-                put(s_s0 & ((1u << tl) - 1), tl);
-                put(1u, 1u);
-            }
+            put(s_s1 & ((1u << tl) - 1), tl);
+            put(s_s0 & ((1u << tl) - 1), tl);
+            put(1u, 1u);
         }
-        __syncthreads();
+        group_sync(bar);
     }
     if (mode == 0) {  // raw
-        if (threadIdx.x == 0) out[0] = 0;
-        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) out[1 + i] = src[i];
-        if (threadIdx.x == 0) sizes[b] = 1 + n;  // flag 0
+        if (tid == 0) out[0] = 0;
+        for (unsigned i = tid; i < n; i += kFseGroupThreads) out[1 + i] = src[i];
+        if (tid == 0) sizes[b] = 1 + n;  // flag 0
     } else if (mode == 1) {  // a single repeated symbol
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             out[0] = 2;
             out[1] = src[0];
             sizes[b] = 2 | (2ULL << 56);
@@ -524,8 +597,8 @@ __global__ void __launch_bounds__(256, 4) k_fse_encode_blocks(const uint8_t *__r
         const size_t r = s_hdr + body;
         uint8_t *d = out + 5 + s_hdr;
         const uint8_t *bb = reinterpret_cast<const uint8_t *>(bw);
-        for (size_t i = threadIdx.x; i < body; i += blockDim.x) d[i] = bb[i];
-        if (threadIdx.x == 0) {
+        for (size_t i = tid; i < body; i += kFseGroupThreads) d[i] = bb[i];
+        if (tid == 0) {
             out[0] = 1;
             const uint32_t rr = (uint32_t)r;
             out[1] = (uint8_t)rr;
@@ -788,11 +861,70 @@ __global__ void k_pick_u64(const unsigned long long *__restrict__ src, const uns
     if (i < n) out[i] = src[idx[i]];
 }
 
-GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
-                      cudaStream_t st, uint32_t ckpt_part) {
-    Trace tr("gamma");
+// The FSE class blocks of the gamma classes, launched by gamma_launch; gamma_finish packs the
+// mantissas and collects the blocks.  Between the two the caller may launch other work: the class
+// blocks are long sequential chains, so they go to the GPU before the order-1 chain encoder.
+struct GammaBlocks {
+    long long T = 0;
+    std::vector<unsigned long long> gstart;
+    uint8_t *cls = nullptr;
+    std::vector<BlockJob> jobs;
+    std::vector<int> job_group;
+    uint8_t *slots = nullptr;
+    unsigned long long *sizes = nullptr;
+    FseCkpt *cks = nullptr;
+    size_t ck_per_block = 0;
+};
+
+GammaBlocks gamma_launch(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
+                         cudaStream_t st, uint32_t ckpt_part, cudaEvent_t queued = nullptr) {
+    GammaBlocks gb;
+    gb.gstart = gstart;
     const int G = (int)gstart.size() - 1;
     const long long T = (long long)gstart.back();
+    gb.T = T;
+    if (T == 0) {
+        if (queued) FB2_CUDA(cudaEventRecord(queued, st));
+        return gb;
+    }
+    uint8_t *cls = pool.get<uint8_t>(T);
+    gb.cls = cls;
+    k_gamma_cls<<<grid_for(T, 256), 256, 0, st>>>(d_vals, T, cls);
+    FB2_CHECK_LAUNCH();
+    for (int g = 0; g < G; g++) {
+        for (unsigned long long b = gstart[g]; b < gstart[g + 1]; b += FBLK) {
+            gb.jobs.push_back(BlockJob{b, (unsigned)std::min<unsigned long long>(FBLK, gstart[g + 1] - b), 0, 0, 0});
+            gb.job_group.push_back(g);
+        }
+    }
+    const size_t nj = gb.jobs.size();
+    if (std::getenv("FALCONS_TRACE"))
+        std::fprintf(stderr, "[falcons trace] escapes: %lld values in %d groups, %zu class blocks\n", T, G, nj);
+    BlockJob *d_jobs = h2d(pool, gb.jobs, st);
+    gb.slots = pool.get<uint8_t>(nj * kBlockSlot);
+    uint8_t *bits = pool.get<uint8_t>(nj * kBlockSlot);
+    gb.sizes = pool.get<unsigned long long>(nj);
+    gb.ck_per_block = ckpt_part ? FBLK / ckpt_part : 0;
+    gb.cks = ckpt_part ? pool.get<FseCkpt>(nj * gb.ck_per_block) : nullptr;
+    uint32_t *recs = pool.get<uint32_t>(nj * kFseRecWords);
+    std::vector<uint32_t> order(nj);
+    for (size_t j = 0; j < nj; j++) order[j] = (uint32_t)j;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return gb.jobs[a].n > gb.jobs[b].n; });
+    uint32_t *d_order = h2d(pool, order, st);
+    if (queued) FB2_CUDA(cudaEventRecord(queued, st));  // what the blocks wait for is on the stream
+    constexpr int smem = (int)(kFseGroups * kFseNxtBytes);
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_fse_encode_blocks<<<(unsigned)((nj + kFseGroups - 1) / kFseGroups), kFseGroups * kFseGroupThreads, smem, st>>>(
+        cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, ckpt_part ? ckpt_part : 4096u, gb.cks, recs, d_order);
+    FB2_CHECK_LAUNCH();
+    return gb;
+}
+
+GammaOut gamma_finish(Pool &pool, const GammaBlocks &gb, const uint32_t *d_vals, cudaStream_t st) {
+    Trace tr("gamma");
+    const std::vector<unsigned long long> &gstart = gb.gstart;
+    const int G = (int)gstart.size() - 1;
+    const long long T = gb.T;
     GammaOut out;
     out.cls_pieces.resize(G);
     out.cls_n.resize(G);
@@ -802,9 +934,7 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     out.man_ptr.assign(G, nullptr);
     out.man_bytes.assign(G, 0);
     if (T == 0) return out;
-    uint8_t *cls = pool.get<uint8_t>(T);
-    k_gamma_cls<<<grid_for(T, 256), 256, 0, st>>>(d_vals, T, cls);
-    FB2_CHECK_LAUNCH();
+    const uint8_t *cls = gb.cls;
     unsigned long long *boff = pool.get<unsigned long long>(T + 1);
     void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
     exclusive_scan<uint8_t, unsigned long long>(cls, T, boff, sc, st);
@@ -813,12 +943,12 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     unsigned long long *d_gb = pool.get<unsigned long long>(G + 1);
     k_pick_u64<<<grid_for(G + 1, 256), 256, 0, st>>>(boff, d_gstart, G + 1, d_gb);
     FB2_CHECK_LAUNCH();
-    const std::vector<unsigned long long> gb = d2h(d_gb, (size_t)G + 1, st);
+    const std::vector<unsigned long long> gbits = d2h(d_gb, (size_t)G + 1, st);
     tr.mark("group bits known");
     std::vector<unsigned long long> gword(G);
     unsigned long long words = 0;
     for (int g = 0; g < G; g++) {
-        const unsigned long long bits = gb[g + 1] - gb[g];
+        const unsigned long long bits = gbits[g + 1] - gbits[g];
         out.man_bytes[g] = (size_t)((bits + 7) / 8);
         gword[g] = words;
         words += (bits + 31) / 32 + 2;
@@ -829,47 +959,24 @@ GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsi
     k_gamma_pack<<<grid_for(T, 256, 148 * 8), 256, 0, st>>>(d_vals, cls, boff, T, d_gstart, G, d_gword, wbuf);
     FB2_CHECK_LAUNCH();
     for (int g = 0; g < G; g++) out.man_ptr[g] = reinterpret_cast<const uint8_t *>(wbuf + gword[g]);
-    // FSE class blocks
-    std::vector<BlockJob> jobs;
-    std::vector<int> job_group;
-    for (int g = 0; g < G; g++) {
-        for (unsigned long long b = gstart[g]; b < gstart[g + 1]; b += FBLK) {
-            jobs.push_back(BlockJob{b, (unsigned)std::min<unsigned long long>(FBLK, gstart[g + 1] - b), 0, 0, 0});
-            job_group.push_back(g);
-        }
-    }
-    if (std::getenv("FALCONS_TRACE"))
-        std::fprintf(stderr, "[falcons trace] escapes: %lld values in %d groups, %zu class blocks\n", T, G,
-                     jobs.size());
-    BlockJob *d_jobs = h2d(pool, jobs, st);
-    uint8_t *slots = pool.get<uint8_t>(jobs.size() * kBlockSlot);
-    uint8_t *bits = pool.get<uint8_t>(jobs.size() * kBlockSlot);
-    unsigned long long *sizes = pool.get<unsigned long long>(jobs.size());
-    const size_t ck_per_block = ckpt_part ? FBLK / ckpt_part : 0;
-    FseCkpt *cks = ckpt_part ? pool.get<FseCkpt>(jobs.size() * ck_per_block) : nullptr;
-    uint32_t *recs = pool.get<uint32_t>(jobs.size() * kFseRecWords);
-    std::vector<uint32_t> order(jobs.size());
-    for (size_t j = 0; j < jobs.size(); j++) order[j] = (uint32_t)j;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return jobs[a].n > jobs[b].n; });
-    uint32_t *d_order = h2d(pool, order, st);
-    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFseNxtBytes));
-    k_fse_encode_blocks<<<(unsigned)jobs.size(), 256, kFseNxtBytes, st>>>(cls, d_jobs, slots, sizes, bits,
-                                                                         ckpt_part ? ckpt_part : 4096u, cks, recs,
-                                                                         d_order);
-    FB2_CHECK_LAUNCH();
-    tr.mark("class blocks launched");
-    std::vector<unsigned long long> hs = d2h(sizes, jobs.size(), st);
+    std::vector<unsigned long long> hs = d2h(gb.sizes, gb.jobs.size(), st);
     tr.mark("class blocks coded");
-    for (size_t j = 0; j < jobs.size(); j++) {
-        const int g = job_group[j];
+    for (size_t j = 0; j < gb.jobs.size(); j++) {
+        const int g = gb.job_group[j];
         const size_t sz = (size_t)(hs[j] & ((1ULL << 56) - 1));
-        out.cls_pieces[g].push_back({slots + j * kBlockSlot, sz});
-        out.cls_n[g].push_back(jobs[j].n);
+        out.cls_pieces[g].push_back({gb.slots + j * kBlockSlot, sz});
+        out.cls_n[g].push_back(gb.jobs[j].n);
         out.cls_flag[g].push_back((uint8_t)(hs[j] >> 56));
-        out.cls_ck[g].push_back(cks ? cks + j * ck_per_block : nullptr);
+        out.cls_ck[g].push_back(gb.cks ? gb.cks + j * gb.ck_per_block : nullptr);
         out.cls_bytes[g] += sz;
     }
     return out;
+}
+
+GammaOut gamma_encode(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
+                      cudaStream_t st, uint32_t ckpt_part) {
+    const GammaBlocks gb = gamma_launch(pool, d_vals, gstart, st, ckpt_part);
+    return gamma_finish(pool, gb, d_vals, st);
 }
 
 // Adds the fse_enc records of group g, recording each record's header bytes for the index.
@@ -2386,6 +2493,21 @@ __global__ void __launch_bounds__(kScanThreads) k_esc_tiles(const int16_t *__res
     if (threadIdx.x == 0) cnt[blockIdx.x] = tot;
 }
 
+// Escapes before each of npos code positions: the tile offset of the position's tile (exclusive
+// scan of the tile counts) plus the escapes of the tile before the position, one warp per position.
+__global__ void __launch_bounds__(256) k_esc_before(const int16_t *__restrict__ q,
+                                                    const uint32_t *__restrict__ tile_off,
+                                                    const unsigned long long *__restrict__ pos, int npos,
+                                                    unsigned long long *__restrict__ out) {
+    const int w = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = (int)(threadIdx.x & 31u);
+    if (w >= npos) return;
+    const unsigned long long p = pos[w], t = p / kScanTile;
+    uint32_t c = 0;
+    for (unsigned long long i = t * kScanTile + lane; i < p; i += 32) c += o1_sym(q[i]) == O1_NSYM - 1;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) out[w] = (unsigned long long)tile_off[t] + c;
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_esc_extract(const int16_t *__restrict__ q, long long n,
                                                              const uint32_t *__restrict__ tile_off,
                                                              uint32_t *__restrict__ vals, int16_t *__restrict__ raw) {
@@ -2653,18 +2775,9 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         uint16_t *keys = pool.get<uint16_t>((size_t)N + 8);
         FB2_CUDA(cudaMemsetAsync(hist, 0, (size_t)S * O1_NCTX * O1_NSYM * 4, st));
         FB2_CUDA(cudaMemsetAsync(nvk, 0, (size_t)S * kMaxK * 4, st));
-        enable_big_smem();
-        {
-            // about four CTAs per SM over all segments, a slice at least 64 Ki codes long
-            const long long want = (4LL * 148 + S - 1) / S;
-            const long long U = std::max<long long>(1, std::min<long long>(want, (seg + 65535) / 65536));
-            k_o1_hist<<<dim3((unsigned)S, (unsigned)U), 1024, kHistSmem, st>>>(
-                q, d_segs, hist, nvk, keys, (reinterpret_cast<uintptr_t>(q) & 15) == 0);
-        }
-        FB2_CHECK_LAUNCH();
         // The escape side stream (escape values in index order, their gamma classes, the FSE class
-        // blocks) needs only the codes and the per-chain escape counts of the histogram pass, so
-        // with a second stream it runs next to the table builds and the chain encoder.
+        // blocks) needs only the codes, so it forks before the histogram pass and runs next to it,
+        // the table builds and the chain encoder.
         const long long tiles = std::max<long long>(1, (N + kScanTile - 1) / kScanTile);
         uint32_t *tcnt = pool.get<uint32_t>(tiles + 2);
         FB2_CUDA(cudaMemsetAsync(tcnt, 0, (tiles + 2) * 4, st));
@@ -2694,6 +2807,43 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         }
         k_scan_small<uint32_t><<<1, 1024, 0, es>>>(tcnt, tiles);
         FB2_CHECK_LAUNCH();
+        // escapes before every segment start (the groups of the escape stream)
+        unsigned long long *d_gstart = spool.get<unsigned long long>(S + 1);
+        {
+            std::vector<unsigned long long> pos(S + 1);
+            for (long long g = 0; g < S; g++) pos[g] = segs[g].lo;
+            pos[S] = (unsigned long long)N;
+            unsigned long long *d_pos = h2d(spool, pos, es);
+            k_esc_before<<<(unsigned)((S + 1 + 7) / 8), 256, 0, es>>>(q, tcnt, d_pos, (int)(S + 1), d_gstart);
+            FB2_CHECK_LAUNCH();
+        }
+        enable_big_smem();
+        tr.gpu("histogram start", st);
+        {
+            // about four CTAs per SM over all segments, a slice at least 64 Ki codes long
+            const long long want = (4LL * 148 + S - 1) / S;
+            const long long U = std::max<long long>(1, std::min<long long>(want, (seg + 65535) / 65536));
+            k_o1_hist<<<dim3((unsigned)S, (unsigned)U), 1024, kHistSmem, st>>>(
+                q, d_segs, hist, nvk, keys, (reinterpret_cast<uintptr_t>(q) & 15) == 0);
+        }
+        FB2_CHECK_LAUNCH();
+        tr.gpu("histogram done", st);
+        // escapes in index order, on the second stream (the host waits here for their count; the
+        // histogram pass runs meanwhile)
+        const std::vector<unsigned long long> gstart = d2h(d_gstart, (size_t)S + 1, es);
+        const unsigned long long E = gstart[S];
+        uint32_t *evals = spool.get<uint32_t>(E + 1);
+        int16_t *eraw = spool.get<int16_t>(E + 1);
+        if (E > 0) {
+            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt, evals, eraw);
+            FB2_CHECK_LAUNCH();
+        }
+        // the class blocks (long sequential chains) reach the GPU before the chain encoder, so that
+        // they take a few SMs of their own instead of waiting for the chain encoder's last wave
+        const bool queue_first = fork && tune.queued_ev != nullptr;
+        const GammaBlocks gblocks = gamma_launch(spool, evals, gstart, es, cc.fse_part,
+                                                 queue_first ? tune.queued_ev : nullptr);
+        tr.gpu("class blocks done", es);
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
         std::vector<int> seg_region(S, 0), rs{0};
@@ -2740,6 +2890,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             k_spec_image<<<dim3((items + 255) / 256, (unsigned)R), 256, 0, st>>>(stab, stt, rhist, image, meta);
             FB2_CHECK_LAUNCH();
         }
+        if (queue_first) FB2_CUDA(cudaStreamWaitEvent(st, tune.queued_ev, 0));
+        tr.mark("class blocks launched");
         // chain output slots
         const long long nchains = S * kMaxK;
         std::vector<unsigned long long> soff(nchains + 1, 0);
@@ -2765,31 +2917,28 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             uint32_t *stage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
             uint32_t *rstage = pool.get<uint32_t>(ctas.size() * kSpecThreads * spec_stage_words(enc_part));
             enable_big_smem();
+            tr.gpu("chain encoder start", st);
             k_o1_encode_spec<<<(unsigned)ctas.size(), kSpecThreads, kSpecSmem, st>>>(
                 keys, d_segs, d_ctas, image, meta, sparse, sparse_bits, stage, rstage, slots, d_soff, blen, enc_part, o1ck,
                 d_ck_off, ck_every, d_err);
             FB2_CHECK_LAUNCH();
+            tr.gpu("chain encoder done", st);
             tr.mark("chains launched");
         }
-        // escapes in index order, on the second stream (the histogram pass has finished there)
-        std::vector<uint32_t> h_nvk = d2h(nvk, (size_t)S * kMaxK, es);
-        std::vector<unsigned long long> gstart(S + 1, 0);
+        GammaOut go = gamma_finish(spool, gblocks, evals, es);
+        tr.gpu("escape mantissas packed", es);
+        // the chains' escape counts (stream header) from the histogram pass; their sums per segment
+        // are the escape groups counted above
+        const std::vector<uint32_t> h_nvk = d2h(nvk, (size_t)S * kMaxK, st);
         for (long long g = 0; g < S; g++) {
             unsigned long long e = 0;
             for (int k = 0; k < K; k++) e += h_nvk[g * kMaxK + k];
-            gstart[g + 1] = gstart[g] + e;
+            if (e != gstart[g + 1] - gstart[g]) throw std::runtime_error("escape counts of the two passes differ");
         }
-        const unsigned long long E = gstart[S];
-        uint32_t *evals = spool.get<uint32_t>(E + 1);
-        int16_t *eraw = spool.get<int16_t>(E + 1);
-        if (E > 0) {
-            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt, evals, eraw);
-            FB2_CHECK_LAUNCH();
-        }
-        GammaOut go = gamma_encode(spool, evals, gstart, es, cc.fse_part);
         tr.mark("escapes coded");
         std::vector<unsigned long long> h_blen = d2h(blen, (size_t)nchains, st);
         std::vector<int> h_err = d2h(d_err, 5, st);
+        tr.gpu_dump();
         if (h_err[0]) throw std::runtime_error("tANS encoding failed (table construction or chain repair)");
         // Decode checkpoints cost 12 bytes each: keep them within 1.5 % of the chains' bytes by
         // keeping every m-th one (m a power of two; the decoder's parts become m times longer, so
@@ -3059,6 +3208,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 uid[g] = (int)lead.size() - 1;
             }
         }
+        tr.mark("shared tables found");
         const int U = (int)lead.size();
         const int ntab = U * O1_NCTX;
         uint16_t *nf = pool.get<uint16_t>((size_t)ntab * O1_NSYM);
@@ -3068,6 +3218,9 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                 pcs.push_back(Piece{d_in + lead[u], (unsigned long long)u * O1_NCTX * O1_NSYM * 2, O1_NCTX * O1_NSYM * 2});
             launch_gather(pool, pcs, reinterpret_cast<uint8_t *>(nf), st);
         }
+        // the host ranks the tables' contexts while the device builds the decode tables
+        const std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
+        tr.mark("tables read");
         uint32_t *dt = pool.get<uint32_t>((size_t)ntab * O1_M);
         uint8_t *spread = pool.get<uint8_t>(16);
         k_o1_dtable<<<ntab, kTabThreads, 0, st>>>(nf, dt, spread, d_err);
@@ -3085,8 +3238,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         }
         DecChain *dch = h2d(pool, chains, st);
         {
-            std::vector<uint16_t> hnf = d2h(nf, (size_t)ntab * O1_NSYM, st);
-            tr.mark("decode tables built");
+            tr.mark("decode tables launched");
             std::vector<unsigned long long> maps(U), revs(U);
             for (int u = 0; u < U; u++) {
                 auto mr = hot_contexts(hnf.data() + (size_t)u * O1_NCTX * O1_NSYM, kDecSlots);

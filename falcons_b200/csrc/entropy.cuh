@@ -62,6 +62,10 @@ struct EntropyTuning {
     // encoder; none: everything runs on the calling stream
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+    // recorded on `side` when the escape class blocks are next in line; the chain encoder waits
+    // for it, so that both are queued when its CTAs are dispatched and the blocks (on the
+    // higher-priority stream) take their SMs first
+    cudaEvent_t queued_ev = nullptr;
 };
 
 EntropyChoice choose_entropy(Context &ctx, const int16_t *d_codes, size_t n, cudaStream_t st);

@@ -204,6 +204,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             tune.side = side_stream(ctx);
             tune.fork_ev = ctx.side_ev[0];
             tune.join_ev = ctx.side_ev[1];
+            tune.queued_ev = ctx.side_ev[2];
             entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st, tune);
             tr.mark("entropy stage launched");
             if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
