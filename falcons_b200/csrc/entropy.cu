@@ -116,6 +116,7 @@ constexpr unsigned kFseRecWords = kFseChainRec;  // both chains, 2 records per w
 // kFseMaxLog per position, plus the partial word in front and one behind), staged with its records,
 // symbols and slice offsets in the next-state table's space.
 constexpr unsigned kPackChunk = 8192;
+constexpr unsigned kStageBatch = 16;  // loads a thread has in flight while staging a chunk
 constexpr unsigned kPackWords = kPackChunk * kFseMaxLog / 32 + 2;
 static_assert(kPackChunk * 3 + (kPackWords + kPackChunk / 32 + 1) * 4 <= kFseNxtBytes,
               "the packer's staging fits the next-state table's space");
@@ -343,13 +344,16 @@ __global__ void __launch_bounds__(kFseGroups * kFseGroupThreads, 4 / kFseGroups)
             }
             group_sync(bar);
         }
-        if ((tid & 31u) == 0 && tid < 64) {
+        // The chains run on the group's warps cw, cw + 1, chosen so that the CTA's eight chain warps
+        // sit two on each SM sub-partition (warp w of a CTA issues from sub-partition w mod 4).
+        const unsigned cw = (2u * grp) & 3u;
+        if ((tid & 31u) == 0 && (tid >> 5) - cw < 2u) {
             // The two state chains, one per warp: chain k codes the symbols i <= n - 3 of parity k
             // from the top down (step j codes symbol top - 2 j), starting from the state that
             // symbol n-1 or n-2 (of parity k) initialised.  Each step records twice the state
             // before it minus L (16 bits, table log <= 11): its low bits are the emitted ones, and
             // the record of the chain's next step holds the state after it.
-            const unsigned k = tid >> 5;
+            const unsigned k = (tid >> 5) - cw;
             uint32_t v;  // the state minus L
             {
                 const unsigned i0 = ((n - 1) % 2 == k) ? n - 1 : n - 2;
@@ -497,10 +501,24 @@ __global__ void __launch_bounds__(kFseGroups * kFseGroupThreads, 4 / kFseGroups)
         for (unsigned c0 = 0; c0 < ns; c0 += kPackChunk) {
             const unsigned cn = min(kPackChunk, ns - c0), nsl = (cn + 31) / 32;
             group_sync(bar);  // the previous chunk's words are out (the first time: the scratch is zero)
-            for (unsigned j = tid; j < cn; j += kFseGroupThreads) {
-                const unsigned e = c0 + j;
-                sv[j] = rec16[((e & 1u) ? offB : offA) + (e >> 1)];
-                ss[j] = src[n - 3 - e];
+            // the records come from L2: each thread issues a batch of loads before it stores any
+#pragma unroll
+            for (unsigned h = 0; h < kPackChunk / kFseGroupThreads; h += kStageBatch) {
+                uint32_t r[kStageBatch], y[kStageBatch];
+#pragma unroll
+                for (unsigned u = 0; u < kStageBatch; u++) {
+                    const unsigned j = tid + (h + u) * kFseGroupThreads, e = c0 + j;
+                    r[u] = j < cn ? rec16[((e & 1u) ? offB : offA) + (e >> 1)] : 0u;
+                    y[u] = j < cn ? src[n - 3 - e] : 0u;
+                }
+#pragma unroll
+                for (unsigned u = 0; u < kStageBatch; u++) {
+                    const unsigned j = tid + (h + u) * kFseGroupThreads;
+                    if (j < cn) {
+                        sv[j] = (uint16_t)r[u];
+                        ss[j] = (uint8_t)y[u];
+                    }
+                }
             }
             for (unsigned z = tid; z < kPackWords; z += kFseGroupThreads) sw[z] = 0u;
             group_sync(bar);
@@ -2817,6 +2835,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             k_esc_before<<<(unsigned)((S + 1 + 7) / 8), 256, 0, es>>>(q, tcnt, d_pos, (int)(S + 1), d_gstart);
             FB2_CHECK_LAUNCH();
         }
+        tr.gpu("escape counts done", es);
         enable_big_smem();
         tr.gpu("histogram start", st);
         {
@@ -2828,22 +2847,6 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         }
         FB2_CHECK_LAUNCH();
         tr.gpu("histogram done", st);
-        // escapes in index order, on the second stream (the host waits here for their count; the
-        // histogram pass runs meanwhile)
-        const std::vector<unsigned long long> gstart = d2h(d_gstart, (size_t)S + 1, es);
-        const unsigned long long E = gstart[S];
-        uint32_t *evals = spool.get<uint32_t>(E + 1);
-        int16_t *eraw = spool.get<int16_t>(E + 1);
-        if (E > 0) {
-            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt, evals, eraw);
-            FB2_CHECK_LAUNCH();
-        }
-        // the class blocks (long sequential chains) reach the GPU before the chain encoder, so that
-        // they take a few SMs of their own instead of waiting for the chain encoder's last wave
-        const bool queue_first = fork && tune.queued_ev != nullptr;
-        const GammaBlocks gblocks = gamma_launch(spool, evals, gstart, es, cc.fse_part,
-                                                 queue_first ? tune.queued_ev : nullptr);
-        tr.gpu("class blocks done", es);
         // table regions: segments whose statistics come from the same part of the code stream
         // share one table set (tune.regions holds the code positions where statistics change)
         std::vector<int> seg_region(S, 0), rs{0};
@@ -2890,6 +2893,23 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
             k_spec_image<<<dim3((items + 255) / 256, (unsigned)R), 256, 0, st>>>(stab, stt, rhist, image, meta);
             FB2_CHECK_LAUNCH();
         }
+        // escapes in index order, on the second stream (the host waits here for their count; the
+        // histogram pass and the table builds, launched above, run meanwhile)
+        const std::vector<unsigned long long> gstart = d2h(d_gstart, (size_t)S + 1, es);
+        const unsigned long long E = gstart[S];
+        uint32_t *evals = spool.get<uint32_t>(E + 1);
+        int16_t *eraw = spool.get<int16_t>(E + 1);
+        if (E > 0) {
+            k_esc_extract<<<(unsigned)tiles, kScanThreads, 0, es>>>(q, N, tcnt, evals, eraw);
+            FB2_CHECK_LAUNCH();
+        }
+        tr.gpu("escapes extracted", es);
+        // the class blocks (long sequential chains) reach the GPU before the chain encoder, so that
+        // they take a few SMs of their own instead of waiting for the chain encoder's last wave
+        const bool queue_first = fork && tune.queued_ev != nullptr;
+        const GammaBlocks gblocks = gamma_launch(spool, evals, gstart, es, cc.fse_part,
+                                                 queue_first ? tune.queued_ev : nullptr);
+        tr.gpu("class blocks done", es);
         if (queue_first) FB2_CUDA(cudaStreamWaitEvent(st, tune.queued_ev, 0));
         tr.mark("class blocks launched");
         // chain output slots
