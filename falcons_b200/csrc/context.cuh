@@ -81,15 +81,12 @@ struct Context {
     }
 };
 
-// The context's second stream (non-blocking), created on first use on the current device, at the
-// device's highest priority: it carries the escape coders, whose CTAs are long sequential chains,
-// and those must take their SMs before the chain encoder's CTAs queued beside them.
+// The context's second stream (non-blocking), created on first use on the current device.  (At
+// the highest stream priority it let the large encoders of one field start a few percent sooner,
+// but under many concurrent requests it held back the other workers' kernels: serving latency
+// several times higher.)
 inline cudaStream_t side_stream(Context &ctx) {
-    if (!ctx.side) {
-        int least = 0, greatest = 0;
-        FB2_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        FB2_CUDA(cudaStreamCreateWithPriority(&ctx.side, cudaStreamNonBlocking, greatest));
-    }
+    if (!ctx.side) FB2_CUDA(cudaStreamCreateWithFlags(&ctx.side, cudaStreamNonBlocking));
     for (auto &e : ctx.side_ev)
         if (!e) FB2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return ctx.side;

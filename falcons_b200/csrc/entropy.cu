@@ -131,10 +131,11 @@ struct FseSmem {
     uint16_t state_table[1 << kFseMaxLog];
     uint8_t sym[1 << kFseMaxLog];
 };
-// A CTA codes kFseGroups blocks side by side, one group of kFseGroupThreads threads each, with
-// its own shared memory and its own named barrier: the CTA fills an SM (registers), so the blocks
-// of one launch sit on a quarter as many SMs as one CTA per block would spread over, and the chain
-// encoder launched beside them keeps the other SMs.
+// A CTA codes G blocks side by side, one group of kFseGroupThreads threads each, with its own
+// shared memory and its own named barrier.  G = 1 when the blocks and the chain encoder's CTAs
+// together fit the SMs (a block alone on an SM codes fastest); G = kFseGroups otherwise: the CTA
+// fills an SM (registers), so the blocks sit on a quarter as many SMs as one CTA per block would
+// spread over, and the chain encoder launched beside them keeps the other SMs.
 constexpr unsigned kFseGroups = 4, kFseGroupThreads = 256;
 struct FseGroupSmem {
     FseSmem w;
@@ -168,15 +169,16 @@ __device__ __forceinline__ uint32_t group_excl_scan(uint32_t v, uint32_t *sh, ui
     return before + incl - v;
 }
 
-__global__ void __launch_bounds__(kFseGroups * kFseGroupThreads, 4 / kFseGroups)
+template <unsigned G>
+__global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
     k_fse_encode_blocks(const uint8_t *__restrict__ cls, const BlockJob *__restrict__ jobs, unsigned njobs,
                         uint8_t *__restrict__ slots, unsigned long long *__restrict__ sizes,
                         uint8_t *__restrict__ scratch, uint32_t part, FseCkpt *__restrict__ cks,
                         uint32_t *__restrict__ recs, const uint32_t *__restrict__ order) {
-    __shared__ FseGroupSmem groups[kFseGroups];
+    __shared__ FseGroupSmem groups[G];
     extern __shared__ uint4 s_nxt_all[];  // the groups' next-state tables (kFseNxtBytes each)
     const unsigned grp = threadIdx.x / kFseGroupThreads, tid = threadIdx.x % kFseGroupThreads;
-    const unsigned slot = blockIdx.x * kFseGroups + grp;
+    const unsigned slot = blockIdx.x * G + grp;
     if (slot >= njobs) return;  // the other groups synchronise on barriers of their own
     const unsigned bar = 1 + grp;  // named barrier of this group (0 is the CTA's)
     FseGroupSmem &gm = groups[grp];
@@ -894,8 +896,9 @@ struct GammaBlocks {
     size_t ck_per_block = 0;
 };
 
+// `beside`: CTAs of whole SMs that run next to the class blocks (the chain encoder's).
 GammaBlocks gamma_launch(Pool &pool, const uint32_t *d_vals, const std::vector<unsigned long long> &gstart,
-                         cudaStream_t st, uint32_t ckpt_part, cudaEvent_t queued = nullptr) {
+                         cudaStream_t st, uint32_t ckpt_part, cudaEvent_t queued = nullptr, size_t beside = 0) {
     GammaBlocks gb;
     gb.gstart = gstart;
     const int G = (int)gstart.size() - 1;
@@ -930,10 +933,19 @@ GammaBlocks gamma_launch(Pool &pool, const uint32_t *d_vals, const std::vector<u
     std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return gb.jobs[a].n > gb.jobs[b].n; });
     uint32_t *d_order = h2d(pool, order, st);
     if (queued) FB2_CUDA(cudaEventRecord(queued, st));  // what the blocks wait for is on the stream
-    constexpr int smem = (int)(kFseGroups * kFseNxtBytes);
-    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_fse_encode_blocks<<<(unsigned)((nj + kFseGroups - 1) / kFseGroups), kFseGroups * kFseGroupThreads, smem, st>>>(
-        cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, ckpt_part ? ckpt_part : 4096u, gb.cks, recs, d_order);
+    const uint32_t part = ckpt_part ? ckpt_part : 4096u;
+    if (nj + beside > (size_t)sm_count()) {
+        constexpr unsigned G = kFseGroups;
+        constexpr int smem = (int)(G * kFseNxtBytes);
+        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_fse_encode_blocks<G><<<(unsigned)((nj + G - 1) / G), G * kFseGroupThreads, smem, st>>>(
+            cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order);
+    } else {
+        constexpr int smem = (int)kFseNxtBytes;
+        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_fse_encode_blocks<1><<<(unsigned)nj, kFseGroupThreads, smem, st>>>(cls, d_jobs, (unsigned)nj, gb.slots,
+                                                                            gb.sizes, bits, part, gb.cks, recs, d_order);
+    }
     FB2_CHECK_LAUNCH();
     return gb;
 }
@@ -2908,7 +2920,7 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         // they take a few SMs of their own instead of waiting for the chain encoder's last wave
         const bool queue_first = fork && tune.queued_ev != nullptr;
         const GammaBlocks gblocks = gamma_launch(spool, evals, gstart, es, cc.fse_part,
-                                                 queue_first ? tune.queued_ev : nullptr);
+                                                 queue_first ? tune.queued_ev : nullptr, (size_t)(S * K));
         tr.gpu("class blocks done", es);
         if (queue_first) FB2_CUDA(cudaStreamWaitEvent(st, tune.queued_ev, 0));
         tr.mark("class blocks launched");

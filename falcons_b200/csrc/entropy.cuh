@@ -63,8 +63,8 @@ struct EntropyTuning {
     cudaStream_t side = nullptr;
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     // recorded on `side` when the escape class blocks are next in line; the chain encoder waits
-    // for it, so that both are queued when its CTAs are dispatched and the blocks (on the
-    // higher-priority stream) take their SMs first
+    // for it, so that the blocks, launched first, take their SMs before the encoder's CTAs fill
+    // the rest
     cudaEvent_t queued_ev = nullptr;
 };
 
