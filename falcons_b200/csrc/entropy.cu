@@ -145,8 +145,21 @@ struct FseGroupSmem {
     uint32_t sh[32];
 };
 
+// A group's barrier.  bar.sync counts whole warps, so the warp is made convergent first (after
+// code where some lanes ran on alone, such as the two chain lanes).
 __device__ __forceinline__ void group_sync(unsigned bar) {
+    __syncwarp();
     asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(kFseGroupThreads) : "memory");
+}
+
+// Phase times of a block (traced calls only): the global timer at the block's start and after its
+// count, plan, tables, chain walk, pack and output, kFsePhases words per block.
+constexpr int kFsePhases = 8;
+__device__ __forceinline__ void fse_phase(unsigned long long *phase, unsigned slot, int k) {
+    if (!phase) return;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    phase[(size_t)slot * kFsePhases + k] = t;
 }
 
 // Exclusive scan over a group's threads (tid = index in the group), total of the group in `total`.
@@ -174,7 +187,8 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
     k_fse_encode_blocks(const uint8_t *__restrict__ cls, const BlockJob *__restrict__ jobs, unsigned njobs,
                         uint8_t *__restrict__ slots, unsigned long long *__restrict__ sizes,
                         uint8_t *__restrict__ scratch, uint32_t part, FseCkpt *__restrict__ cks,
-                        uint32_t *__restrict__ recs, const uint32_t *__restrict__ order) {
+                        uint32_t *__restrict__ recs, const uint32_t *__restrict__ order,
+                        unsigned long long *__restrict__ phase) {
     __shared__ FseGroupSmem groups[G];
     extern __shared__ uint4 s_nxt_all[];  // the groups' next-state tables (kFseNxtBytes each)
     const unsigned grp = threadIdx.x / kFseGroupThreads, tid = threadIdx.x % kFseGroupThreads;
@@ -190,6 +204,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
     unsigned *s_lead = gm.lead;
     uint32_t *s_sh = gm.sh;
     const unsigned b = order[slot];  // the largest blocks first
+    if (tid == 0) fse_phase(phase, slot, 0);
     const BlockJob jb = jobs[b];
     const uint8_t *src = cls + jb.src;
     uint8_t *out = slots + (size_t)b * kBlockSlot;
@@ -229,6 +244,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
         if (run) atomicAdd(&w.count[cur], run);
     }
     group_sync(bar);
+    if (tid == 0) fse_phase(phase, slot, 1);
     if (tid == 0) {
         int mode = 0;
         unsigned tl = 0, hdr = 0, maxSV = 255;
@@ -267,6 +283,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
         s_maxsv = maxSV;
     }
     group_sync(bar);
+    if (tid == 0) fse_phase(phase, slot, 2);
     if (s_mode == 2) {
         const unsigned tl = s_tl, L = 1u << tl, maxSV = s_maxsv;
         {
@@ -349,6 +366,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
         // The chains run on the group's warps cw, cw + 1, chosen so that the CTA's eight chain warps
         // sit two on each SM sub-partition (warp w of a CTA issues from sub-partition w mod 4).
         const unsigned cw = (2u * grp) & 3u;
+        if (tid == 0) fse_phase(phase, slot, 3);
         if ((tid & 31u) == 0 && (tid >> 5) - cw < 2u) {
             // The two state chains, one per warp: chain k codes the symbols i <= n - 3 of parity k
             // from the top down (step j codes symbol top - 2 j), starting from the state that
@@ -467,6 +485,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
         }
     }
     group_sync(bar);
+    if (tid == 0) fse_phase(phase, slot, 4);
     int mode = s_mode;
     size_t body = 0;
     if (mode == 2) {
@@ -603,6 +622,7 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
         }
         group_sync(bar);
     }
+    if (tid == 0) fse_phase(phase, slot, 5);
     if (mode == 0) {  // raw
         if (tid == 0) out[0] = 0;
         for (unsigned i = tid; i < n; i += kFseGroupThreads) out[1 + i] = src[i];
@@ -627,6 +647,10 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
             out[4] = (uint8_t)(rr >> 24);
             sizes[b] = (5 + r) | (1ULL << 56);
         }
+    }
+    if (phase) {
+        group_sync(bar);
+        if (tid == 0) fse_phase(phase, slot, 6);
     }
 }
 
@@ -894,6 +918,7 @@ struct GammaBlocks {
     unsigned long long *sizes = nullptr;
     FseCkpt *cks = nullptr;
     size_t ck_per_block = 0;
+    unsigned long long *phase = nullptr;  // per-block phase times, traced calls only
 };
 
 // `beside`: CTAs of whole SMs that run next to the class blocks (the chain encoder's).
@@ -934,17 +959,21 @@ GammaBlocks gamma_launch(Pool &pool, const uint32_t *d_vals, const std::vector<u
     uint32_t *d_order = h2d(pool, order, st);
     if (queued) FB2_CUDA(cudaEventRecord(queued, st));  // what the blocks wait for is on the stream
     const uint32_t part = ckpt_part ? ckpt_part : 4096u;
+    if (std::getenv("FALCONS_TRACE")) {
+        gb.phase = pool.get<unsigned long long>(nj * kFsePhases);
+        FB2_CUDA(cudaMemsetAsync(gb.phase, 0, nj * kFsePhases * 8, st));
+    }
     if (nj + beside > (size_t)sm_count()) {
         constexpr unsigned G = kFseGroups;
         constexpr int smem = (int)(G * kFseNxtBytes);
         FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         k_fse_encode_blocks<G><<<(unsigned)((nj + G - 1) / G), G * kFseGroupThreads, smem, st>>>(
-            cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order);
+            cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order, gb.phase);
     } else {
         constexpr int smem = (int)kFseNxtBytes;
         FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        k_fse_encode_blocks<1><<<(unsigned)nj, kFseGroupThreads, smem, st>>>(cls, d_jobs, (unsigned)nj, gb.slots,
-                                                                            gb.sizes, bits, part, gb.cks, recs, d_order);
+        k_fse_encode_blocks<1><<<(unsigned)nj, kFseGroupThreads, smem, st>>>(
+            cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order, gb.phase);
     }
     FB2_CHECK_LAUNCH();
     return gb;
@@ -991,6 +1020,24 @@ GammaOut gamma_finish(Pool &pool, const GammaBlocks &gb, const uint32_t *d_vals,
     for (int g = 0; g < G; g++) out.man_ptr[g] = reinterpret_cast<const uint8_t *>(wbuf + gword[g]);
     std::vector<unsigned long long> hs = d2h(gb.sizes, gb.jobs.size(), st);
     tr.mark("class blocks coded");
+    if (gb.phase && tr.on) {
+        const size_t nj = gb.jobs.size();
+        const std::vector<unsigned long long> ph = d2h(gb.phase, nj * kFsePhases, st);
+        unsigned long long t0 = ~0ULL, t1 = 0;
+        double sum[6] = {0};
+        for (size_t j = 0; j < nj; j++) {
+            const unsigned long long *p = ph.data() + j * kFsePhases;
+            t0 = std::min(t0, p[0]);
+            t1 = std::max(t1, p[6]);
+            for (int k = 0; k < 6; k++)
+                if (p[k] && p[k + 1]) sum[k] += (double)(p[k + 1] - p[k]);
+        }
+        std::fprintf(stderr,
+                     "[falcons trace] gamma class blocks: %zu, span %.3f ms; per block (us): count %.1f plan %.1f "
+                     "tables %.1f chain walk %.1f pack %.1f output %.1f\n",
+                     nj, (double)(t1 - t0) / 1e6, sum[0] / nj / 1e3, sum[1] / nj / 1e3, sum[2] / nj / 1e3,
+                     sum[3] / nj / 1e3, sum[4] / nj / 1e3, sum[5] / nj / 1e3);
+    }
     for (size_t j = 0; j < gb.jobs.size(); j++) {
         const int g = gb.job_group[j];
         const size_t sz = (size_t)(hs[j] & ((1ULL << 56) - 1));
@@ -1063,59 +1110,97 @@ void add_class_pieces(Assembler &as, const GammaOut &go, int g, CkptCollector *c
 // the group's running bit offset boff), k = cls[i].  The group starts (and, when there are few
 // groups, the group tables) sit in shared memory; the mantissa bits come from at most two
 // aligned words.
-constexpr int kUnpackGroupsSmem = 1024;
-__global__ void __launch_bounds__(256) k_gamma_unpack(const uint8_t *__restrict__ cls,
-                                                      const unsigned long long *__restrict__ boff, long long n,
-                                                      const unsigned long long *__restrict__ gstart, int G,
-                                                      const unsigned long long *__restrict__ gman,
-                                                      const uint8_t *__restrict__ base,
-                                                      const unsigned long long *__restrict__ gman_len,
-                                                      uint32_t *__restrict__ v, int *__restrict__ err,
-                                                      const unsigned long long *__restrict__ gdst,
-                                                      int16_t *__restrict__ ovf) {
-    __shared__ unsigned long long s_gs[kUnpackGroupsSmem + 1];
-    const bool in_smem = G + 1 <= kUnpackGroupsSmem;
-    if (in_smem)
-        for (int g = threadIdx.x; g <= G; g += blockDim.x) s_gs[g] = gstart[g];
-    __syncthreads();
-    const unsigned long long *gs = in_smem ? s_gs : gstart;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int k = cls[i];
-        // the last group whose start is at or before i
-        int lo = 0, hi = G - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (gs[mid] <= (unsigned long long)i) lo = mid;
-            else hi = mid - 1;
+// Gamma unpacking in units of kUnit values: the values of group g, [gstart[g], gstart[g + 1]),
+// are cut into units from the group's start; unit u of the whole list belongs to the last group g
+// with ustart[g] <= u.  A warp sums a unit's classes (its mantissa bits); an exclusive scan of the
+// unit sums gives every unit its first bit; a thread then reads its unit's mantissas in order
+// (MSB-first bits of the group's byte region, one aligned word at a time).
+constexpr unsigned kUnit = 1024;
+
+__device__ __forceinline__ int unit_group(const unsigned long long *__restrict__ ustart, int G, unsigned long long u) {
+    int lo = 0, hi = G - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ustart[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_unit_bits(const uint8_t *__restrict__ cls,
+                                                   const unsigned long long *__restrict__ gstart,
+                                                   const unsigned long long *__restrict__ ustart, int G,
+                                                   unsigned long long nunits, unsigned long long *__restrict__ usum) {
+    const unsigned long long u = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (u >= nunits) return;
+    const int g = unit_group(ustart, G, u);
+    const unsigned long long first = gstart[g] + (u - ustart[g]) * kUnit;
+    const unsigned long long end = min(first + kUnit, gstart[g + 1]);
+    uint32_t s = 0;
+    for (unsigned long long i = first + lane; i < end; i += 32) s += cls[i];
+    s = __reduce_add_sync(0xffffffffu, s);
+    if (lane == 0) usum[u] = s;
+}
+
+// Escape values (zigzag + 1, gamma-coded) of every unit, a warp per unit: v[i] = (1 << k) |
+// mantissa, or, with `ovf`, the escape code unzz(v - 1) at its place gdst[g] + (i - gstart[g]).
+// uoff is the exclusive scan of the unit bit sums; the warp takes its unit's values 32 at a time,
+// a warp scan of their classes giving each lane its mantissa's bit offset.  A class above 31 sets
+// err 2, a mantissa past its group's region err 3.
+__global__ void __launch_bounds__(256) k_gamma_unpack_units(
+    const uint8_t *__restrict__ cls, const unsigned long long *__restrict__ gstart,
+    const unsigned long long *__restrict__ ustart, int G, unsigned long long nunits,
+    const unsigned long long *__restrict__ uoff, const unsigned long long *__restrict__ gman,
+    const uint8_t *__restrict__ base, const unsigned long long *__restrict__ gman_len, uint32_t *__restrict__ v,
+    int *__restrict__ err, const unsigned long long *__restrict__ gdst, int16_t *__restrict__ ovf) {
+    const unsigned long long u = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31u;
+    if (u >= nunits) return;
+    const int g = unit_group(ustart, G, u);
+    const unsigned long long g0 = gstart[g];
+    const unsigned long long first = g0 + (u - ustart[g]) * kUnit;
+    const unsigned long long end = min(first + kUnit, gstart[g + 1]);
+    const unsigned long long len = gman_len[g];
+    const uint8_t *rb = base + gman[g];
+    unsigned long long run = uoff[u] - uoff[ustart[g]];  // bit offset of the values below
+    bool bad2 = false, bad3 = false;
+    for (unsigned long long i0 = first; i0 < end; i0 += 32) {
+        const unsigned long long i = i0 + lane;
+        const bool act = i < end;
+        const unsigned k = act ? cls[i] : 0u;
+        uint32_t incl = k;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += t;
         }
-        const int g = lo;
+        const unsigned long long bb = run + incl - k;
+        run += __shfl_sync(0xffffffffu, incl, 31);
+        if (!act) continue;
         uint32_t m = 0;
         if (k > 31) {
-            atomicExch(err, 2);
+            bad2 = true;
         } else if (k > 0) {
-            const unsigned long long bb = boff[i] - boff[gs[g]];
-            const unsigned long long byte0 = bb >> 3;
-            if (((bb + k + 7) >> 3) > gman_len[g]) {
-                atomicExch(err, 3);
+            if (((bb + k + 7) >> 3) > len) {
+                bad3 = true;
             } else {
-                const uintptr_t a = reinterpret_cast<uintptr_t>(base + gman[g] + byte0);
+                const uintptr_t a = reinterpret_cast<uintptr_t>(rb + (bb >> 3));
                 const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
-                const unsigned lead = (unsigned)(a & 3);                 // bytes before the first one
+                const unsigned lead = (unsigned)(a & 3);
                 const unsigned need = lead + (unsigned)((((bb & 7) + k) + 7) >> 3);  // bytes from w[0]
                 const uint32_t w0 = __byte_perm(w[0], 0, 0x0123);
                 const uint32_t w1 = need > 4 ? __byte_perm(w[1], 0, 0x0123) : 0u;
                 const unsigned long long be = ((unsigned long long)w0 << 32) | w1;  // big-endian bytes
-                const unsigned off = lead * 8 + (unsigned)(bb & 7);
-                m = (uint32_t)((be << off) >> (64 - k));
+                m = (uint32_t)((be << (lead * 8 + (unsigned)(bb & 7))) >> (64 - k));
             }
         }
-        const uint32_t val = (k <= 31) ? ((1u << k) | m) : 0u;
-        if (ovf) {  // escape values: zigzag + 1 gamma-coded, written in place as int16
-            ovf[gdst[g] + ((unsigned long long)i - gs[g])] = (int16_t)unzz(val - 1u);
-        } else {
-            v[i] = val;
-        }
+        const uint32_t val = k <= 31 ? ((1u << k) | m) : 0u;
+        if (ovf) ovf[gdst[g] + (i - g0)] = (int16_t)unzz(val - 1u);
+        else v[i] = val;
     }
+    if (bad2) atomicExch(err, 2);
+    if (bad3) atomicExch(err, 3);
 }
 
 // ------------------------------------------------------------------ delta
@@ -2622,19 +2707,25 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, FBLK));
     k_fse_decode_blocks<<<(unsigned)jobs.size(), kFseDecThreads, FBLK, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
     FB2_CHECK_LAUNCH();
-    unsigned long long *boff = pool.get<unsigned long long>(T + 1);
-    void *sc = pool.get<uint8_t>(scan_scratch_bytes(T, 8));
-    exclusive_scan<uint8_t, unsigned long long>(cls, T, boff, sc, st);
-    std::vector<unsigned long long> gman(G), glen(G);
+    std::vector<unsigned long long> gman(G), glen(G), ust(G + 1, 0);
     for (int g = 0; g < G; g++) {
         gman[g] = man_off[g];
         glen[g] = man_len[g];
+        ust[g + 1] = ust[g] + (gstart[g + 1] - gstart[g] + kUnit - 1) / kUnit;
     }
+    const unsigned long long NU = ust[G];
     unsigned long long *d_gstart = h2d(pool, gstart, st);
     unsigned long long *d_gman = h2d(pool, gman, st);
     unsigned long long *d_glen = h2d(pool, glen, st);
-    k_gamma_unpack<<<grid_for(T, 256, 148 * 8), 256, 0, st>>>(cls, boff, T, d_gstart, G, d_gman, d, d_glen, d_vals, d_err,
-                                                    d_gdst, d_ovf);
+    unsigned long long *d_ust = h2d(pool, ust, st);
+    unsigned long long *usum = pool.get<unsigned long long>(NU + 1);
+    unsigned long long *uoff = pool.get<unsigned long long>(NU + 1);
+    void *sc = pool.get<uint8_t>(scan_scratch_bytes((long long)NU, 8));
+    k_unit_bits<<<grid_for((long long)NU * 32, 256), 256, 0, st>>>(cls, d_gstart, d_ust, G, NU, usum);
+    FB2_CHECK_LAUNCH();
+    exclusive_scan<unsigned long long, unsigned long long>(usum, (long long)NU, uoff, sc, st);
+    k_gamma_unpack_units<<<grid_for((long long)NU * 32, 256), 256, 0, st>>>(cls, d_gstart, d_ust, G, NU, uoff, d_gman,
+                                                                           d, d_glen, d_vals, d_err, d_gdst, d_ovf);
     FB2_CHECK_LAUNCH();
 }
 
@@ -3084,6 +3175,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
                       cudaStream_t st, const DecodeCheckpoints *ck) {
     Trace tr("decode");
     Pool pool(st);
+    tr.gpu("decode begin", st);
     // checkpoint arrays, copied to aligned scratch (their place in the stream has any alignment)
     auto pow2 = [](uint32_t v) { return v >= 64 && v <= (uint32_t)FBLK && (v & (v - 1)) == 0; };
     const O1Ckpt *o1ck = nullptr;
@@ -3224,6 +3316,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
             }
             launch_gather(spool, pcs, reinterpret_cast<uint8_t *>(ovf), fork.side);
         }
+        tr.gpu("escapes decoded", fork.side);
         tr.mark("escapes launched");
         // decode tables: consecutive segments with identical tables share one decode table set
         std::vector<int> uid(S, 0);
@@ -3257,6 +3350,7 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         uint8_t *spread = pool.get<uint8_t>(16);
         k_o1_dtable<<<ntab, kTabThreads, 0, st>>>(nf, dt, spread, d_err);
         FB2_CHECK_LAUNCH();
+        tr.gpu("decode tables built", st);
         for (auto &c : chains) c.table = uid[c.table];
         // checkpoint base of every chain; the checkpoints are used only if their count matches
         bool parts_ok = false;
@@ -3319,8 +3413,10 @@ size_t entropy_decode(Context &ctx, const uint8_t *d_in, const ByteView &h, size
         throw std::invalid_argument("unsupported entropy method");
     }
     tr.mark("chains launched");
+    tr.gpu("chains decoded", st);
     if (delta) undelta(pool, d_codes, N, st);
     std::vector<int> he = d2h(d_err, 2, st);
+    tr.gpu_dump();
     tr.mark("chains done");
     if (he[1] && ck) {
         // a checkpoint did not match the stream: decode again, sequentially
