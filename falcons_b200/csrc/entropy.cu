@@ -143,6 +143,7 @@ struct FseGroupSmem {
     unsigned tl, hdr, s0, s1, maxsv, i0, i1, minsv, fast, high;
     unsigned lead[2];
     uint32_t sh[32];
+    unsigned long long tend[2];  // traced calls: when each chain walk ended
 };
 
 // A group's barrier.  bar.sync counts whole warps, so the warp is made convergent first (after
@@ -155,11 +156,13 @@ __device__ __forceinline__ void group_sync(unsigned bar) {
 // Phase times of a block (traced calls only): the global timer at the block's start and after its
 // count, plan, tables, chain walk, pack and output, kFsePhases words per block.
 constexpr int kFsePhases = 8;
-__device__ __forceinline__ void fse_phase(unsigned long long *phase, unsigned slot, int k) {
-    if (!phase) return;
+__device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    phase[(size_t)slot * kFsePhases + k] = t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t)::"memory");
+    return t;
+}
+__device__ __forceinline__ void fse_phase(unsigned long long *phase, unsigned slot, int k) {
+    if (phase) phase[(size_t)slot * kFsePhases + k] = global_ns();
 }
 
 // Exclusive scan over a group's threads (tid = index in the group), total of the group in `total`.
@@ -482,10 +485,13 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
             s_lead[k] = lead;
             if (k == 0) s_s0 = v + L;
             else s_s1 = v + L;
+            // the walk's end, taken by the chain lane itself (a lane that waits at the barrier
+            // below may read the timer before the barrier completes)
+            if (phase) gm.tend[k] = global_ns();
         }
     }
     group_sync(bar);
-    if (tid == 0) fse_phase(phase, slot, 4);
+    if (tid == 0 && phase) phase[(size_t)slot * kFsePhases + 4] = s_mode == 2 ? max(gm.tend[0], gm.tend[1]) : global_ns();
     int mode = s_mode;
     size_t body = 0;
     if (mode == 2) {
