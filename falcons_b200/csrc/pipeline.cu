@@ -116,7 +116,9 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
     c.openmp = 0;  // serial stream format
     if (c.quantbinCnt <= 0 || c.quantbinCnt > 65536) throw std::invalid_argument("QuantizationBinTotal must be in [2, 65536]");
     double max_abs = -1;
+    tr.gpu("begin", st);
     resolve_error_bound<T>(ctx, c, d_x, st, &max_abs);
+    tr.gpu("error bound resolved", st);
     tr.mark("error bound resolved");
     // the interpolation kernels' choice of fused passes depends on the field's largest |value|
     // (requant_exact in interp.cu); measured here when the error bound did not need the range
@@ -167,6 +169,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
             unsigned long long *nesc = pool.get<unsigned long long>(2);
             interp_compress_passes<T>(plan, d_x, codes, ws, nesc, st);
+            tr.gpu("prediction done", st);
             tr.mark("interpolation launched");
             const EntropyChoice ch = choose_entropy(ctx, codes, (size_t)plan.n_codes, st);  // syncs: nesc ready
             tr.mark("entropy method chosen");
@@ -178,6 +181,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             // the unpredictable list, sized from the escape count (not the field)
             T *unpred = pool.get<T>((size_t)n_unpred + 16);
             interp_compress_finish<T>(plan, d_x, codes, unpred, ws, st);
+            tr.gpu("unpredictable list done", st);
             DecompHeader dh{};
             dh.N = c.N;
             for (int i = 0; i < c.N; i++) dh.dims[i] = c.dims[i];
@@ -206,11 +210,14 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             tune.join_ev = ctx.side_ev[1];
             tune.queued_ev = ctx.side_ev[2];
             entropy_encode_into(pool, as, codes, (size_t)plan.n_codes, ch, st, tune);
+            tr.gpu("entropy stage done", st);
             tr.mark("entropy stage launched");
             if (as.framed_size() > pcap) throw std::length_error("The buffer for compressed data is not large enough.");
             tr.mark("framed size checked");
             payload = as.run_framed(pool, d_pay, st);
             core = 8 + zstd_raw_frame_size(as.pos);
+            tr.gpu("payload assembled", st);
+            tr.gpu_dump();
             tr.mark("payload assembled");
             c.cmprAlgo = ALGO_INTERP;
         } catch (std::length_error &) {
@@ -304,6 +311,7 @@ template <class T>
 void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_out, cudaStream_t st) {
     Trace tr("decompress");
     Pool pool(st);
+    tr.gpu("begin", st);
     const uint64_t L = pl.L;
     const ByteView &view = pl.view;
     uint8_t *d_flat = pool.get<uint8_t>(L + 16);
@@ -359,12 +367,16 @@ void decompress_core(Context &ctx, const falcons_config &c, Payload &pl, T *d_ou
     if ((long long)n_codes != plan.n_codes) throw std::invalid_argument("code count does not match the field");
     int16_t *codes = pool.get<int16_t>((size_t)n_codes + 16);
     tr.mark("headers parsed");
+    tr.gpu("payload gathered", st);
     entropy_decode(ctx, d_flat + off, view.sub(off), (size_t)n_codes, codes, st,
                    pl.ck.n_o1 + pl.ck.n_fse ? &pl.ck : nullptr);
     tr.mark("entropy stage launched");
+    tr.gpu("codes decoded", st);
     void *ws = pool.get<uint8_t>(interp_workspace_bytes(plan, sizeof(T)));
     interp_decompress<T>(plan, codes, unpred, n_unpred, d_out, ws, st);
+    tr.gpu("field reconstructed", st);
     interp_decompress_check(plan, sizeof(T), ws, n_unpred, st);  // waits for the stream
+    tr.gpu_dump();
     tr.mark("reconstructed");
 }
 
