@@ -1,7 +1,8 @@
 // Batches of fields (batch.cuh): a worker per host thread, each with its own context, fields
 // handed out largest first; the worker count per direction and field-size class is tuned on the
-// first batch of that class (successive slices of the batch run with 2, 4, 8 and 16 workers, and
-// the count with the highest field bytes per second is kept).
+// first batch of that class (successive slices of the batch run with 2, 4, 8 and 16 workers, then,
+// where the batch has the fields, with 16, 8, 4 and 2 again, and the count with the highest field
+// bytes per second in either round is kept).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -140,25 +141,40 @@ void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n
         } else {
             // tune on the batch's own fields, in their given order (a mix of sizes): per candidate
             // count, a slice of w fields that is not timed (the workers' first calls size their
-            // scratch), then a timed slice of 6 w fields
-            double best_rate = 0;
-            int best_w = 0, measured = 0;
-            for (int w : {2, 4, 8, 16}) {
-                if (n - pos < (size_t)(7 * w)) break;
-                ensure_workers(bp, w);
-                run_range(bp, compress, items, order, pos, pos + w, w, errs);
-                pos += w;
-                const double s = run_range(bp, compress, items, order, pos, pos + 6 * w, w, errs);
-                size_t b = 0;
-                for (size_t k = pos; k < pos + 6 * w; k++) b += bytes[order[k]];
-                const double rate = s > 0 ? (double)b / s : 0;
-                if (rate > best_rate) {
-                    best_rate = rate;
-                    best_w = w;
+            // scratch), then a timed slice of 6 w fields; where the batch has the fields, the
+            // candidates run a second time in the reverse order and each keeps its better rate (a
+            // slice that met a stall of the device or the driver does not decide alone)
+            const int cand[4] = {2, 4, 8, 16};
+            double rate_of[4] = {0, 0, 0, 0};
+            int measured = 0;
+            for (int round = 0; round < 2; round++) {
+                for (int c = 0; c < 4; c++) {
+                    const int ci = round == 0 ? c : 3 - c;
+                    const int w = cand[ci];
+                    if (round == 1 && rate_of[ci] == 0) continue;  // not measured in the first round
+                    if (n - pos < (size_t)(7 * w)) {
+                        if (round == 0) break;
+                        continue;
+                    }
+                    ensure_workers(bp, w);
+                    run_range(bp, compress, items, order, pos, pos + w, w, errs);
+                    pos += w;
+                    const double s = run_range(bp, compress, items, order, pos, pos + 6 * w, w, errs);
+                    size_t b = 0;
+                    for (size_t k = pos; k < pos + 6 * w; k++) b += bytes[order[k]];
+                    const double rate = s > 0 ? (double)b / s : 0;
+                    if (round == 0) measured++;
+                    rate_of[ci] = std::max(rate_of[ci], rate);
+                    pos += 6 * w;
                 }
-                measured++;
-                pos += 6 * w;
             }
+            int best_w = 0;
+            double best_rate = 0;
+            for (int c = 0; c < 4; c++)
+                if (rate_of[c] > best_rate) {
+                    best_rate = rate_of[c];
+                    best_w = cand[c];
+                }
             W = best_w ? best_w : 8;
             if (measured >= 2) bp.best[key] = W;
         }
