@@ -24,6 +24,44 @@ Pool::~Pool() {
 }
 
 namespace {
+std::mutex g_stage_mu;
+std::vector<void *> g_stage_free;  // page-locked buffers of kStageBytes not in use (kept for the process)
+}  // namespace
+
+void *stage_acquire() {
+    {
+        std::lock_guard<std::mutex> lk(g_stage_mu);
+        if (!g_stage_free.empty()) {
+            void *p = g_stage_free.back();
+            g_stage_free.pop_back();
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, kStageBytes, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();  // the caller falls back to a pageable copy
+        return nullptr;
+    }
+    return p;
+}
+
+void stage_release(void *p) {
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    g_stage_free.push_back(p);
+}
+
+void stage_reserve(int n) {
+    for (int i = 0; i < n; i++) {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, kStageBytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        stage_release(p);
+    }
+}
+
+namespace {
 __global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__restrict__ out) {
     for (int p = blockIdx.x; p < np; p += gridDim.x) {
         const Piece pc = pieces[p];

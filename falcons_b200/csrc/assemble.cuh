@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <vector>
 
@@ -35,12 +36,33 @@ struct Pool {
     ~Pool();
 };
 
+// Pinned host staging for small device-to-host reads: a process-wide free list of page-locked
+// buffers of kStageBytes, one taken per read and given back after it (the list grows only while
+// more reads are in flight at once than ever before).  A copy into pageable memory goes through
+// the driver's own staging, which concurrent callers share.
+constexpr size_t kStageBytes = 1 << 20;
+void *stage_acquire();
+void stage_release(void *p);
+// Adds n buffers to the free list (page-locking host memory synchronizes the device, so a context
+// reserves its share when it is created rather than on a call that other streams are running beside).
+void stage_reserve(int n);
+
 template <class T>
 std::vector<T> d2h(const T *d, size_t n, cudaStream_t st) {
     std::vector<T> h(n);
     if (n) {
-        FB2_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaStreamSynchronize(st));
+        const size_t bytes = n * sizeof(T);
+        void *stage = bytes <= kStageBytes ? stage_acquire() : nullptr;
+        if (stage) {
+            cudaError_t e = cudaMemcpyAsync(stage, d, bytes, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) std::memcpy(h.data(), stage, bytes);
+            stage_release(stage);
+            FB2_CUDA(e);
+        } else {
+            FB2_CUDA(cudaMemcpyAsync(h.data(), d, bytes, cudaMemcpyDeviceToHost, st));
+            FB2_CUDA(cudaStreamSynchronize(st));
+        }
     }
     return h;
 }

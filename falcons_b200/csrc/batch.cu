@@ -11,6 +11,7 @@
 #include <string>
 #include <thread>
 
+#include "assemble.cuh"
 #include "batch.cuh"
 #include "pipeline.cuh"
 
@@ -41,6 +42,7 @@ void init_worker(Context &c, int device) {
     c.device = device;
     FB2_CUDA(cudaSetDevice(device));
     FB2_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    stage_reserve(2);  // this worker's share of the pinned read staging
     for (auto &e : c.ev) FB2_CUDA(cudaEventCreate(&e));
 }
 

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../../include/falcons_b200.h"
+#include "assemble.cuh"
 #include "batch.cuh"
 #include "context.cuh"
 #include "interp.cuh"
@@ -159,6 +160,7 @@ int falcons_ctx_create(falcons_ctx **out, int device) {
         c->c.device = device;
         c->batch.device = device;
         FB2_CUDA(cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking));
+        fb2::stage_reserve(2);  // this context's share of the pinned read staging
         for (auto &e : c->c.ev) FB2_CUDA(cudaEventCreate(&e));
         *out = c;
     });

@@ -911,6 +911,22 @@ __global__ void k_pick_u64(const unsigned long long *__restrict__ src, const uns
     if (i < n) out[i] = src[idx[i]];
 }
 
+// The FSE block coders' shared-memory limits, set once per device (a function attribute set while
+// other threads launch the same kernel would only add driver work to every call).
+void enable_fse_smem() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    FB2_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return;
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<kFseGroups>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kFseGroups * kFseNxtBytes)));
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kFseNxtBytes));
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, FBLK));
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 // The FSE class blocks of the gamma classes, launched by gamma_launch; gamma_finish packs the
 // mantissas and collects the blocks.  Between the two the caller may launch other work: the class
 // blocks are long sequential chains, so they go to the GPU before the order-1 chain encoder.
@@ -969,15 +985,14 @@ GammaBlocks gamma_launch(Pool &pool, const uint32_t *d_vals, const std::vector<u
         gb.phase = pool.get<unsigned long long>(nj * kFsePhases);
         FB2_CUDA(cudaMemsetAsync(gb.phase, 0, nj * kFsePhases * 8, st));
     }
+    enable_fse_smem();
     if (nj + beside > (size_t)sm_count()) {
         constexpr unsigned G = kFseGroups;
         constexpr int smem = (int)(G * kFseNxtBytes);
-        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         k_fse_encode_blocks<G><<<(unsigned)((nj + G - 1) / G), G * kFseGroupThreads, smem, st>>>(
             cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order, gb.phase);
     } else {
         constexpr int smem = (int)kFseNxtBytes;
-        FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         k_fse_encode_blocks<1><<<(unsigned)nj, kFseGroupThreads, smem, st>>>(
             cls, d_jobs, (unsigned)nj, gb.slots, gb.sizes, bits, part, gb.cks, recs, d_order, gb.phase);
     }
@@ -2710,7 +2725,7 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     }
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
-    FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, FBLK));
+    enable_fse_smem();
     k_fse_decode_blocks<<<(unsigned)jobs.size(), kFseDecThreads, FBLK, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> gman(G), glen(G), ust(G + 1, 0);
@@ -2822,11 +2837,8 @@ void entropy_encode_into(Pool &pool, Assembler &as, const int16_t *d_codes_in, s
         FB2_CHECK_LAUNCH();
         k_prefix_last<<<1, 1024, 0, st>>>(tlast, tiles);
         FB2_CHECK_LAUNCH();
-        uint32_t nv32 = 0;
-        long long lastnz = -1;
-        FB2_CUDA(cudaMemcpyAsync(&nv32, tcnt + tiles, 4, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaMemcpyAsync(&lastnz, tlast + tiles, 8, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaStreamSynchronize(st));
+        const uint32_t nv32 = d2h(tcnt + tiles, 1, st)[0];
+        const long long lastnz = d2h(tlast + tiles, 1, st)[0];
         const unsigned long long nv = nv32;
         const bool trailing = N > 0 && lastnz < N - 1;
         const unsigned long long nr = nv + (trailing ? 1 : 0);

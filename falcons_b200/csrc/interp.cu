@@ -12,6 +12,7 @@
 #include <type_traits>
 
 #include "interp.cuh"
+#include "assemble.cuh"
 
 namespace fb2 {
 
@@ -1440,10 +1441,8 @@ void interp_decompress_check(const InterpPlan &plan, int elem_size, const void *
                              cudaStream_t st) {
     const WsLayout w = ws_layout(plan, elem_size);
     unsigned long long total = 0;
-    if (w.ntiles > 0) {
-        FB2_CUDA(cudaMemcpyAsync(&total, static_cast<const char *>(d_ws) + w.total_off, 8, cudaMemcpyDeviceToHost, st));
-        FB2_CUDA(cudaStreamSynchronize(st));
-    }
+    if (w.ntiles > 0)
+        total = d2h(reinterpret_cast<const unsigned long long *>(static_cast<const char *>(d_ws) + w.total_off), 1, st)[0];
     if ((long long)total > n_unpred - plan.n_anchor)
         throw std::invalid_argument("the codes name " + std::to_string(total) + " unpredictable values but the list holds " +
                                     std::to_string(n_unpred - plan.n_anchor) + " after the anchors");

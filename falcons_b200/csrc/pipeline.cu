@@ -173,9 +173,7 @@ size_t compress_impl(Context &ctx, const falcons_config &in_conf, T *d_x, uint8_
             tr.mark("interpolation launched");
             const EntropyChoice ch = choose_entropy(ctx, codes, (size_t)plan.n_codes, st);  // syncs: nesc ready
             tr.mark("entropy method chosen");
-            unsigned long long h_nesc = 0;
-            FB2_CUDA(cudaMemcpyAsync(&h_nesc, nesc, 8, cudaMemcpyDeviceToHost, st));
-            FB2_CUDA(cudaStreamSynchronize(st));
+            const unsigned long long h_nesc = d2h(nesc, 1, st)[0];
             const long long n_unpred = plan.n_anchor + (long long)h_nesc;
             if (n_unpred > 0x7fffffffLL) throw std::length_error("The buffer for compressed data is not large enough.");
             // the unpredictable list, sized from the escape count (not the field)
@@ -486,9 +484,7 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
     if (!d_stream_v || !d_out) throw std::invalid_argument("null pointer");
     const uint8_t *d_stream = static_cast<const uint8_t *>(d_stream_v);
     // Only the headers are needed on the host: the stream prefix and the header index frame.
-    std::vector<uint8_t> pre(std::min<size_t>(len, 4096));
-    FB2_CUDA(cudaMemcpyAsync(pre.data(), d_stream, pre.size(), cudaMemcpyDeviceToHost, st));
-    FB2_CUDA(cudaStreamSynchronize(st));
+    const std::vector<uint8_t> pre = d2h(d_stream, std::min<size_t>(len, 4096), st);
     falcons_config c;
     const size_t hs = config_load(pre.data(), len, c);
     if (c.num > cap_elems) throw std::invalid_argument("The decompression buffer is too small");
@@ -510,10 +506,9 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
             if (v == pl.L) {
                 const size_t frame = zstd_raw_frame_size(pl.L);
                 const size_t ipos = hs + 8 + frame;
-                uint8_t ih[8];
                 if (ipos + 8 <= len) {
-                    FB2_CUDA(cudaMemcpyAsync(ih, d_stream + ipos, 8, cudaMemcpyDeviceToHost, st));
-                    FB2_CUDA(cudaStreamSynchronize(st));
+                    const std::vector<uint8_t> ihv = d2h(d_stream + ipos, 8, st);
+                    const uint8_t *ih = ihv.data();
                     uint32_t m, sz;
                     memcpy(&m, ih, 4);
                     memcpy(&sz, ih + 4, 4);
@@ -521,10 +516,7 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
                         // the index content, plus the header of a checkpoint frame right after it
                         const size_t after = ipos + 8 + sz;
                         const size_t extra = std::min<size_t>(len - after, 8 + kCkptHeader);
-                        std::vector<uint8_t> content(sz + extra);
-                        FB2_CUDA(cudaMemcpyAsync(content.data(), d_stream + ipos + 8, sz + extra,
-                                                 cudaMemcpyDeviceToHost, st));
-                        FB2_CUDA(cudaStreamSynchronize(st));
+                        std::vector<uint8_t> content = d2h(d_stream + ipos + 8, sz + extra, st);
                         if (extra == 8 + kCkptHeader) {
                             uint32_t m2, sz2;
                             memcpy(&m2, content.data() + sz, 4);
