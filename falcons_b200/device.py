@@ -133,13 +133,14 @@ def decompress(stream_bytes: torch.Tensor, dtype, out: torch.Tensor | None = Non
     """Falcons_decompress of a device-resident stream into a device tensor (flat)."""
     assert stream_bytes.is_cuda and stream_bytes.dtype == torch.uint8
     ctx = ctx or _lib.default_context(stream_bytes.device.index or 0)
-    head = stream_bytes[:256].cpu().numpy()
-    c = _lib.Config()
-    # the header (at most 255 bytes) is inside the first 256 bytes of the stream
-    buf = bytearray(head.tobytes())
-    _lib.check(_lib.lib().falcons_read_config((ctypes.c_char * len(buf)).from_buffer(buf), ctypes.c_size_t(len(buf)),
-                                              ctypes.byref(c)), "read_config")
     if out is None:
+        # the field's size from the header (at most 255 bytes, inside the first 256 of the stream):
+        # a small device-to-host read, made only when the caller gives no output tensor
+        head = stream_bytes[:256].cpu().numpy()
+        c = _lib.Config()
+        buf = bytearray(head.tobytes())
+        _lib.check(_lib.lib().falcons_read_config((ctypes.c_char * len(buf)).from_buffer(buf),
+                                                  ctypes.c_size_t(len(buf)), ctypes.byref(c)), "read_config")
         out = torch.empty(int(c.num), dtype=dtype, device=stream_bytes.device)
     conf_out = _lib.Config()
     _lib.check(_lib.lib().falcons_decompress_device(ctx.ptr, _dtype_code(out), ctypes.c_void_p(stream_bytes.data_ptr()),
