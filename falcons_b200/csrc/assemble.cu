@@ -327,6 +327,9 @@ size_t Assembler::run_framed(Pool &pool, uint8_t *d_out, cudaStream_t st) {
     }
     tr.mark("index frame built");
     uint8_t *dh = h2d(pool, hb, st);
+    tr.mark("host bytes copied");
+    if (tr.on)
+        std::fprintf(stderr, "[falcons trace] assemble: %zu host bytes, %zu pieces\n", hb.size(), out.size());
     for (size_t i : host_pieces) out[i].src = dh + reinterpret_cast<uintptr_t>(out[i].src);
     launch_gather(pool, out, d_out, st);
     tr.mark("gather launched");
