@@ -62,9 +62,23 @@ void stage_reserve(int n) {
 }
 
 namespace {
-__global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__restrict__ out) {
-    for (int p = blockIdx.x; p < np; p += gridDim.x) {
-        const Piece pc = pieces[p];
+// Pieces are cut into chunks of kGatherChunk bytes (at multiples of 16 bytes, which keeps the
+// alignment of source and destination), a CTA per chunk: chunk c belongs to the last piece whose
+// first chunk (cstart, an exclusive scan of the pieces' chunk counts) is at or before c.
+constexpr unsigned long long kGatherChunk = 32 * 1024;
+
+__global__ void k_gather(const Piece *__restrict__ pieces, const unsigned *__restrict__ cstart, int np,
+                         unsigned nchunks, uint8_t *__restrict__ out) {
+    for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        int lo = 0, hi = np - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cstart[mid] <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const Piece whole = pieces[lo];
+        const unsigned long long o = (unsigned long long)(c - cstart[lo]) * kGatherChunk;
+        const Piece pc{whole.src + o, whole.dst + o, min(kGatherChunk, whole.len - o)};
         const uint8_t *s = pc.src;
         uint8_t *d = out + pc.dst;
         // bytes up to the first 16-byte destination boundary, whole 16-byte destination words, and
@@ -75,15 +89,15 @@ __global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__re
         const uint8_t *s2 = s + head;
         uint4 *dv = reinterpret_cast<uint4 *>(d + head);
         const unsigned long long nv = (pc.len - head) / 16;
-        const unsigned o = (unsigned)((uintptr_t)s2 & 15);
-        if (o == 0) {
+        const unsigned so = (unsigned)((uintptr_t)s2 & 15);
+        if (so == 0) {
             const uint4 *sv = reinterpret_cast<const uint4 *>(s2);
             for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
         } else {
             // a destination word from the two aligned source words that hold its 16 bytes (both
             // hold bytes of the piece, so they are readable)
-            const uint4 *sa = reinterpret_cast<const uint4 *>(s2 - o);
-            const unsigned q = o >> 2, r = 8 * (o & 3);
+            const uint4 *sa = reinterpret_cast<const uint4 *>(s2 - so);
+            const unsigned q = so >> 2, r = 8 * (so & 3);
             for (unsigned long long i = threadIdx.x; i < nv; i += blockDim.x) {
                 const uint4 A = sa[i], B = sa[i + 1];
                 uint32_t w0, w1, w2, w3, w4;
@@ -102,24 +116,24 @@ __global__ void k_gather(const Piece *__restrict__ pieces, int np, uint8_t *__re
 
 void launch_gather(Pool &pool, const std::vector<Piece> &pieces, uint8_t *d_out, cudaStream_t st) {
     if (pieces.empty()) return;
-    // pieces longer than kGatherChunk are split (at multiples of 16 bytes, which keeps the
-    // alignment of source and destination) so that large copies spread over many CTAs
-    constexpr unsigned long long kGatherChunk = 32 * 1024;
-    std::vector<Piece> split;
-    const std::vector<Piece> *use = &pieces;
-    bool big = false;
-    for (const Piece &pc : pieces) big |= pc.len > kGatherChunk;
-    if (big) {
-        split.reserve(pieces.size() + 64);
-        for (const Piece &pc : pieces)
-            for (unsigned long long o = 0; o < pc.len || (o == 0 && pc.len == 0); o += kGatherChunk) {
-                split.push_back(Piece{pc.src + o, pc.dst + o, std::min(kGatherChunk, pc.len - o)});
-                if (pc.len == 0) break;
-            }
-        use = &split;
+    // the pieces and their first chunks go to the device in one copy
+    const size_t np = pieces.size();
+    std::vector<unsigned char> blob(np * sizeof(Piece) + (np + 1) * sizeof(unsigned));
+    Piece *hp = reinterpret_cast<Piece *>(blob.data());
+    unsigned *hc = reinterpret_cast<unsigned *>(blob.data() + np * sizeof(Piece));
+    unsigned long long chunks = 0;
+    for (size_t i = 0; i < np; i++) {
+        hp[i] = pieces[i];
+        hc[i] = (unsigned)chunks;
+        chunks += pieces[i].len ? (pieces[i].len + kGatherChunk - 1) / kGatherChunk : 1;
     }
-    Piece *dp = h2d(pool, *use, st);
-    k_gather<<<(unsigned)std::min<size_t>(use->size(), 65535), 256, 0, st>>>(dp, (int)use->size(), d_out);
+    hc[np] = (unsigned)chunks;
+    if (chunks >= (1ull << 32)) throw std::length_error("gather too large");
+    uint8_t *d = h2d(pool, blob, st);
+    const Piece *dp = reinterpret_cast<const Piece *>(d);
+    const unsigned *dc = reinterpret_cast<const unsigned *>(d + np * sizeof(Piece));
+    k_gather<<<(unsigned)std::min<unsigned long long>(chunks, 65535), 256, 0, st>>>(dp, dc, (int)np, (unsigned)chunks,
+                                                                                    d_out);
     FB2_CHECK_LAUNCH();
 }
 

@@ -99,7 +99,7 @@ struct Piece {
     unsigned long long len;
 };
 
-// Copies every piece to out + dst (one CTA per piece of at most 32 KiB, 16-byte destination words).
+// Copies every piece to out + dst (one CTA per 32 KiB chunk of a piece, 16-byte destination words).
 void launch_gather(Pool &pool, const std::vector<Piece> &pieces, uint8_t *d_out, cudaStream_t st);
 
 // Size of a raw-block zstd frame holding `content` bytes.
