@@ -507,8 +507,9 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
                 const size_t frame = zstd_raw_frame_size(pl.L);
                 const size_t ipos = hs + 8 + frame;
                 if (ipos + 8 <= len) {
-                    const std::vector<uint8_t> ihv = d2h(d_stream + ipos, 8, st);
-                    const uint8_t *ih = ihv.data();
+                    // the index frame's header and (usually all of) its content in one read
+                    const std::vector<uint8_t> head = d2h(d_stream + ipos, std::min<size_t>(len - ipos, 64 << 10), st);
+                    const uint8_t *ih = head.data();
                     uint32_t m, sz;
                     memcpy(&m, ih, 4);
                     memcpy(&sz, ih + 4, 4);
@@ -516,7 +517,10 @@ void decompress_device(Context &ctx, int elem, const void *d_stream_v, size_t le
                         // the index content, plus the header of a checkpoint frame right after it
                         const size_t after = ipos + 8 + sz;
                         const size_t extra = std::min<size_t>(len - after, 8 + kCkptHeader);
-                        std::vector<uint8_t> content = d2h(d_stream + ipos + 8, sz + extra, st);
+                        std::vector<uint8_t> content =
+                            8 + sz + extra <= head.size()
+                                ? std::vector<uint8_t>(head.begin() + 8, head.begin() + 8 + sz + extra)
+                                : d2h(d_stream + ipos + 8, sz + extra, st);
                         if (extra == 8 + kCkptHeader) {
                             uint32_t m2, sz2;
                             memcpy(&m2, content.data() + sz, 4);
