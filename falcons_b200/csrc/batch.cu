@@ -2,7 +2,7 @@
 // handed out largest first; the worker count per direction and field-size class is tuned on the
 // first batch of that class (successive slices of the batch run with 2, 4, 8 and 16 workers, then,
 // where the batch has the fields, with 16, 8, 4 and 2 again, and the count with the highest field
-// bytes per second in either round is kept).
+// bytes per second in either pass is kept).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -149,13 +149,13 @@ void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n
             const int cand[4] = {2, 4, 8, 16};
             double rate_of[4] = {0, 0, 0, 0};
             int measured = 0;
-            for (int round = 0; round < 2; round++) {
+            for (int pass = 0; pass < 2; pass++) {
                 for (int c = 0; c < 4; c++) {
-                    const int ci = round == 0 ? c : 3 - c;
+                    const int ci = pass == 0 ? c : 3 - c;
                     const int w = cand[ci];
-                    if (round == 1 && rate_of[ci] == 0) continue;  // not measured in the first round
+                    if (pass == 1 && rate_of[ci] == 0) continue;  // not measured in the first pass
                     if (n - pos < (size_t)(7 * w)) {
-                        if (round == 0) break;
+                        if (pass == 0) break;
                         continue;
                     }
                     ensure_workers(bp, w);
@@ -165,7 +165,7 @@ void run_batch(BatchPool &bp, bool compress, falcons_batch_item *items, size_t n
                     size_t b = 0;
                     for (size_t k = pos; k < pos + 6 * w; k++) b += bytes[order[k]];
                     const double rate = s > 0 ? (double)b / s : 0;
-                    if (round == 0) measured++;
+                    if (pass == 0) measured++;
                     rate_of[ci] = std::max(rate_of[ci], rate);
                     pos += 6 * w;
                 }
