@@ -668,6 +668,10 @@ __global__ void __launch_bounds__(G * kFseGroupThreads, 4 / G)
 // verified against the next one (a mismatch sets err[1] and the caller decodes again without
 // checkpoints).
 constexpr int kFseDecThreads = 64;  // parts of a block decode one per thread
+constexpr unsigned kPartPad = 4;     // bytes between the parts' regions of the decoded block (>= 2:
+                                     // the last part may hold two symbols past `part`)
+// the decoded block in shared memory: FBLK symbols plus kPartPad per part (parts of >= 64 symbols)
+constexpr int kFseDecSmem = FBLK + (FBLK / 64) * kPartPad;
 __global__ void __launch_bounds__(kFseDecThreads) k_fse_decode_blocks(const uint8_t *__restrict__ in,
                                                          const BlockJob *__restrict__ jobs,
                                                          uint8_t *__restrict__ cls, int *__restrict__ err,
@@ -793,16 +797,27 @@ __global__ void __launch_bounds__(kFseDecThreads) k_fse_decode_blocks(const uint
             s0 = c.s0;
             s1 = c.s1;
         }
+        // Part q's symbols go to its own region of shared memory, kPartPad bytes more than a part
+        // apart, four to a word: the parts' word stores then fall on different banks.
+        uint8_t *so = s_out + (size_t)q * (nparts > 1 ? part + kPartPad : 0u);
         unsigned i = start;
+        uint32_t wv = 0;
+        unsigned k = 0;
         for (; i + 1 < end; i += 2) {
             const fse::DEntry e0 = dt[s0];
             const fse::DEntry e1 = dt[s1];
-            s_out[i] = e0.symbol;
-            s_out[i + 1] = e1.symbol;
+            wv |= ((uint32_t)e0.symbol | ((uint32_t)e1.symbol << 8)) << (8 * k);
+            k += 2;
+            if (k == 4) {
+                *reinterpret_cast<uint32_t *>(so + (i + 2 - start - 4)) = wv;
+                wv = 0;
+                k = 0;
+            }
             s0 = e0.newState + br.read(e0.nbBits);
             s1 = e1.newState + br.read(e1.nbBits);
         }
-        if (i < end) s_out[i] = dt[s0].symbol;
+        for (unsigned t = 0; t < k; t++) so[i - start - k + t] = (uint8_t)(wv >> (8 * t));
+        if (i < end) so[i - start] = dt[s0].symbol;
         if (q + 1 < nparts) {
             const FseCkpt c = cks[jb.ck + q];
             if (c.s0 != s0 || c.s1 != s1 || br.pos != br.start_bit(sp) + (int32_t)c.bitpos) atomicExch(err + 1, 1);
@@ -811,7 +826,17 @@ __global__ void __launch_bounds__(kFseDecThreads) k_fse_decode_blocks(const uint
     // the symbols leave in consecutive bytes across the CTA (each thread's part decoded into
     // shared memory, so that no warp store scatters over the parts)
     __syncthreads();
-    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) dst[i] = s_out[i];
+    if (nparts > 1) {
+        // the last part runs to the block's end (up to two symbols past `part`, which its
+        // region's padding holds)
+        const unsigned lp = 31 - __clz(part);
+        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
+            const unsigned r = min(i >> lp, nparts - 1);
+            dst[i] = s_out[(size_t)r * (part + kPartPad) + (i - r * part)];
+        }
+    } else {
+        for (unsigned i = threadIdx.x; i < n; i += blockDim.x) dst[i] = s_out[i];
+    }
 }
 
 // Walks an fse_enc record sequence (host bytes) for n symbols starting at `off`; appends jobs.
@@ -923,7 +948,7 @@ void enable_fse_smem() {
                                   (int)(kFseGroups * kFseNxtBytes)));
     FB2_CUDA(cudaFuncSetAttribute(k_fse_encode_blocks<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kFseNxtBytes));
-    FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, FBLK));
+    FB2_CUDA(cudaFuncSetAttribute(k_fse_decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, kFseDecSmem));
     done.fetch_or(bit, std::memory_order_acq_rel);
 }
 
@@ -2726,7 +2751,7 @@ void gamma_decode(Pool &pool, const uint8_t *d, const ByteView &h,
     uint8_t *cls = pool.get<uint8_t>(T);
     BlockJob *dj = h2d(pool, jobs, st);
     enable_fse_smem();
-    k_fse_decode_blocks<<<(unsigned)jobs.size(), kFseDecThreads, FBLK, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
+    k_fse_decode_blocks<<<(unsigned)jobs.size(), kFseDecThreads, kFseDecSmem, st>>>(d, dj, cls, d_err, fpart ? fpart : FBLK, d_fck);
     FB2_CHECK_LAUNCH();
     std::vector<unsigned long long> gman(G), glen(G), ust(G + 1, 0);
     for (int g = 0; g < G; g++) {
