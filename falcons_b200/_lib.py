@@ -57,7 +57,7 @@ EXPORTS = [
     "falcons_compress_device", "falcons_decompress_device", "falcons_interp_compress",
     "falcons_interp_decompress", "falcons_device_range", "falcons_encode_codes", "falcons_decode_codes",
     "falcons_interp_decompress_noalloc", "falcons_compress_batch", "falcons_decompress_batch",
-    "falcons_batch_workers",
+    "falcons_batch_workers", "falcons_time_levels", "falcons_level_times",
 ]
 
 

@@ -192,17 +192,53 @@ int falcons_interp_compress(falcons_ctx *ctx, int dtype, const size_t *dims, int
         const int es = dtype == FALCONS_DTYPE_F32 ? 4 : 8;
         void *ws = ctx->c.work.get(fb2::interp_workspace_bytes(plan, es));
         auto *cnt = static_cast<unsigned long long *>(ctx->c.small.get(64));
+        fb2::LaunchTimes lt;
+        fb2::LaunchTimes *ltp = ctx->c.time_levels ? &lt : nullptr;
         if (dtype == FALCONS_DTYPE_F32)
             fb2::interp_compress<float>(plan, static_cast<float *>(d_data), d_codes, static_cast<float *>(d_unpred),
-                                        ws, cnt, st);
+                                        ws, cnt, st, ltp);
         else
             fb2::interp_compress<double>(plan, static_cast<double *>(d_data), d_codes,
-                                         static_cast<double *>(d_unpred), ws, cnt, st);
+                                         static_cast<double *>(d_unpred), ws, cnt, st, ltp);
         unsigned long long h = 0;
         FB2_CUDA(cudaMemcpyAsync(&h, cnt, 8, cudaMemcpyDeviceToHost, st));
         FB2_CUDA(cudaStreamSynchronize(st));
+        if (ltp) {
+            lt.read();
+            ctx->c.lt_level.clear();
+            ctx->c.lt_ms.clear();
+            ctx->c.lt_codes.clear();
+            // plan levels run from the first point and the coarsest level down to level 1
+            for (const auto &x : lt.e) {
+                ctx->c.lt_level.push_back(x.level);
+                ctx->c.lt_ms.push_back(x.ms);
+                ctx->c.lt_codes.push_back((unsigned long long)fb2::level_codes(plan, x.level));
+            }
+        }
         if (n_codes) *n_codes = (size_t)plan.n_codes;
         if (n_unpred) *n_unpred = (size_t)(plan.n_anchor + (long long)h);
+    });
+}
+
+int falcons_time_levels(falcons_ctx *ctx, int on) {
+    return guarded([&] {
+        check_ctx(ctx);
+        std::lock_guard<std::mutex> lk(ctx->c.mu);
+        ctx->c.time_levels = on != 0;
+    });
+}
+
+int falcons_level_times(falcons_ctx *ctx, int *level, float *ms, unsigned long long *codes, int cap, int *count) {
+    return guarded([&] {
+        check_ctx(ctx);
+        std::lock_guard<std::mutex> lk(ctx->c.mu);
+        const int n = (int)ctx->c.lt_ms.size();
+        for (int i = 0; i < n && i < cap; i++) {
+            if (level) level[i] = ctx->c.lt_level[i];
+            if (ms) ms[i] = ctx->c.lt_ms[i];
+            if (codes) codes[i] = ctx->c.lt_codes[i];
+        }
+        if (count) *count = n;
     });
 }
 

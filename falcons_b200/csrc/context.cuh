@@ -55,6 +55,11 @@ struct PinnedBuf {
 struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // measurement of falcons_interp_compress (falcons_time_levels): the last call's launches
+    bool time_levels = false;
+    std::vector<int> lt_level;
+    std::vector<float> lt_ms;
+    std::vector<unsigned long long> lt_codes;
     std::mutex mu;                 // one call at a time per context
     DevBuf field, codes, unpred, work, work2, out, small;
     PinnedBuf host_small;

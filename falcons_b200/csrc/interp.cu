@@ -1389,17 +1389,22 @@ bool requant_exact(double eb, double max_abs) {
 
 // Runs the plan's passes in order, the fusable z + y + x and y + x passes as one kernel.
 template <class T, bool DECOMP>
-void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, unsigned *etile, cudaStream_t st) {
+void run_passes(const InterpPlan &plan, T *x, int16_t *codes, T *esc, unsigned *etile, cudaStream_t st,
+                LaunchTimes *lt = nullptr) {
     const std::vector<PassLaunch> &ps = plan.passes;
     for (size_t i = 0; i < ps.size();) {
         FusedYX F{};
         size_t used = 0;
         if ((fusable_zyx(ps, i, sizeof(T), F, used) || fusable_yx(ps, i, sizeof(T), F, used)) &&
             (DECOMP || requant_exact<T>(plan.levels[F.y.level].eb, plan.max_abs))) {
+            if (lt) lt->begin(F.y.level, st);
             launch_fused_yx<T, DECOMP>(F, x, codes, esc, plan.levels[F.y.level], etile, st);
+            if (lt) lt->end(st);
             i += used;
         } else {
+            if (lt) lt->begin(ps[i].level, st);
             launch_pass<T, DECOMP>(ps[i], x, codes, esc, plan.levels[ps[i].level], etile, st);
+            if (lt) lt->end(st);
             i++;
         }
     }
@@ -1450,7 +1455,7 @@ void interp_decompress_check(const InterpPlan &plan, int elem_size, const void *
 
 template <class T>
 void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, void *d_ws, unsigned long long *d_n_esc,
-                            cudaStream_t st) {
+                            cudaStream_t st, LaunchTimes *lt) {
     const WsLayout w = ws_layout(plan, sizeof(T));
     char *ws = static_cast<char *>(d_ws);
     T *esc = reinterpret_cast<T *>(ws + w.esc_off);
@@ -1463,7 +1468,7 @@ void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, vo
         k_first_point<T, false><<<1, 1, 0, st>>>(d_x, d_codes, esc, plan.levels[0], etile);
         FB2_CHECK_LAUNCH();
     }
-    run_passes<T, false>(plan, d_x, d_codes, esc, etile, st);
+    run_passes<T, false>(plan, d_x, d_codes, esc, etile, st, lt);
     if (w.ntiles > 0) {
         k_scan_u32<<<1, 1024, 0, st>>>(tiles, scan, w.ntiles, d_n_esc);
         FB2_CHECK_LAUNCH();
@@ -1495,8 +1500,8 @@ void interp_compress_finish(const InterpPlan &plan, const T *d_x, const int16_t 
 
 template <class T>
 void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
-                     unsigned long long *d_n_esc, cudaStream_t st) {
-    interp_compress_passes<T>(plan, d_x, d_codes, d_ws, d_n_esc, st);
+                     unsigned long long *d_n_esc, cudaStream_t st, LaunchTimes *lt) {
+    interp_compress_passes<T>(plan, d_x, d_codes, d_ws, d_n_esc, st, lt);
     interp_compress_finish<T>(plan, d_x, d_codes, d_unpred, d_ws, st);
 }
 
@@ -1639,18 +1644,47 @@ cudaError_t interp_decompress_preload() {
     return e != cudaSuccess ? e : preload_decompress_kernels<double>();
 }
 
+void LaunchTimes::begin(int level, cudaStream_t st) {
+    Entry x{level, nullptr, nullptr, 0.f};
+    FB2_CUDA(cudaEventCreate(&x.a));
+    FB2_CUDA(cudaEventCreate(&x.b));
+    e.push_back(x);
+    FB2_CUDA(cudaEventRecord(x.a, st));
+}
+void LaunchTimes::end(cudaStream_t st) { FB2_CUDA(cudaEventRecord(e.back().b, st)); }
+void LaunchTimes::read() {
+    for (Entry &x : e) {
+        FB2_CUDA(cudaEventSynchronize(x.b));
+        FB2_CUDA(cudaEventElapsedTime(&x.ms, x.a, x.b));
+    }
+}
+LaunchTimes::~LaunchTimes() {
+    for (Entry &x : e) {
+        if (x.a) cudaEventDestroy(x.a);
+        if (x.b) cudaEventDestroy(x.b);
+    }
+}
+
+long long level_codes(const InterpPlan &plan, int li) {
+    const long long off = (long long)plan.levels.size() - (long long)plan.level_starts.size();
+    const long long k = li - off;
+    if (k < 0 || k >= (long long)plan.level_starts.size()) return 0;
+    const long long end = k + 1 < (long long)plan.level_starts.size() ? plan.level_starts[k + 1] : plan.n_codes;
+    return end - plan.level_starts[k];
+}
+
 template void interp_compress<float>(const InterpPlan &, float *, int16_t *, float *, void *, unsigned long long *,
-                                     cudaStream_t);
+                                     cudaStream_t, LaunchTimes *);
 template void interp_compress_passes<float>(const InterpPlan &, float *, int16_t *, void *, unsigned long long *,
-                                            cudaStream_t);
+                                            cudaStream_t, LaunchTimes *);
 template void interp_compress_passes<double>(const InterpPlan &, double *, int16_t *, void *, unsigned long long *,
-                                             cudaStream_t);
+                                             cudaStream_t, LaunchTimes *);
 template void interp_compress_finish<float>(const InterpPlan &, const float *, const int16_t *, float *, void *,
                                             cudaStream_t);
 template void interp_compress_finish<double>(const InterpPlan &, const double *, const int16_t *, double *, void *,
                                              cudaStream_t);
 template void interp_compress<double>(const InterpPlan &, double *, int16_t *, double *, void *,
-                                      unsigned long long *, cudaStream_t);
+                                      unsigned long long *, cudaStream_t, LaunchTimes *);
 template void interp_decompress<float>(const InterpPlan &, const int16_t *, const float *, long long, float *,
                                        void *, cudaStream_t);
 template void interp_decompress<double>(const InterpPlan &, const int16_t *, const double *, long long, double *,

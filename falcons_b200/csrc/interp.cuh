@@ -68,16 +68,34 @@ InterpPlan make_plan(const long long *dims, int N, const InterpParams &p);
 // Scratch needed by the compress/decompress launchers (bytes).
 size_t interp_workspace_bytes(const InterpPlan &plan, int elem_size);
 
+// Device times of the pass launches of one call, for measurement: when a LaunchTimes is given,
+// a CUDA event pair is recorded on the stream around every pass launch (fused levels are one
+// launch each), with the level it codes; read() waits for the events and fills ms.
+struct LaunchTimes {
+    struct Entry {
+        int level;
+        cudaEvent_t a, b;
+        float ms;
+    };
+    std::vector<Entry> e;
+    void begin(int level, cudaStream_t st);
+    void end(cudaStream_t st);
+    void read();
+    ~LaunchTimes();
+};
+// Codes of plan level li (an index into plan.levels), from the level starts.
+long long level_codes(const InterpPlan &plan, int li);
+
 template <class T>
 void interp_compress(const InterpPlan &plan, T *d_x, int16_t *d_codes, T *d_unpred, void *d_ws,
-                     unsigned long long *d_n_esc, cudaStream_t st);
+                     unsigned long long *d_n_esc, cudaStream_t st, LaunchTimes *lt = nullptr);
 
 // interp_compress in two steps, so that the caller can size the unpredictable list from the
 // escape count (*d_n_esc after the first step) instead of the field: the passes, the escape
 // count and its scan; then the anchors and the escape values into d_unpred (n_anchor + count).
 template <class T>
 void interp_compress_passes(const InterpPlan &plan, T *d_x, int16_t *d_codes, void *d_ws,
-                            unsigned long long *d_n_esc, cudaStream_t st);
+                            unsigned long long *d_n_esc, cudaStream_t st, LaunchTimes *lt = nullptr);
 template <class T>
 void interp_compress_finish(const InterpPlan &plan, const T *d_x, const int16_t *d_codes, T *d_unpred, void *d_ws,
                             cudaStream_t st);

@@ -63,6 +63,25 @@ def interp_compress(x: torch.Tensor, params: _lib.InterpParams, ctx=None, stream
     return codes[:nq.value], unpred[:nu.value]
 
 
+def time_levels(on: bool = True, ctx=None, device: int = 0):
+    """Turns per-launch device timing of interp_compress on this context on or off (measurement)."""
+    ctx = ctx or _lib.default_context(device)
+    _lib.check(_lib.lib().falcons_time_levels(ctx.ptr, int(bool(on))), "time_levels")
+
+
+def level_times(ctx=None, device: int = 0):
+    """The last timed interp_compress call's launches: [(level, ms, codes of that level)], levels in
+    coding order (the coarsest first, the unit-step level last)."""
+    ctx = ctx or _lib.default_context(device)
+    cap = 256
+    lv = (ctypes.c_int * cap)()
+    ms = (ctypes.c_float * cap)()
+    cd = (ctypes.c_ulonglong * cap)()
+    n = ctypes.c_int(0)
+    _lib.check(_lib.lib().falcons_level_times(ctx.ptr, lv, ms, cd, cap, ctypes.byref(n)), "level_times")
+    return [(int(lv[i]), float(ms[i]), int(cd[i])) for i in range(min(n.value, cap))]
+
+
 def interp_decompress(shape, dtype, codes: torch.Tensor, unpred: torch.Tensor, params: _lib.InterpParams,
                       out: torch.Tensor | None = None, ctx=None, stream=None) -> torch.Tensor:
     dev = codes.device

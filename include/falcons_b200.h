@@ -115,6 +115,13 @@ int falcons_decompress_device(falcons_ctx *ctx, int dtype, const void *d_stream,
 int falcons_interp_compress(falcons_ctx *ctx, int dtype, const size_t *dims, int N, const falcons_interp_params *p,
                             void *d_data, int16_t *d_codes, void *d_unpred, size_t *n_codes, size_t *n_unpred,
                             void *stream);
+/* Per-launch device times of falcons_interp_compress on this context, for measurement (off by
+ * default).  With timing on, every call records a CUDA event pair on its stream around each pass
+ * launch (a fused level is one launch); falcons_level_times returns the last call's launches: the
+ * level each codes (levels in coding order, the coarsest first and the unit-step level last), its
+ * time in ms and the codes of that level, up to `cap` entries, and their number in *count. */
+int falcons_time_levels(falcons_ctx *ctx, int on);
+int falcons_level_times(falcons_ctx *ctx, int *level, float *ms, unsigned long long *codes, int cap, int *count);
 /* falcons_interp_decompress: d_unpred holds n_unpred values (the anchors, then one value per escape
  * code in stream order).  Codes that name more escapes than the list holds return FALCONS_EINVAL
  * without reading past the list.  The call waits for `stream` before it returns. */
